@@ -1,0 +1,189 @@
+/*
+ * mqb200: B200 (sm_100a) state-vector engine for MindQuantum's mqvector path.
+ *
+ * A C ABI (plain pointers and sizes, integer status codes, no C++ or torch types)
+ * over hand-written CUDA kernels.  State buffers are owned by the caller (e.g. torch
+ * tensors): a batch of `batch` states, each 2^n interleaved complex numbers
+ * (complex64 = 2 x float32, complex128 = 2 x float64), little endian
+ * (amplitude index bit q <-> qubit q), contiguous with stride 2^n.
+ *
+ * The entry points replace the method table of the reference's pybind module
+ * (`BindSim`, ccsrc/python/simulator/include/python/vector/bind_vec_state.h:47-83)
+ * and the state-vector policy it dispatches to:
+ *
+ *   mqb_program_create / mqb_apply           <- apply_circuit / apply_gate
+ *                                               (VectorState::ApplyCircuit, vector_state.tpp:949-960;
+ *                                                ApplyGate, vector_state.tpp:166-437)
+ *   mqb_ham_create / mqb_apply_hamiltonian   <- apply_hamiltonian (VectorState::ApplyHamiltonian,
+ *                                                vector_state.tpp:963-974; ApplyTerms,
+ *                                                cpu_vector_core_policy.cpp:133-161)
+ *   mqb_expectation                          <- get_expectation (GetExpectation, vector_state.tpp:712-726;
+ *                                                ExpectationOfTerms, cpu_vector_core_policy.cpp:212-261)
+ *   mqb_expectation_with_grad                <- get_expectation_with_grad_multi_multi
+ *                                               (GradientHelper::HermitianAdjointGradient, gradient.h:100-197)
+ *   mqb_vdot                                 <- blas.inner_product / Vdot (cpu_vector_core_dot_like.cpp:33-53)
+ *   mqb_sample_indices                       <- sampling_measure_ending_without_noise
+ *                                               (vector_state.tpp:1326-1373: cumulative probs + lower bound)
+ *   mqb_qubit_one_probability / mqb_collapse <- ApplyMeasure (vector_state.tpp:440-462)
+ *
+ * Every call returns MQB_OK (0) or a negative MQB_ERR_* code; mqb_last_error() returns
+ * the message of the last failure on the calling thread.  Device work is enqueued on
+ * the given cudaStream_t (passed as void*); calls return without synchronizing unless
+ * they say otherwise.
+ */
+#ifndef MQB200_H_
+#define MQB200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MQB_API __attribute__((visibility("default")))
+#else
+#define MQB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MQB_OK 0
+#define MQB_ERR_INVALID (-1)
+#define MQB_ERR_CUDA (-2)
+#define MQB_ERR_UNSUPPORTED (-3)
+#define MQB_ERR_WORKSPACE (-4)
+#define MQB_ERR_ALLOC (-5)
+
+#define MQB_PREC_C64 0  /* complex64 state, FP32 gate arithmetic, FP64 reductions */
+#define MQB_PREC_C128 1 /* complex128 state, FP64 everywhere */
+
+#define MQB_MAX_OBJ 6      /* max object qubits of one gate */
+#define MQB_MAX_ANGLES 3   /* max parameter expressions of one gate (U3 / Rn) */
+
+/* Gate ids: see mindquantum_b200/csrc/mqb_gate_ids.h (shared with the Python lowering). */
+
+/* One lowered gate.  Parameter expressions: angle[a] = angle_const[a] +
+ * sum_{t in [term_begin[a], term_begin[a]+term_count[a])} terms[t].coeff * params[terms[t].param]. */
+typedef struct mqb_gate_desc {
+    int32_t gate_id;
+    int32_t n_obj;
+    int32_t obj[MQB_MAX_OBJ];
+    uint64_t ctrl_mask;
+    int32_t n_angles;
+    int32_t grad_angles;          /* bit a set: angle a requires a gradient */
+    double angle_const[MQB_MAX_ANGLES];
+    int32_t term_begin[MQB_MAX_ANGLES];
+    int32_t term_count[MQB_MAX_ANGLES];
+    int64_t matrix_offset;        /* constant gates: offset (complex entries) into const_matrices;
+                                     custom parameterized gates: offset into the per-sample custom block */
+    uint64_t pauli_x, pauli_y, pauli_z; /* rotation about a Pauli string (GID_RPS), global masks */
+    int32_t pauli_ny;
+    int32_t reserved;
+} mqb_gate_desc;
+
+typedef struct mqb_param_term {
+    int32_t param;
+    int32_t flags;   /* bit 0: the parameter requires a gradient */
+    double coeff;
+} mqb_param_term;
+
+typedef struct mqb_program_options {
+    int32_t fuse;          /* 1: fused tile passes (default), 0: one kernel per gate (plain path) */
+    int32_t tile_bits;     /* 0: automatic */
+    int32_t reserved[6];
+} mqb_program_options;
+
+typedef struct mqb_program mqb_program;
+typedef struct mqb_hamiltonian mqb_hamiltonian;
+
+typedef struct mqb_program_info {
+    int32_t n_qubits;
+    int32_t precision;
+    int32_t n_ops;
+    int32_t n_params;
+    int32_t n_passes;        /* passes of the apply schedule */
+    int32_t tile_bits;
+    int32_t n_grad_slots;    /* gradient angles (per sample per Hamiltonian) */
+    int32_t per_sample_entries; /* complex entries of per-sample matrices */
+    int32_t custom_entries;  /* complex entries the caller uploads per sample for custom parameterized gates */
+    int32_t reserved[7];
+} mqb_program_info;
+
+MQB_API const char *mqb_last_error(void);
+MQB_API int mqb_version(void);
+MQB_API int mqb_device_sm_count(int *out);
+/* sizeof of mqb_gate_desc, mqb_param_term, mqb_program_options, mqb_program_info (ABI check). */
+MQB_API int mqb_abi_struct_sizes(int64_t *out, int n);
+
+/* ------------------------------------------------------------------ programs (circuits) */
+MQB_API int mqb_program_create(int n_qubits, int precision, const mqb_gate_desc *gates, int n_gates,
+                       const mqb_param_term *terms, int n_terms, int n_params, const double *const_matrices,
+                       int64_t n_const_entries, const mqb_program_options *options, mqb_program **out);
+MQB_API int mqb_program_destroy(mqb_program *prog);
+MQB_API int mqb_program_get_info(const mqb_program *prog, mqb_program_info *info);
+/* Host-only, no CUDA call: the pass schedule the engine builds for a gate table.  Arrays hold
+ * n_gates entries: order = gate indices in execution order, pass_of = pass of each executed gate,
+ * qmask / fused = tile qubit mask and kind (1 fused tile pass, 0 single-gate pass) of each pass. */
+MQB_API int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, int n_gates,
+                              const double *const_matrices, int64_t n_const_entries, int tile_bits, int fuse,
+                              int *n_passes, int32_t *order, int32_t *pass_of, uint64_t *qmask, int32_t *fused);
+/* Passes and tile bits of the schedule mqb_expectation_with_grad uses for n_hams Hamiltonians. */
+MQB_API int mqb_program_grad_passes(mqb_program *prog, int n_hams, int *n_passes, int *tile_bits);
+
+/* Workspace (bytes) that mqb_apply needs for `batch` samples. */
+MQB_API int mqb_apply_workspace_size(const mqb_program *prog, int64_t batch, size_t *bytes);
+
+/* Apply the program in place to `batch` states.  params: device [batch][n_params] float64
+ * (row stride param_stride, 0 = broadcast one row); custom: device [batch][custom_entries]
+ * complex128 (NULL if the program has no custom parameterized gate). */
+MQB_API int mqb_apply(mqb_program *prog, void *states, int64_t batch, const double *params, int64_t param_stride,
+              const double *custom, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------------------ Hamiltonians */
+MQB_API int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const uint64_t *mask_y,
+                   const uint64_t *mask_z, const int32_t *num_y, const double *coeff, int n_terms,
+                   mqb_hamiltonian **out);
+MQB_API int mqb_ham_destroy(mqb_hamiltonian *ham);
+
+/* out = H in (separate buffers), `batch` states. */
+MQB_API int mqb_apply_hamiltonian(const mqb_hamiltonian *ham, const void *in, void *out, int64_t batch, void *stream);
+
+/* out[b] = <bra_b| H |ket_b> as (re, im) float64 on the device, out has 2*batch doubles. */
+MQB_API int mqb_expectation(const mqb_hamiltonian *ham, const void *bra, const void *ket, int64_t batch, double *out,
+                    void *stream);
+
+/* out[b] = <a_b|b_b> as (re, im) float64 on the device. */
+MQB_API int mqb_vdot(int n_qubits, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream);
+
+/* ------------------------------------------------------------------ adjoint gradient */
+/* Workspace for mqb_expectation_with_grad with `batch` samples, `n_hams` Hamiltonians and a
+ * checkpoint stride (passes between stored states; 1 = every pass, larger saves memory). */
+MQB_API int mqb_grad_workspace_size(const mqb_program *prog, int64_t batch, int n_hams, int ckpt_stride, size_t *bytes);
+
+/* For every sample b: psi = U(params_b) init (init = |0..0> when init_states is NULL, else
+ * init_states[b] when init_batched, else init_states[0]); f[b][h] = <psi|H_h|psi> as (re, im);
+ * grad[b][h][p] = d f / d params[p] (real, the reference's 2 Re <psi|H dU|psi>).
+ * f: device [batch][n_hams][2] float64, grad: device [batch][n_hams][n_params] float64. */
+MQB_API int mqb_expectation_with_grad(mqb_program *prog, const mqb_hamiltonian *const *hams, int n_hams,
+                              const void *init_states, int init_batched, int64_t batch, const double *params,
+                              int64_t param_stride, const double *custom, double *f, double *grad,
+                              int ckpt_stride, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------------------ sampling / measurement */
+/* Sorted uniforms u[s] (device float64, ascending) -> amplitude indices out[s] (device int64):
+ * out[s] = smallest i with cdf(i) > u[s], cdf(i) = sum_{j<=i} |psi_j|^2 and cdf(dim-1) = 1.
+ * scratch: device buffer of at least mqb_sample_scratch_size bytes. */
+MQB_API int mqb_sample_scratch_size(int n_qubits, size_t *bytes);
+MQB_API int mqb_sample_indices(int n_qubits, int precision, const void *state, const double *sorted_u, int64_t shots,
+                       int64_t *out, void *scratch, size_t scratch_bytes, void *stream);
+
+/* out (device float64) = sum of |psi_i|^2 over indices with bit `qubit` set. */
+MQB_API int mqb_qubit_one_probability(int n_qubits, int precision, const void *state, int qubit, double *out,
+                              void *stream);
+/* Keep the half with bit `qubit` == outcome, scale it by `scale`, zero the other half. */
+MQB_API int mqb_collapse(int n_qubits, int precision, void *state, int qubit, int outcome, double scale, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MQB200_H_ */

@@ -1,0 +1,73 @@
+"""Build libmqb200.so (the CUDA kernels + C ABI) in-tree for sm_100a.
+
+    python -m mindquantum_b200.build_native        # rebuild if any source changed
+
+The library is compiled with nvcc for ``arch=compute_100a,code=sm_100a`` only and links the
+CUDA runtime statically, so the .so has no dependency beyond the NVIDIA driver.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, 'csrc')
+INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
+LIB = os.path.join(HERE, 'libmqb200.so')
+SOURCES = ['kernels.cu', 'capi.cpp', 'scheduler.cpp']
+HEADERS = ['kernels.cuh', 'mqb_internal.h', 'mqb_gate_ids.h']
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+
+
+def _nvcc():
+    for cand in (os.environ.get('NVCC'), '/usr/local/cuda/bin/nvcc', 'nvcc'):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return 'nvcc'
+
+
+def sources():
+    return [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, h) for h in HEADERS] + [
+        os.path.join(INCLUDE, 'mqb200.h')]
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(s) <= t for s in sources())
+
+
+def build(force=False, verbose=False):
+    """Compile the library unless it is newer than every source."""
+    if not force and up_to_date():
+        return LIB
+    bdir = os.path.join(os.path.dirname(HERE), '_build', 'mqb200')
+    os.makedirs(bdir, exist_ok=True)
+    env = dict(os.environ)
+    env.pop('CC', None)
+    env.pop('CXX', None)
+    common = ['-O3', '-std=c++17', '-Xcompiler', '-fPIC', '-Xcompiler', '-fvisibility=hidden',
+              '-Xcompiler', '-fvisibility-inlines-hidden', '-ccbin', 'g++', f'-I{INCLUDE}']
+    steps = [
+        [_nvcc(), *ARCH, '-lineinfo', *common, '-c', os.path.join(CSRC, 'kernels.cu'),
+         '-o', os.path.join(bdir, 'kernels.o')],
+        [_nvcc(), *ARCH, '-lineinfo', *common, '-x', 'cu', '-c', os.path.join(CSRC, 'capi.cpp'),
+         '-o', os.path.join(bdir, 'capi.o')],
+        [_nvcc(), *common, '-x', 'c++', '-c', os.path.join(CSRC, 'scheduler.cpp'),
+         '-o', os.path.join(bdir, 'scheduler.o')],
+        [_nvcc(), *ARCH, '-shared', '-cudart', 'static', '-ccbin', 'g++',
+         *[os.path.join(bdir, o) for o in ('kernels.o', 'capi.o', 'scheduler.o')], '-o', LIB + '.tmp'],
+    ]
+    for cmd in steps:
+        if verbose:
+            print(' '.join(cmd))
+        res = subprocess.run(cmd, capture_output=True, text=True, env=env)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError('building libmqb200.so failed')
+    os.replace(LIB + '.tmp', LIB)
+    return LIB
+
+
+if __name__ == '__main__':
+    print(build(force='--force' in sys.argv, verbose=True))

@@ -1,0 +1,794 @@
+// extern "C" entry points of libmqb200: lowering of gate tables, pass execution, the
+// checkpointed adjoint-gradient driver, Hamiltonian passes, reductions and sampling.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Fail : std::runtime_error {
+    int code;
+    Fail(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    throw Fail(code, buf);
+}
+
+void ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) fail(MQB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+template <typename F>
+int guarded(F &&f) {
+    try {
+        f();
+        return MQB_OK;
+    } catch (const Fail &e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return MQB_ERR_INVALID;
+    }
+}
+
+int sm_count_cached() {
+    static thread_local int dev = -1, count = 0;
+    int d = 0;
+    ck(cudaGetDevice(&d), "cudaGetDevice");
+    if (d != dev) {
+        ck(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, d), "cudaDeviceGetAttribute");
+        dev = d;
+    }
+    return count;
+}
+
+size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+template <typename T>
+T *upload(const std::vector<T> &v) {
+    if (v.empty()) return nullptr;
+    T *d = nullptr;
+    ck(cudaMalloc(&d, sizeof(T) * v.size()), "cudaMalloc");
+    ck(cudaMemcpy(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+    return d;
+}
+
+bool is_diag_gid(int gid) { return gid == GID_RZ || gid == GID_PS || gid == GID_GP || gid == GID_RZZ; }
+
+}  // namespace
+
+using namespace mqb;
+
+struct mqb_hamiltonian {
+    int n = 0, precision = 0;
+    std::vector<HamGroup> groups;
+    HamClass *d_classes = nullptr;
+    HamTerm *d_terms = nullptr;
+    ~mqb_hamiltonian() {
+        cudaFree(d_classes);
+        cudaFree(d_terms);
+    }
+};
+
+struct SchedDev {
+    Schedule s;
+    ~SchedDev() {
+        cudaFree(s.d_pass_ops);
+        cudaFree(s.d_slot_map);
+    }
+};
+
+struct mqb_program {
+    int n = 0, precision = 0, n_params = 0, fuse = 1, tile_bits = 0;
+    std::vector<DevOp> ops;
+    std::vector<mqb_gate_desc> descs;
+    DevOp *d_ops = nullptr;
+    mqb_gate_desc *d_descs = nullptr;
+    mqb_param_term *d_terms = nullptr;
+    void *d_cpool = nullptr;
+    int64_t per_sample = 0;    // complex entries per sample
+    int64_t custom_entries = 0;
+    int n_slots = 0;
+    int32_t *d_csr_ptr = nullptr, *d_csr_slot = nullptr;
+    double *d_csr_coeff = nullptr;
+    std::unique_ptr<SchedDev> apply_sched;
+    std::map<int, std::unique_ptr<SchedDev>> grad_sched;   // by number of Hamiltonians
+    ~mqb_program() {
+        cudaFree(d_ops);
+        cudaFree(d_descs);
+        cudaFree(d_terms);
+        cudaFree(d_cpool);
+        cudaFree(d_csr_ptr);
+        cudaFree(d_csr_slot);
+        cudaFree(d_csr_coeff);
+    }
+    size_t elem() const { return precision == MQB_PREC_C64 ? 8 : 16; }
+};
+
+static std::unique_ptr<SchedDev> make_sched(const mqb_program &p, int K, bool fuse) {
+    auto sd = std::make_unique<SchedDev>();
+    sd->s = build_schedule(p.n, K, contiguity_bits(p.precision), p.ops, fuse);
+    sd->s.d_pass_ops = upload(sd->s.pass_ops);
+    sd->s.d_slot_map = upload(sd->s.slot_map);
+    return sd;
+}
+
+static int grad_tile_bits(const mqb_program &p, int n_hams) {
+    if (p.tile_bits > 0) return std::min(p.tile_bits, default_tile_bits(p.precision, 1 + n_hams) + 1);
+    return default_tile_bits(p.precision, 1 + n_hams);
+}
+
+static SchedDev &grad_schedule(mqb_program &p, int n_hams) {
+    const bool fused = p.fuse && n_hams <= 4;
+    const int key = fused ? n_hams : 0;
+    auto it = p.grad_sched.find(key);
+    if (it != p.grad_sched.end()) return *it->second;
+    auto sd = make_sched(p, fused ? grad_tile_bits(p, n_hams) : p.n, fused);
+    SchedDev &ref = *sd;
+    p.grad_sched[key] = std::move(sd);
+    return ref;
+}
+
+template <typename R>
+static TileGeom pass_geom(int n, const Pass &ps) {
+    return make_geom(n, ps.qbits);
+}
+
+// ---------------------------------------------------------------------------------------------- execution
+template <typename R>
+static void run_forward_pass(const mqb_program &p, const Schedule &s, const Pass &ps, const cplx<R> *mats,
+                             const cplx<R> *src, int64_t src_stride, cplx<R> *dst, int64_t batch, cudaStream_t st) {
+    const int sm = sm_count_cached();
+    const cplx<R> *cpool = static_cast<const cplx<R> *>(p.d_cpool);
+    if (ps.fused) {
+        FwdArgs<R> a{};
+        a.g = make_geom(p.n, ps.qbits);
+        a.pops = s.d_pass_ops + ps.op_begin;
+        a.n_pops = ps.op_end - ps.op_begin;
+        a.ops = p.d_ops;
+        a.mats = mats;
+        a.mats_stride = p.per_sample;
+        a.cpool = cpool;
+        a.src = src;
+        a.dst = dst;
+        a.batch = batch;
+        a.src_batch_stride = src_stride;
+        ck(launch_fused_fwd<R>(a, sm, st), "fused forward pass");
+        return;
+    }
+    if (src != dst) ck(launch_copy_or_zero<R>(dst, src, p.n, batch, src_stride, st), "state copy");
+    ck(launch_plain_apply<R>(dst, p.n, batch, p.ops[ps.op_begin], mats, p.per_sample, cpool, false, sm, st),
+       "gate kernel");
+}
+
+template <typename R>
+static void run_matgen(const mqb_program &p, const double *params, int64_t param_stride, const double *custom,
+                       int64_t batch, cplx<R> *mats, cudaStream_t st) {
+    if (p.per_sample == 0) return;
+    MatgenArgs m{};
+    m.ops = p.d_ops;
+    m.descs = p.d_descs;
+    m.terms = p.d_terms;
+    m.n_ops = int(p.ops.size());
+    m.params = params;
+    m.param_stride = param_stride;
+    m.custom = custom;
+    m.custom_stride = p.custom_entries;
+    m.batch = batch;
+    m.mats = mats;
+    m.mats_stride = p.per_sample;
+    ck(launch_matgen<R>(m, st), "matgen");
+}
+
+template <typename R>
+static void apply_impl(mqb_program &p, void *states, int64_t batch, const double *params, int64_t param_stride,
+                       const double *custom, void *ws, size_t ws_bytes, cudaStream_t st) {
+    const size_t need = align_up(size_t(batch) * p.per_sample * sizeof(cplx<R>));
+    if (p.per_sample && (ws == nullptr || ws_bytes < need)) fail(MQB_ERR_WORKSPACE, "workspace too small");
+    cplx<R> *mats = static_cast<cplx<R> *>(ws);
+    run_matgen<R>(p, params, param_stride, custom, batch, mats, st);
+    cplx<R> *s = static_cast<cplx<R> *>(states);
+    const Schedule &sc = p.apply_sched->s;
+    for (const Pass &ps : sc.passes) run_forward_pass<R>(p, sc, ps, mats, s, int64_t(1) << p.n, s, batch, st);
+}
+
+// Hamiltonian passes: out = H ket (if out), f += <bra|H ket> (if fout)
+template <typename R>
+static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R> *ket, cplx<R> *out, double *fout,
+                     int64_t f_stride, int64_t batch, cudaStream_t st) {
+    const int sm = sm_count_cached();
+    const int64_t dim = int64_t(1) << h.n;
+    if (h.groups.empty()) {
+        // zero Hamiltonian
+        if (out) ck(cudaMemsetAsync(out, 0, sizeof(cplx<R>) * dim * batch, st), "memset");
+        return;
+    }
+    for (size_t gi = 0; gi < h.groups.size(); ++gi) {
+        const HamGroup &g = h.groups[gi];
+        HamArgs<R> a{};
+        a.g = g.geom;
+        a.classes = h.d_classes + g.class_begin;
+        a.n_classes = g.class_count;
+        a.terms = h.d_terms;
+        a.ket = ket;
+        a.bra = bra;
+        a.out = out;
+        a.accumulate = gi > 0;
+        a.fout = fout;
+        a.batch = batch;
+        a.out_batch_stride = dim;
+        a.f_stride = f_stride;
+        ck(launch_ham<R>(a, sm, st), "hamiltonian pass");
+    }
+}
+
+struct GradLayout {
+    size_t mats = 0, gslots = 0, lam = 0, w = 0, ckpt = 0, total = 0;
+    int n_ckpt = 0;
+    bool need_w = false;
+    std::vector<int> ckpt_index;   // p (1..P) -> checkpoint buffer index or -1
+};
+
+static GradLayout grad_layout(const mqb_program &p, const Schedule &s, int64_t batch, int n_hams, int stride) {
+    GradLayout L;
+    const int P = int(s.passes.size());
+    const size_t state = (size_t(1) << p.n) * p.elem() * batch;
+    L.ckpt_index.assign(P + 1, -1);
+    for (int q = 1; q <= P; ++q) {
+        const bool stored = (q == P) || (stride > 0 && q % stride == 0);
+        if (stored) L.ckpt_index[q] = L.n_ckpt++;
+        else L.need_w = true;
+    }
+    for (const Pass &ps : s.passes)
+        if (!ps.fused) L.need_w = true;
+    if (P == 0) L.need_w = true;
+    L.mats = align_up(size_t(batch) * p.per_sample * p.elem());
+    L.gslots = align_up(size_t(batch) * std::max(1, p.n_slots) * n_hams * sizeof(double));
+    L.lam = align_up(state * n_hams);
+    L.w = L.need_w ? align_up(state) : 0;
+    L.ckpt = align_up(state) * L.n_ckpt;
+    L.total = L.mats + L.gslots + L.lam + L.w + L.ckpt;
+    return L;
+}
+
+template <typename R>
+static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_hams, const void *init,
+                      int init_batched, int64_t batch, const double *params, int64_t param_stride, const double *custom,
+                      double *f, double *grad, int stride, void *ws, size_t ws_bytes, cudaStream_t st) {
+    using V = cplx<R>;
+    SchedDev &sd = grad_schedule(p, n_hams);
+    const Schedule &s = sd.s;
+    const GradLayout L = grad_layout(p, s, batch, n_hams, stride);
+    if (ws == nullptr || ws_bytes < L.total) fail(MQB_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, L.total);
+    unsigned char *base = static_cast<unsigned char *>(ws);
+    V *mats = reinterpret_cast<V *>(base);
+    double *gslots = reinterpret_cast<double *>(base + L.mats);
+    V *lam = reinterpret_cast<V *>(base + L.mats + L.gslots);
+    V *W = L.need_w ? reinterpret_cast<V *>(base + L.mats + L.gslots + L.lam) : nullptr;
+    unsigned char *ck0 = base + L.mats + L.gslots + L.lam + L.w;
+    const int64_t dim = int64_t(1) << p.n;
+    const size_t state_bytes = align_up(size_t(dim) * batch * sizeof(V));
+    auto ckpt = [&](int q) -> V * { return reinterpret_cast<V *>(ck0 + state_bytes * L.ckpt_index[q]); };
+    auto loc = [&](int q) -> V * { return L.ckpt_index[q] >= 0 ? ckpt(q) : W; };
+    const int P = int(s.passes.size());
+    const int sm = sm_count_cached();
+    const V *cpool = static_cast<const V *>(p.d_cpool);
+
+    ck(cudaMemsetAsync(gslots, 0, L.gslots, st), "memset");
+    ck(cudaMemsetAsync(f, 0, sizeof(double) * 2 * n_hams * batch, st), "memset");
+    run_matgen<R>(p, params, param_stride, custom, batch, mats, st);
+
+    // forward: psi_{q+1} = pass_q(psi_q), psi_0 = init (or |0...0>)
+    const V *init_v = static_cast<const V *>(init);
+    const int64_t init_stride = init_batched ? dim : 0;
+    for (int q = 0; q < P; ++q) {
+        const V *src = (q == 0) ? init_v : loc(q);
+        const int64_t sstr = (q == 0) ? init_stride : dim;
+        run_forward_pass<R>(p, s, s.passes[q], mats, src, sstr, loc(q + 1), batch, st);
+    }
+    V *psiP = W;
+    if (P > 0) {
+        psiP = loc(P);
+    } else {
+        ck(launch_copy_or_zero<R>(W, init_v, p.n, batch, init_stride, st), "state copy");
+    }
+    // lambda_h = H_h psi_P ; f_h = <psi_P|lambda_h>
+    for (int h = 0; h < n_hams; ++h)
+        ham_impl<R>(*hams[h], psiP, psiP, lam + h * batch * dim, f + 2 * h, 2 * n_hams, batch, st);
+    // backward
+    for (int q = P - 1; q >= 0; --q) {
+        const Pass &ps = s.passes[q];
+        const bool stored_q = L.ckpt_index[q] >= 0;
+        if (ps.fused) {
+            BwdArgs<R> a{};
+            a.g = make_geom(p.n, ps.qbits);
+            a.pops = s.d_pass_ops + ps.op_begin;
+            a.n_pops = ps.op_end - ps.op_begin;
+            a.ops = p.d_ops;
+            a.mats = mats;
+            a.mats_stride = p.per_sample;
+            a.cpool = cpool;
+            a.psi_src = loc(q + 1);
+            a.psi_dst = (q > 0 && !stored_q) ? W : nullptr;
+            a.lam = lam;
+            a.n_hams = n_hams;
+            a.gslots = gslots;
+            a.n_slots = std::max(1, p.n_slots);
+            a.slot_map = s.d_slot_map + ps.slot_begin;
+            a.n_local_slots = ps.n_slots;
+            a.batch = batch;
+            ck(launch_fused_bwd<R>(a, sm, st), "fused backward pass");
+        } else {
+            const DevOp &op = p.ops[ps.op_begin];
+            V *psi_q;
+            if (q > 0 && stored_q) {
+                psi_q = ckpt(q);
+            } else {
+                V *src = loc(q + 1);
+                if (src != W) ck(launch_copy_or_zero<R>(W, src, p.n, batch, dim, st), "state copy");
+                ck(launch_plain_apply<R>(W, p.n, batch, op, mats, p.per_sample, cpool, true, sm, st), "gate kernel");
+                psi_q = W;
+            }
+            ck(launch_plain_grad<R>(psi_q, lam, p.n, batch, n_hams, op, mats, p.per_sample, gslots,
+                                    std::max(1, p.n_slots), sm, st),
+               "gradient kernel");
+            for (int h = 0; h < n_hams; ++h)
+                ck(launch_plain_apply<R>(lam + h * batch * dim, p.n, batch, op, mats, p.per_sample, cpool, true, sm, st),
+                   "gate kernel");
+        }
+    }
+    ck(launch_grad_scatter(gslots, batch, std::max(1, p.n_slots), n_hams, p.d_csr_ptr, p.d_csr_slot, p.d_csr_coeff,
+                           p.n_params, grad, st),
+       "gradient scatter");
+}
+
+
+// Validate one gate record and derive its execution kind, targets and matrix size (no CUDA).
+static DevOp basic_op(const mqb_gate_desc &d, int k, int n_qubits, const mqb_param_term *terms, int n_terms,
+                      int n_params, const double *const_matrices, int64_t n_const_entries) {
+    DevOp op{};
+    op.gate_id = d.gate_id;
+    op.m = d.n_obj;
+    const uint64_t allq = (uint64_t(1) << n_qubits) - 1;
+    if (d.gate_id < 0 || d.gate_id >= GID_COUNT) fail(MQB_ERR_INVALID, "gate %d: unknown gate id %d", k, d.gate_id);
+    if (d.gate_id != GID_RPS && (d.n_obj < 1 || d.n_obj > MQB_MAX_OBJ))
+        fail(MQB_ERR_INVALID, "gate %d: %d object qubits (max %d)", k, d.n_obj, MQB_MAX_OBJ);
+    uint64_t objm = 0;
+    for (int i = 0; i < d.n_obj && i < MQB_MAX_OBJ; ++i) {
+        if (d.obj[i] < 0 || d.obj[i] >= n_qubits) fail(MQB_ERR_INVALID, "gate %d: qubit %d out of range", k, d.obj[i]);
+        if (objm >> d.obj[i] & 1) fail(MQB_ERR_INVALID, "gate %d: repeated object qubit %d", k, d.obj[i]);
+        objm |= uint64_t(1) << d.obj[i];
+        op.tq[i] = d.obj[i];
+    }
+    if (d.ctrl_mask & ~allq) fail(MQB_ERR_INVALID, "gate %d: control qubit out of range", k);
+    if (d.ctrl_mask & objm) fail(MQB_ERR_INVALID, "gate %d: control and object qubits overlap", k);
+    op.ctrl = d.ctrl_mask;
+    if (d.n_angles < 0 || d.n_angles > MQB_MAX_ANGLES) fail(MQB_ERR_INVALID, "gate %d: bad angle count", k);
+    op.n_angles = d.n_angles;
+    op.grad_mask = d.grad_angles & ((1 << d.n_angles) - 1);
+    if (terms) {
+        for (int a = 0; a < d.n_angles; ++a) {
+            if (d.term_begin[a] < 0 || d.term_count[a] < 0 || d.term_begin[a] + d.term_count[a] > n_terms)
+                fail(MQB_ERR_INVALID, "gate %d: bad parameter term range", k);
+            for (int t = d.term_begin[a]; t < d.term_begin[a] + d.term_count[a]; ++t)
+                if (terms[t].param < 0 || terms[t].param >= n_params)
+                    fail(MQB_ERR_INVALID, "gate %d: parameter index %d out of range", k, terms[t].param);
+        }
+    }
+    if (d.gate_id == GID_MATRIX) {
+        const int dimm = 1 << d.n_obj;
+        if (!const_matrices || d.matrix_offset < 0 || d.matrix_offset + int64_t(dimm) * dimm > n_const_entries)
+            fail(MQB_ERR_INVALID, "gate %d: constant matrix out of range", k);
+        const double *m = const_matrices + 2 * d.matrix_offset;
+        bool diag = true;
+        for (int r = 0; r < dimm && diag; ++r)
+            for (int c = 0; c < dimm; ++c)
+                if (r != c && (m[2 * (r * dimm + c)] != 0 || m[2 * (r * dimm + c) + 1] != 0)) {
+                    diag = false;
+                    break;
+                }
+        op.per_sample = 0;
+        op.n_angles = 0;
+        op.grad_mask = 0;
+        op.kind = diag ? KIND_DIAG : KIND_DENSE;
+        op.mat_size = diag ? dimm : dimm * dimm;
+        return op;
+    }
+    if (d.gate_id == GID_RPS) {
+        op.kind = KIND_RPS;
+        op.mat_size = 1;
+        op.px = d.pauli_x;
+        op.py = d.pauli_y;
+        op.pz = d.pauli_z;
+        op.pny = d.pauli_ny;
+        op.m = 0;
+        if ((d.pauli_x | d.pauli_y | d.pauli_z) & ~allq) fail(MQB_ERR_INVALID, "gate %d: Pauli mask out of range", k);
+        if ((d.pauli_x | d.pauli_y | d.pauli_z) & d.ctrl_mask)
+            fail(MQB_ERR_INVALID, "gate %d: control and object qubits overlap", k);
+        return op;
+    }
+    if (is_diag_gid(d.gate_id)) {
+        op.kind = KIND_DIAG;
+        op.mat_size = 1 << d.n_obj;
+    } else {
+        op.kind = KIND_DENSE;
+        op.mat_size = 1 << (2 * d.n_obj);
+    }
+    const int expect_obj =
+        (d.gate_id == GID_RZZ || (d.gate_id >= GID_RXX && d.gate_id <= GID_SWAPALPHA) || d.gate_id == GID_FSIM) ? 2 : 1;
+    if (d.gate_id != GID_CUSTOM && d.n_obj != expect_obj)
+        fail(MQB_ERR_INVALID, "gate %d: gate id %d acts on %d qubits, got %d", k, d.gate_id, expect_obj, d.n_obj);
+    return op;
+}
+
+// ---------------------------------------------------------------------------------------------- C ABI
+extern "C" {
+
+const char *mqb_last_error(void) { return g_last_error.c_str(); }
+
+int mqb_version(void) { return 100; }
+
+int mqb_device_sm_count(int *out) {
+    return guarded([&] { *out = sm_count_cached(); });
+}
+
+int mqb_abi_struct_sizes(int64_t *out, int n) {
+    return guarded([&] {
+        const int64_t v[4] = {int64_t(sizeof(mqb_gate_desc)), int64_t(sizeof(mqb_param_term)),
+                              int64_t(sizeof(mqb_program_options)), int64_t(sizeof(mqb_program_info))};
+        for (int i = 0; i < n && i < 4; ++i) out[i] = v[i];
+    });
+}
+
+int mqb_program_create(int n_qubits, int precision, const mqb_gate_desc *gates, int n_gates, const mqb_param_term *terms,
+                       int n_terms, int n_params, const double *const_matrices, int64_t n_const_entries,
+                       const mqb_program_options *options, mqb_program **out) {
+    return guarded([&] {
+        if (!out) fail(MQB_ERR_INVALID, "out is null");
+        *out = nullptr;
+        if (n_qubits < 1 || n_qubits > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40], got %d", n_qubits);
+        if (precision != MQB_PREC_C64 && precision != MQB_PREC_C128) fail(MQB_ERR_INVALID, "bad precision %d", precision);
+        if (n_gates < 0 || (n_gates > 0 && !gates)) fail(MQB_ERR_INVALID, "bad gate table");
+        auto p = std::make_unique<mqb_program>();
+        p->n = n_qubits;
+        p->precision = precision;
+        p->n_params = n_params;
+        p->fuse = options ? options->fuse : 1;
+        p->tile_bits = options ? options->tile_bits : 0;
+        p->descs.assign(gates, gates + n_gates);
+        std::vector<std::complex<double>> pool;
+        std::vector<std::vector<std::pair<int32_t, double>>> csr(std::max(0, n_params));
+        int64_t cursor = 0;
+        int slots = 0;
+        for (int k = 0; k < n_gates; ++k) {
+            const mqb_gate_desc &d = gates[k];
+            DevOp op = basic_op(d, k, n_qubits, terms, n_terms, n_params, const_matrices, n_const_entries);
+            if (d.gate_id == GID_MATRIX) {
+                const int dimm = 1 << d.n_obj;
+                const double *m = const_matrices + 2 * d.matrix_offset;
+                op.mat_off = int64_t(pool.size());
+                if (op.kind == KIND_DIAG) {
+                    for (int r = 0; r < dimm; ++r) pool.emplace_back(m[2 * (r * dimm + r)], m[2 * (r * dimm + r) + 1]);
+                } else {
+                    for (int e = 0; e < dimm * dimm; ++e) pool.emplace_back(m[2 * e], m[2 * e + 1]);
+                }
+            } else {
+                op.per_sample = 1;
+                op.mat_off = cursor;
+                cursor += op.mat_size;
+                if (op.grad_mask) {
+                    op.dmat_off = int32_t(cursor);
+                    cursor += int64_t(op.mat_size) * op.n_angles;
+                }
+                if (d.gate_id == GID_CUSTOM) {
+                    op.custom_off = int32_t(d.matrix_offset);
+                    p->custom_entries = std::max<int64_t>(p->custom_entries, d.matrix_offset + 2 * op.mat_size);
+                }
+            }
+            if (op.grad_mask) {
+                op.slot0 = slots;
+                int r = 0;
+                for (int a = 0; a < op.n_angles; ++a) {
+                    if (!(op.grad_mask >> a & 1)) continue;
+                    for (int t = d.term_begin[a]; t < d.term_begin[a] + d.term_count[a]; ++t)
+                        if (terms[t].flags & 1) csr[terms[t].param].emplace_back(slots + r, terms[t].coeff);
+                    ++r;
+                }
+                slots += r;
+            }
+            p->ops.push_back(op);
+        }
+        p->per_sample = cursor;
+        p->n_slots = slots;
+        p->d_ops = upload(p->ops);
+        p->d_descs = upload(p->descs);
+        p->d_terms = upload(std::vector<mqb_param_term>(terms, terms + n_terms));
+        if (!pool.empty()) {
+            if (precision == MQB_PREC_C64) {
+                std::vector<float2> v;
+                for (auto &c : pool) v.push_back(make_float2(float(c.real()), float(c.imag())));
+                p->d_cpool = upload(v);
+            } else {
+                std::vector<double2> v;
+                for (auto &c : pool) v.push_back(make_double2(c.real(), c.imag()));
+                p->d_cpool = upload(v);
+            }
+        }
+        std::vector<int32_t> ptr(std::max(0, n_params) + 1, 0), slot;
+        std::vector<double> coeff;
+        for (int q = 0; q < n_params; ++q) {
+            for (auto &e : csr[q]) {
+                slot.push_back(e.first);
+                coeff.push_back(e.second);
+            }
+            ptr[q + 1] = int32_t(slot.size());
+        }
+        p->d_csr_ptr = upload(ptr);
+        p->d_csr_slot = upload(slot);
+        p->d_csr_coeff = upload(coeff);
+        const int K = p->tile_bits > 0 ? p->tile_bits : default_tile_bits(precision, 1);
+        p->apply_sched = make_sched(*p, K, p->fuse != 0);
+        *out = p.release();
+    });
+}
+
+int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, int n_gates, const double *const_matrices,
+                      int64_t n_const_entries, int tile_bits, int fuse, int *n_passes, int32_t *order, int32_t *pass_of,
+                      uint64_t *qmask, int32_t *fused) {
+    return guarded([&] {
+        if (n_qubits < 1 || n_qubits > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
+        std::vector<DevOp> ops;
+        for (int k = 0; k < n_gates; ++k)
+            ops.push_back(basic_op(gates[k], k, n_qubits, nullptr, 0, 0, const_matrices, n_const_entries));
+        const int K = tile_bits > 0 ? tile_bits : default_tile_bits(precision, 1);
+        Schedule s = build_schedule(n_qubits, K, contiguity_bits(precision), ops, fuse != 0);
+        int pos = 0;
+        for (size_t pi = 0; pi < s.passes.size(); ++pi) {
+            const Pass &ps = s.passes[pi];
+            uint64_t qm = 0;
+            for (int q : ps.qbits) qm |= uint64_t(1) << q;
+            qmask[pi] = qm;
+            fused[pi] = ps.fused;
+            if (ps.fused) {
+                for (int i = ps.op_begin; i < ps.op_end; ++i) {
+                    order[pos] = s.pass_ops[i].op;
+                    pass_of[pos++] = int32_t(pi);
+                }
+            } else {
+                order[pos] = ps.op_begin;
+                pass_of[pos++] = int32_t(pi);
+            }
+        }
+        *n_passes = int(s.passes.size());
+    });
+}
+
+int mqb_program_destroy(mqb_program *prog) {
+    return guarded([&] { delete prog; });
+}
+
+int mqb_program_get_info(const mqb_program *p, mqb_program_info *info) {
+    return guarded([&] {
+        if (!p || !info) fail(MQB_ERR_INVALID, "null argument");
+        std::memset(info, 0, sizeof(*info));
+        info->n_qubits = p->n;
+        info->precision = p->precision;
+        info->n_ops = int(p->ops.size());
+        info->n_params = p->n_params;
+        info->n_passes = int(p->apply_sched->s.passes.size());
+        info->tile_bits = p->apply_sched->s.K;
+        info->n_grad_slots = p->n_slots;
+        info->per_sample_entries = int32_t(p->per_sample);
+        info->custom_entries = int32_t(p->custom_entries);
+    });
+}
+
+int mqb_program_grad_passes(mqb_program *p, int n_hams, int *n_passes, int *tile_bits) {
+    return guarded([&] {
+        SchedDev &sd = grad_schedule(*p, n_hams);
+        *n_passes = int(sd.s.passes.size());
+        *tile_bits = sd.s.K;
+    });
+}
+
+int mqb_apply_workspace_size(const mqb_program *p, int64_t batch, size_t *bytes) {
+    return guarded([&] { *bytes = std::max<size_t>(256, align_up(size_t(batch) * p->per_sample * p->elem())); });
+}
+
+int mqb_apply(mqb_program *p, void *states, int64_t batch, const double *params, int64_t param_stride,
+              const double *custom, void *ws, size_t ws_bytes, void *stream) {
+    return guarded([&] {
+        if (!p || !states) fail(MQB_ERR_INVALID, "null argument");
+        if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
+        if (p->per_sample && !params && p->n_params) fail(MQB_ERR_INVALID, "parameters required");
+        if (p->custom_entries && !custom) fail(MQB_ERR_INVALID, "custom gate matrices required");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (p->precision == MQB_PREC_C64)
+            apply_impl<float>(*p, states, batch, params, param_stride, custom, ws, ws_bytes, st);
+        else
+            apply_impl<double>(*p, states, batch, params, param_stride, custom, ws, ws_bytes, st);
+    });
+}
+
+int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const uint64_t *mask_y, const uint64_t *mask_z,
+                   const int32_t *num_y, const double *coeff, int n_terms, mqb_hamiltonian **out) {
+    return guarded([&] {
+        if (!out) fail(MQB_ERR_INVALID, "out is null");
+        *out = nullptr;
+        if (n_qubits < 1 || n_qubits > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
+        const uint64_t allq = (uint64_t(1) << n_qubits) - 1;
+        std::vector<uint64_t> mx, my, mz;
+        std::vector<int> ny;
+        std::vector<double> cf;
+        for (int t = 0; t < n_terms; ++t) {
+            if ((mask_x[t] | mask_y[t] | mask_z[t]) & ~allq) fail(MQB_ERR_INVALID, "term %d acts outside the register", t);
+            if ((mask_x[t] & mask_y[t]) || (mask_x[t] & mask_z[t]) || (mask_y[t] & mask_z[t]))
+                fail(MQB_ERR_INVALID, "term %d has overlapping Pauli masks", t);
+            if (coeff[t] == 0) continue;
+            mx.push_back(mask_x[t]);
+            my.push_back(mask_y[t]);
+            mz.push_back(mask_z[t]);
+            ny.push_back(num_y[t]);
+            cf.push_back(coeff[t]);
+        }
+        auto h = std::make_unique<mqb_hamiltonian>();
+        h->n = n_qubits;
+        h->precision = precision;
+        std::vector<HamClass> classes;
+        std::vector<HamTerm> hterms;
+        build_ham_groups(n_qubits, default_tile_bits(precision, 1), contiguity_bits(precision), mx, my, mz, ny, cf,
+                         h->groups, classes, hterms);
+        h->d_classes = upload(classes);
+        h->d_terms = upload(hterms);
+        *out = h.release();
+    });
+}
+
+int mqb_ham_destroy(mqb_hamiltonian *h) {
+    return guarded([&] { delete h; });
+}
+
+int mqb_apply_hamiltonian(const mqb_hamiltonian *h, const void *in, void *out, int64_t batch, void *stream) {
+    return guarded([&] {
+        if (!h || !in || !out) fail(MQB_ERR_INVALID, "null argument");
+        if (in == out) fail(MQB_ERR_INVALID, "in and out must be different buffers");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (h->precision == MQB_PREC_C64)
+            ham_impl<float>(*h, nullptr, static_cast<const float2 *>(in), static_cast<float2 *>(out), nullptr, 2, batch, st);
+        else
+            ham_impl<double>(*h, nullptr, static_cast<const double2 *>(in), static_cast<double2 *>(out), nullptr, 2, batch,
+                             st);
+    });
+}
+
+int mqb_expectation(const mqb_hamiltonian *h, const void *bra, const void *ket, int64_t batch, double *out, void *stream) {
+    return guarded([&] {
+        if (!h || !bra || !ket || !out) fail(MQB_ERR_INVALID, "null argument");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        ck(cudaMemsetAsync(out, 0, sizeof(double) * 2 * batch, st), "memset");
+        if (h->precision == MQB_PREC_C64)
+            ham_impl<float>(*h, static_cast<const float2 *>(bra), static_cast<const float2 *>(ket), nullptr, out, 2, batch, st);
+        else
+            ham_impl<double>(*h, static_cast<const double2 *>(bra), static_cast<const double2 *>(ket), nullptr, out, 2,
+                             batch, st);
+    });
+}
+
+int mqb_vdot(int n, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream) {
+    return guarded([&] {
+        if (!a || !b || !out) fail(MQB_ERR_INVALID, "null argument");
+        const int sm = sm_count_cached();
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (precision == MQB_PREC_C64)
+            ck(launch_vdot<float>(static_cast<const float2 *>(a), static_cast<const float2 *>(b), n, batch, out, sm, st), "vdot");
+        else
+            ck(launch_vdot<double>(static_cast<const double2 *>(a), static_cast<const double2 *>(b), n, batch, out, sm, st),
+               "vdot");
+    });
+}
+
+int mqb_grad_workspace_size(const mqb_program *p, int64_t batch, int n_hams, int stride, size_t *bytes) {
+    return guarded([&] {
+        if (n_hams < 1) fail(MQB_ERR_INVALID, "need at least one Hamiltonian");
+        SchedDev &sd = grad_schedule(const_cast<mqb_program &>(*p), n_hams);
+        *bytes = grad_layout(*p, sd.s, batch, n_hams, stride).total;
+    });
+}
+
+int mqb_expectation_with_grad(mqb_program *p, const mqb_hamiltonian *const *hams, int n_hams, const void *init,
+                              int init_batched, int64_t batch, const double *params, int64_t param_stride,
+                              const double *custom, double *f, double *grad, int stride, void *ws, size_t ws_bytes,
+                              void *stream) {
+    return guarded([&] {
+        if (!p || !hams || !f || !grad) fail(MQB_ERR_INVALID, "null argument");
+        if (n_hams < 1) fail(MQB_ERR_INVALID, "need at least one Hamiltonian");
+        if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
+        for (int h = 0; h < n_hams; ++h) {
+            if (!hams[h]) fail(MQB_ERR_INVALID, "Hamiltonian %d is null", h);
+            if (hams[h]->n != p->n || hams[h]->precision != p->precision)
+                fail(MQB_ERR_INVALID, "Hamiltonian %d does not match the program's qubits / precision", h);
+        }
+        if (p->custom_entries && !custom) fail(MQB_ERR_INVALID, "custom gate matrices required");
+        if (batch > 65535 / 12) fail(MQB_ERR_INVALID, "batch too large for one call");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (p->precision == MQB_PREC_C64)
+            grad_impl<float>(*p, hams, n_hams, init, init_batched, batch, params, param_stride, custom, f, grad, stride, ws,
+                             ws_bytes, st);
+        else
+            grad_impl<double>(*p, hams, n_hams, init, init_batched, batch, params, param_stride, custom, f, grad, stride, ws,
+                              ws_bytes, st);
+    });
+}
+
+int mqb_sample_scratch_size(int n, size_t *bytes) {
+    return guarded([&] {
+        const int cb = std::min(n, 12);
+        *bytes = sizeof(double) * ((size_t(1) << (n - cb)) + 1);
+    });
+}
+
+int mqb_sample_indices(int n, int precision, const void *state, const double *u, int64_t shots, int64_t *out,
+                       void *scratch, size_t scratch_bytes, void *stream) {
+    return guarded([&] {
+        const int cb = std::min(n, 12);
+        const size_t need = sizeof(double) * ((size_t(1) << (n - cb)) + 1);
+        if (!scratch || scratch_bytes < need) fail(MQB_ERR_WORKSPACE, "scratch too small");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        double *sums = static_cast<double *>(scratch);
+        const int64_t nch = int64_t(1) << (n - cb);
+        if (precision == MQB_PREC_C64) {
+            ck(launch_chunk_probs<float>(static_cast<const float2 *>(state), n, cb, sums, st), "chunk probs");
+            ck(launch_prefix(sums, nch, st), "prefix");
+            ck(launch_sample_search<float>(static_cast<const float2 *>(state), n, cb, sums, u, shots, out, st), "search");
+        } else {
+            ck(launch_chunk_probs<double>(static_cast<const double2 *>(state), n, cb, sums, st), "chunk probs");
+            ck(launch_prefix(sums, nch, st), "prefix");
+            ck(launch_sample_search<double>(static_cast<const double2 *>(state), n, cb, sums, u, shots, out, st), "search");
+        }
+    });
+}
+
+int mqb_qubit_one_probability(int n, int precision, const void *state, int q, double *out, void *stream) {
+    return guarded([&] {
+        if (q < 0 || q >= n) fail(MQB_ERR_INVALID, "qubit out of range");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (precision == MQB_PREC_C64)
+            ck(launch_one_prob<float>(static_cast<const float2 *>(state), n, q, out, st), "probability");
+        else
+            ck(launch_one_prob<double>(static_cast<const double2 *>(state), n, q, out, st), "probability");
+    });
+}
+
+int mqb_collapse(int n, int precision, void *state, int q, int outcome, double scale, void *stream) {
+    return guarded([&] {
+        if (q < 0 || q >= n) fail(MQB_ERR_INVALID, "qubit out of range");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (precision == MQB_PREC_C64)
+            ck(launch_collapse<float>(static_cast<float2 *>(state), n, q, outcome, scale, st), "collapse");
+        else
+            ck(launch_collapse<double>(static_cast<double2 *>(state), n, q, outcome, scale, st), "collapse");
+    });
+}
+
+}  // extern "C"

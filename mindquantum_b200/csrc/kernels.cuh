@@ -1,0 +1,128 @@
+// Kernel argument structures and launch wrappers of the mqb200 engine.
+#ifndef MQB_KERNELS_CUH_
+#define MQB_KERNELS_CUH_
+
+#include "mqb_internal.h"
+
+namespace mqb {
+
+template <typename R>
+struct CT;
+template <>
+struct CT<float> {
+    using T = float2;
+};
+template <>
+struct CT<double> {
+    using T = double2;
+};
+template <typename R>
+using cplx = typename CT<R>::T;
+
+struct MatgenArgs {
+    const DevOp *ops;
+    const mqb_gate_desc *descs;
+    const mqb_param_term *terms;
+    int n_ops;
+    const double *params;
+    int64_t param_stride;
+    const double *custom;      // interleaved complex128, per sample
+    int64_t custom_stride;     // complex entries per sample
+    int64_t batch;
+    void *mats;                // per-sample matrices (cplx<R>)
+    int64_t mats_stride;       // complex entries per sample
+};
+
+template <typename R>
+struct FwdArgs {
+    TileGeom g;
+    const PassOp *pops;
+    int n_pops;
+    const DevOp *ops;
+    const cplx<R> *mats;
+    int64_t mats_stride;
+    const cplx<R> *cpool;
+    const cplx<R> *src;        // nullptr: start from |0...0>
+    cplx<R> *dst;
+    int64_t batch;
+    int64_t src_batch_stride;  // 0: every sample starts from the same state
+};
+
+template <typename R>
+struct BwdArgs {
+    TileGeom g;
+    const PassOp *pops;
+    int n_pops;
+    const DevOp *ops;
+    const cplx<R> *mats;
+    int64_t mats_stride;
+    const cplx<R> *cpool;
+    const cplx<R> *psi_src;    // state after the pass
+    cplx<R> *psi_dst;          // where to store the state before the pass (nullptr: not needed)
+    cplx<R> *lam;              // [n_hams][batch][dim]
+    int n_hams;
+    double *gslots;            // [batch][n_slots][n_hams]
+    int n_slots;
+    const int32_t *slot_map;   // pass-local slot -> global slot
+    int n_local_slots;
+    int64_t batch;
+};
+
+template <typename R>
+struct HamArgs {
+    TileGeom g;
+    const HamClass *classes;
+    int n_classes;
+    const HamTerm *terms;
+    const cplx<R> *ket;
+    const cplx<R> *bra;        // used for the expectation accumulation
+    cplx<R> *out;              // nullptr: expectation only
+    int accumulate;            // out += H ket (else out = H ket)
+    double *fout;              // [batch][2] (re, im) accumulators, may be nullptr
+    int64_t batch;
+    int64_t out_batch_stride;
+    int64_t f_stride;          // doubles between samples in fout
+};
+
+// launch wrappers (kernels.cu); all return cudaError_t of the launch
+template <typename R>
+cudaError_t launch_matgen(const MatgenArgs &a, cudaStream_t s);
+template <typename R>
+cudaError_t launch_fused_fwd(const FwdArgs<R> &a, int sm_count, cudaStream_t s);
+template <typename R>
+cudaError_t launch_fused_bwd(const BwdArgs<R> &a, int sm_count, cudaStream_t s);
+template <typename R>
+cudaError_t launch_ham(const HamArgs<R> &a, int sm_count, cudaStream_t s);
+template <typename R>
+cudaError_t launch_plain_apply(cplx<R> *st, int n, int64_t batch, const DevOp &op, const cplx<R> *mats,
+                               int64_t mats_stride, const cplx<R> *cpool, bool adjoint, int sm_count, cudaStream_t s);
+template <typename R>
+cudaError_t launch_plain_grad(const cplx<R> *psi, const cplx<R> *lam, int n, int64_t batch, int n_hams,
+                              const DevOp &op, const cplx<R> *mats, int64_t mats_stride, double *gslots,
+                              int n_slots, int sm_count, cudaStream_t s);
+template <typename R>
+cudaError_t launch_vdot(const cplx<R> *a, const cplx<R> *b, int n, int64_t batch, double *out, int sm_count,
+                        cudaStream_t s);
+template <typename R>
+cudaError_t launch_copy_or_zero(cplx<R> *dst, const cplx<R> *src, int n, int64_t batch, int64_t src_stride,
+                                cudaStream_t s);
+cudaError_t launch_grad_scatter(const double *gslots, int64_t batch, int n_slots, int n_hams, const int32_t *csr_ptr,
+                                const int32_t *csr_slot, const double *csr_coeff, int n_params, double *grad,
+                                cudaStream_t s);
+template <typename R>
+cudaError_t launch_chunk_probs(const cplx<R> *st, int n, int chunk_bits, double *sums, cudaStream_t s);
+cudaError_t launch_prefix(double *sums, int64_t n, cudaStream_t s);
+template <typename R>
+cudaError_t launch_sample_search(const cplx<R> *st, int n, int chunk_bits, const double *prefix,
+                                 const double *u, int64_t shots, int64_t *out, cudaStream_t s);
+template <typename R>
+cudaError_t launch_one_prob(const cplx<R> *st, int n, int q, double *out, cudaStream_t s);
+template <typename R>
+cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale, cudaStream_t s);
+
+size_t fused_fwd_smem(const TileGeom &g, int n_pops, int elem_bytes);
+size_t fused_bwd_smem(const TileGeom &g, int n_pops, int n_hams, int n_local_slots, int elem_bytes);
+size_t ham_smem(const TileGeom &g, int elem_bytes);
+
+}  // namespace mqb
+#endif

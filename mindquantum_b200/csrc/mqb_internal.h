@@ -1,0 +1,119 @@
+// Internal data structures of the mqb200 engine: the lowered op table, the pass schedule
+// produced by the host scheduler, and the launch interfaces of the CUDA kernels.
+#ifndef MQB_INTERNAL_H_
+#define MQB_INTERNAL_H_
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mqb200.h"
+#include "mqb_gate_ids.h"
+
+namespace mqb {
+
+constexpr int kMaxFusedM = 3;        // dense gates with <= 3 targets run inside fused tiles
+constexpr int kMaxTileBits = 14;     // upper bound of the tile size 2^K
+constexpr int kMaxPassOps = 256;     // ops of one fused pass (staged in shared memory)
+constexpr int kMaxPassSlots = 96;    // gradient slots of one fused pass (accumulated in shared memory)
+constexpr int kMaxGroupClasses = 64; // flip classes of one Hamiltonian pass
+constexpr int kMaxClassTerms = 64;   // Pauli terms of one flip class
+constexpr int kThreads = 256;        // threads of the tile kernels
+
+enum OpKind : int32_t { KIND_DENSE = 0, KIND_DIAG = 1, KIND_RPS = 2 };
+
+// One lowered gate in execution order.
+struct DevOp {
+    int32_t kind;
+    int32_t m;                   // number of target qubits
+    int32_t tq[MQB_MAX_OBJ];     // global target qubits; tq[b] is matrix index bit b
+    uint64_t ctrl;               // global control mask
+    int32_t gate_id;
+    int32_t per_sample;          // 1: matrices live in the per-sample block
+    int64_t mat_off;             // complex entries: const pool offset or per-sample offset of M
+    int32_t n_angles;
+    int32_t grad_mask;           // bit a: angle a has a gradient
+    int32_t slot0;               // gradient slot of the first gradient angle (consecutive)
+    int32_t dmat_off;            // per-sample offset of dM_0; dM_a = dmat_off + a * mat_size
+    int32_t mat_size;            // complex entries of one matrix (4^m dense, 2^m diagonal, 1 RPS)
+    int32_t custom_off;          // GID_CUSTOM: offset of M in the caller's per-sample custom block
+    uint64_t px, py, pz;         // GID_RPS masks
+    int32_t pny;
+    int32_t pad;
+};
+
+// An op as seen inside one fused pass (targets remapped to tile-local bits).
+struct PassOp {
+    int32_t op;        // program op index
+    int32_t kind;
+    int32_t m;
+    int32_t lt[kMaxFusedM];   // local target bit (dense: always >= 0; diag: -1 when outside the tile)
+    int32_t gt[kMaxFusedM];   // global target qubit
+    uint32_t lctrl;           // control bits inside the tile (local mask)
+    int32_t lslot;            // pass-local gradient slot of the first gradient angle (-1: none)
+    uint64_t octrl;           // control bits outside the tile (global mask)
+};
+
+// A pass: one sweep over the state(s).
+struct Pass {
+    int fused = 1;                 // 1: fused tile pass over ops [op_begin, op_end) of pass_ops; 0: single op
+    int K = 0;                     // tile bits
+    int c = 0;                     // contiguity bits (low qubits always in the tile)
+    std::vector<int> qbits;        // local bit -> global qubit (ascending)
+    std::vector<int> outside;      // global qubits not in the tile (ascending)
+    int op_begin = 0, op_end = 0;  // fused: range in Schedule::pass_ops; single: op index in op_begin
+    int prog_op_begin = 0, prog_op_end = 0;  // program ops covered (execution order)
+    int slot_begin = 0, n_slots = 0;         // fused: range in Schedule::slot_map (pass-local gradient slots)
+};
+
+struct Schedule {
+    int K = 0;
+    std::vector<Pass> passes;
+    std::vector<PassOp> pass_ops;
+    std::vector<int32_t> slot_map;  // pass-local slot -> global gradient slot
+    PassOp *d_pass_ops = nullptr;   // device copies
+    int32_t *d_slot_map = nullptr;
+};
+
+// Kernel-facing description of a fused pass (passed by value).
+struct TileGeom {
+    int32_t n;          // qubits
+    int32_t K;          // tile bits
+    int32_t c;          // contiguity bits
+    int32_t n_out;      // outside bits
+    int8_t qbits[kMaxTileBits];
+    int8_t outside[64];
+};
+
+// Hamiltonian: terms grouped into passes; every group's flip masks fit in one tile.
+struct HamTerm {
+    double coeff;
+    uint64_t my_mz;     // mask_y | mask_z (global), phase sign bits
+    int32_t ny;
+    int32_t pad;
+};
+struct HamClass {       // terms sharing one flip mask
+    uint64_t flip;      // global flip mask (mask_x | mask_y)
+    uint32_t lflip;     // the same mask on the group's tile-local bits
+    int32_t term_begin, term_count;
+    int32_t pad;
+};
+struct HamGroup {
+    TileGeom geom;
+    int class_begin, class_count;
+};
+
+// Builders (scheduler.cpp)
+Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool fuse);
+void build_ham_groups(int n, int K, int c, const std::vector<uint64_t> &mx, const std::vector<uint64_t> &my,
+                      const std::vector<uint64_t> &mz, const std::vector<int> &ny, const std::vector<double> &coeff,
+                      std::vector<HamGroup> &groups, std::vector<HamClass> &classes, std::vector<HamTerm> &terms);
+TileGeom make_geom(int n, const std::vector<int> &qbits);
+int contiguity_bits(int precision);
+int default_tile_bits(int precision, int n_states_in_tile);
+
+}  // namespace mqb
+
+#endif

@@ -1,0 +1,267 @@
+// Host-side pass scheduler.
+//
+// The reference applies every gate as its own sweep over the state
+// (VectorState::ApplyCircuit, ccsrc/include/simulator/vector/vector_state.tpp:949-960).  Here a
+// circuit is cut into passes: a fused pass owns a set Q of K "tile" qubits (always including
+// the lowest c qubits, so every tile is made of 128-byte contiguous runs) and applies, in one
+// read + write of the state, every gate whose non-diagonal targets lie in Q.  Diagonal gates
+// and control qubits may sit anywhere: outside Q their bits are constant over a tile.
+//
+// The greedy scan keeps the circuit's order of non-commuting gates: a gate that cannot join
+// the current pass blocks all its qubits for the rest of the scan, so no later gate sharing a
+// qubit with it can overtake it.
+#include <algorithm>
+#include <stdexcept>
+
+#include "mqb_internal.h"
+
+namespace mqb {
+
+static inline int popc(uint64_t x) { return __builtin_popcountll(x); }
+
+int contiguity_bits(int precision) { return precision == MQB_PREC_C64 ? 4 : 3; }
+
+int default_tile_bits(int precision, int n_states_in_tile) {
+    // keep the shared-memory tiles of all states at <= 64 KB so 2-3 blocks fit per SM
+    const size_t amp = precision == MQB_PREC_C64 ? 8 : 16;
+    int K = kMaxTileBits;
+    while (K > 6 && (size_t(n_states_in_tile) << K) * amp > 65536) --K;
+    return K;
+}
+
+TileGeom make_geom(int n, const std::vector<int> &qbits) {
+    TileGeom g{};
+    g.n = n;
+    g.K = int(qbits.size());
+    g.c = 0;
+    while (g.c < g.K && qbits[g.c] == g.c) ++g.c;
+    uint64_t qm = 0;
+    for (int i = 0; i < g.K; ++i) {
+        g.qbits[i] = int8_t(qbits[i]);
+        qm |= uint64_t(1) << qbits[i];
+    }
+    g.n_out = 0;
+    for (int q = 0; q < n; ++q)
+        if (!(qm >> q & 1)) g.outside[g.n_out++] = int8_t(q);
+    return g;
+}
+
+static uint64_t dense_targets(const DevOp &op) {
+    if (op.kind != KIND_DENSE) return 0;
+    uint64_t m = 0;
+    for (int k = 0; k < op.m; ++k) m |= uint64_t(1) << op.tq[k];
+    return m;
+}
+
+static uint64_t touched(const DevOp &op) {
+    uint64_t m = op.ctrl;
+    for (int k = 0; k < op.m; ++k) m |= uint64_t(1) << op.tq[k];
+    if (op.kind == KIND_RPS) m |= op.px | op.py | op.pz;
+    return m;
+}
+
+static bool fusable(const DevOp &op) { return (op.kind == KIND_DENSE || op.kind == KIND_DIAG) && op.m <= kMaxFusedM; }
+
+Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool fuse) {
+    Schedule s;
+    if (K > n) K = n;
+    // leave room for the widest fused gate next to the contiguity bits; keep at least one
+    // contiguity bit so 16-byte vector accesses never straddle two tile runs
+    if (c > K - kMaxFusedM) c = std::max(1, K - kMaxFusedM);
+    if (n > K && K < kMaxFusedM + 1) fuse = false;
+    s.K = K;
+    const int L = int(ops.size());
+    std::vector<char> done(L, 0);
+    int n_done = 0;
+    int first = 0;
+    const uint64_t all = n >= 64 ? ~uint64_t(0) : ((uint64_t(1) << n) - 1);
+    while (n_done < L) {
+        while (first < L && done[first]) ++first;
+        if (!fuse || !fusable(ops[first])) {
+            Pass p;
+            p.fused = 0;
+            p.op_begin = first;
+            p.op_end = first + 1;
+            p.prog_op_begin = first;
+            p.prog_op_end = first + 1;
+            s.passes.push_back(p);
+            done[first] = 1;
+            ++n_done;
+            continue;
+        }
+        uint64_t Q = (n <= K) ? all : ((uint64_t(1) << c) - 1);
+        uint64_t blocked = 0;
+        std::vector<int> members;
+        int n_slots = 0;
+        for (int i = first; i < L && int(members.size()) < kMaxPassOps; ++i) {
+            if (done[i]) continue;
+            const DevOp &op = ops[i];
+            const uint64_t t = touched(op);
+            if (t & blocked) {
+                blocked |= t;
+                if ((blocked & all) == all) break;
+                continue;
+            }
+            if (!fusable(op)) {
+                blocked |= t;
+                continue;
+            }
+            const uint64_t need = dense_targets(op) & ~Q;
+            const int op_slots = popc(uint64_t(op.grad_mask));
+            if (popc(Q | need) <= K && n_slots + op_slots <= kMaxPassSlots) {
+                Q |= need;
+                n_slots += op_slots;
+                members.push_back(i);
+            } else {
+                blocked |= t;
+            }
+        }
+        if (members.empty()) {
+            // the first gate does not fit next to the contiguity bits: run it on its own
+            Pass p;
+            p.fused = 0;
+            p.op_begin = first;
+            p.op_end = first + 1;
+            p.prog_op_begin = first;
+            p.prog_op_end = first + 1;
+            s.passes.push_back(p);
+            done[first] = 1;
+            ++n_done;
+            continue;
+        }
+        // pad the tile to exactly K qubits with the lowest free qubits
+        for (int q = 0; q < n && popc(Q) < K; ++q) Q |= uint64_t(1) << q;
+        Pass p;
+        p.fused = 1;
+        p.K = K;
+        for (int q = 0; q < n; ++q) {
+            if (Q >> q & 1)
+                p.qbits.push_back(q);
+            else
+                p.outside.push_back(q);
+        }
+        p.c = 0;
+        while (p.c < K && p.qbits[p.c] == p.c) ++p.c;
+        int local[64];
+        for (int i = 0; i < 64; ++i) local[i] = -1;
+        for (int i = 0; i < K; ++i) local[p.qbits[i]] = i;
+        p.op_begin = int(s.pass_ops.size());
+        p.slot_begin = int(s.slot_map.size());
+        for (int i : members) {
+            const DevOp &op = ops[i];
+            PassOp po{};
+            po.op = i;
+            po.kind = op.kind;
+            po.m = op.m;
+            for (int k = 0; k < kMaxFusedM; ++k) {
+                po.lt[k] = -1;
+                po.gt[k] = 0;
+            }
+            for (int k = 0; k < op.m; ++k) {
+                po.gt[k] = op.tq[k];
+                po.lt[k] = local[op.tq[k]];
+                if (op.kind == KIND_DENSE && po.lt[k] < 0) throw std::logic_error("dense target outside tile");
+            }
+            po.lctrl = 0;
+            po.octrl = 0;
+            for (int q = 0; q < n; ++q) {
+                if (!(op.ctrl >> q & 1)) continue;
+                if (local[q] >= 0)
+                    po.lctrl |= 1u << local[q];
+                else
+                    po.octrl |= uint64_t(1) << q;
+            }
+            po.lslot = -1;
+            if (op.grad_mask) {
+                po.lslot = int(s.slot_map.size()) - p.slot_begin;
+                for (int a = 0, r = 0; a < op.n_angles; ++a)
+                    if (op.grad_mask >> a & 1) s.slot_map.push_back(op.slot0 + r++);
+            }
+            s.pass_ops.push_back(po);
+            done[i] = 1;
+            ++n_done;
+        }
+        p.op_end = int(s.pass_ops.size());
+        p.n_slots = int(s.slot_map.size()) - p.slot_begin;
+        p.prog_op_begin = members.empty() ? first : members.front();
+        p.prog_op_end = members.empty() ? first : members.back() + 1;
+        s.passes.push_back(p);
+    }
+    return s;
+}
+
+void build_ham_groups(int n, int K, int c, const std::vector<uint64_t> &mx, const std::vector<uint64_t> &my,
+                      const std::vector<uint64_t> &mz, const std::vector<int> &ny, const std::vector<double> &coeff,
+                      std::vector<HamGroup> &groups, std::vector<HamClass> &classes, std::vector<HamTerm> &terms) {
+    if (K > n) K = n;
+    if (c > K) c = K;
+    const int T = int(coeff.size());
+    // classes: distinct flip masks, in order of first appearance
+    std::vector<uint64_t> flips;
+    std::vector<std::vector<int>> members;
+    for (int t = 0; t < T; ++t) {
+        const uint64_t f = mx[t] | my[t];
+        auto it = std::find(flips.begin(), flips.end(), f);
+        if (it == flips.end()) {
+            flips.push_back(f);
+            members.push_back({t});
+        } else {
+            members[it - flips.begin()].push_back(t);
+        }
+    }
+    // split oversized classes
+    std::vector<uint64_t> cflip;
+    std::vector<std::vector<int>> cmem;
+    for (size_t i = 0; i < flips.size(); ++i) {
+        for (size_t s = 0; s < members[i].size(); s += kMaxClassTerms) {
+            cflip.push_back(flips[i]);
+            cmem.emplace_back(members[i].begin() + s,
+                              members[i].begin() + std::min(members[i].size(), s + size_t(kMaxClassTerms)));
+        }
+    }
+    const uint64_t all = n >= 64 ? ~uint64_t(0) : ((uint64_t(1) << n) - 1);
+    std::vector<char> used(cflip.size(), 0);
+    size_t n_used = 0;
+    while (n_used < cflip.size()) {
+        uint64_t Q = (n <= K) ? all : ((uint64_t(1) << c) - 1);
+        std::vector<int> in_group;
+        for (size_t i = 0; i < cflip.size() && int(in_group.size()) < kMaxGroupClasses; ++i) {
+            if (used[i]) continue;
+            if (popc(Q | cflip[i]) <= K) {
+                Q |= cflip[i];
+                in_group.push_back(int(i));
+                used[i] = 1;
+                ++n_used;
+            }
+        }
+        if (in_group.empty()) throw std::runtime_error("Pauli term acts on more qubits than a tile holds");
+        for (int q = 0; q < n && popc(Q) < K; ++q) Q |= uint64_t(1) << q;
+        std::vector<int> qb;
+        for (int q = 0; q < n; ++q)
+            if (Q >> q & 1) qb.push_back(q);
+        HamGroup g{};
+        g.geom = make_geom(n, qb);
+        g.class_begin = int(classes.size());
+        g.class_count = int(in_group.size());
+        for (int ci : in_group) {
+            HamClass hc{};
+            hc.flip = cflip[ci];
+            hc.lflip = 0;
+            for (int i = 0; i < g.geom.K; ++i)
+                if (hc.flip >> g.geom.qbits[i] & 1) hc.lflip |= 1u << i;
+            hc.term_begin = int(terms.size());
+            hc.term_count = int(cmem[ci].size());
+            for (int t : cmem[ci]) {
+                HamTerm ht{};
+                ht.coeff = coeff[t];
+                ht.my_mz = my[t] | mz[t];
+                ht.ny = ny[t];
+                terms.push_back(ht);
+            }
+            classes.push_back(hc);
+        }
+        groups.push_back(g);
+    }
+}
+
+}  // namespace mqb

@@ -1,0 +1,463 @@
+"""MQVectorB200: the B200 state-vector backend behind ``Simulator('mqvector_b200', n)``.
+
+It keeps the reference ``MQSim`` interface (mindquantum/simulator/mqsim.py:51-560): argument
+checks, the encoder/ansatz split of ``get_expectation_with_grad`` and the result layout
+``(f, g_enc, g_ans)`` with shapes ``[n_prs][n_hams]`` / ``[n_prs][n_hams][n_params]``.  The state
+is a torch tensor on the current CUDA device; all arithmetic runs in libmqb200 through its C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import warnings
+
+import numpy as np
+import torch
+
+from .. import _native as N
+from ..core import gates as G
+from ..core.circuit import Circuit
+from ..core.operators import Hamiltonian
+from ..core.parameterresolver import ParameterResolver, to_pr
+from ..dtype import complex64, complex128, to_mq_type
+from .backend_base import BackendBase
+from .lowering import lowered, native_ham
+from .measure_result import MeasureResult
+from .rng import Mt19937Uniform
+from .utils import GradOpsWrapper
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("the mqvector_b200 backend needs a CUDA device (B200, sm_100a); none is visible")
+
+
+class MQVectorB200(BackendBase):
+    """State-vector simulator on one B200.
+
+    Args:
+        name: backend name.
+        n_qubits: number of qubits.
+        seed: seed of the measurement random stream (std::mt19937 as in the reference).
+        dtype: ``complex128`` (default) or ``complex64``.
+        fuse: fused tile passes (default) or one kernel per gate.
+        device: CUDA device (default: the current one).
+    """
+
+    def __init__(self, name, n_qubits, seed=None, dtype=None, fuse=True, device=None):
+        _require_cuda()
+        super().__init__(name, n_qubits, seed, dtype)
+        if not isinstance(n_qubits, int) or n_qubits < 1:
+            raise ValueError(f"n_qubits should be a positive integer, but get {n_qubits}")
+        if seed is None:
+            seed = int(np.random.randint(1, 2**23))
+        self.seed = int(seed)
+        self.fuse = fuse
+        self.device = torch.device('cuda', torch.cuda.current_device()) if device is None else torch.device(device)
+        self._state = None          # None means |0...0>, like the reference's null state
+        self._rng = Mt19937Uniform(self.seed)
+        N.lib()
+
+    # ------------------------------------------------------------------ basics
+    @property
+    def precision(self):
+        return N.MQB_PREC_C64 if self.arithmetic_type == complex64 else N.MQB_PREC_C128
+
+    @property
+    def torch_dtype(self):
+        return torch.complex64 if self.arithmetic_type == complex64 else torch.complex128
+
+    @property
+    def dtype(self):
+        return self.arithmetic_type
+
+    def device_name(self):
+        return f"{self.n_qubits} qubits {self.name} simulator."
+
+    def _zero_state(self, batch=None):
+        shape = (1 << self.n_qubits,) if batch is None else (batch, 1 << self.n_qubits)
+        s = torch.zeros(shape, dtype=self.torch_dtype, device=self.device)
+        s[..., 0] = 1
+        return s
+
+    @property
+    def state(self):
+        """The state as a device tensor (allocated on first use)."""
+        if self._state is None:
+            self._state = self._zero_state()
+        return self._state
+
+    def reset(self):
+        self._state = None
+
+    def copy(self):
+        sim = MQVectorB200(self.name, self.n_qubits, self.seed, self.arithmetic_type, self.fuse, self.device)
+        if self._state is not None:
+            sim._state = self._state.clone()
+        return sim
+
+    def astype(self, dtype, seed=None):
+        sim = MQVectorB200(self.name, self.n_qubits, self.seed if seed is None else seed, dtype, self.fuse, self.device)
+        if self._state is not None:
+            sim._state = self._state.to(sim.torch_dtype)
+        return sim
+
+    def get_qs(self, ket=False):
+        qs = self.state.detach().to(torch.complex128).cpu().numpy()
+        if ket:
+            return '\n'.join(f"{v}¦{format(i, f'0{self.n_qubits}b')}⟩" for i, v in enumerate(qs) if abs(v) > 1e-12)
+        return qs
+
+    def set_qs(self, quantum_state):
+        """Set the state; the vector is normalised first (mqsim.py:538-544)."""
+        v = np.asarray(quantum_state)
+        if v.ndim != 1:
+            raise ValueError(f"vec requires a 1-dimensional array, but get {v.shape}")
+        n = np.log2(v.shape[0])
+        if n % 1 != 0:
+            raise ValueError(f"vec size {v.shape[0]} is not power of 2")
+        if int(n) != self.n_qubits:
+            raise ValueError(f"{int(n)} qubits vec does not match with simulation qubits ({self.n_qubits})")
+        norm = np.sqrt(np.sum(np.abs(v) ** 2))
+        if norm == 0.0:
+            raise ValueError("Wrong quantum state.")
+        self._state = torch.as_tensor(v / norm, dtype=self.torch_dtype).to(self.device)
+
+    def set_state_tensor(self, t):
+        """Set the state from a device tensor without normalising (zero-copy when dtype/device match)."""
+        if t.shape != (1 << self.n_qubits,):
+            raise ValueError(f"state must have shape ({1 << self.n_qubits},)")
+        self._state = t.to(device=self.device, dtype=self.torch_dtype).contiguous()
+
+    # ------------------------------------------------------------------ gate application
+    def _params_tensor(self, prog, pr):
+        names = prog.param_names
+        if not names:
+            return torch.zeros((1, 1), dtype=torch.float64, device=self.device), np.zeros((1, 0))
+        vals = np.array([[float(np.real(pr[k])) for k in names]], dtype=np.float64)
+        return torch.as_tensor(vals, device=self.device), vals
+
+    def _custom_tensor(self, prog, params_np):
+        blk = prog.custom_block(params_np)
+        if blk is None:
+            return None
+        return torch.as_tensor(np.ascontiguousarray(blk).view(np.float64), device=self.device)
+
+    def _apply_segment(self, states, circuit, pr, batch=1):
+        """Apply a measurement-free circuit in place to ``states`` ([batch][2^n])."""
+        names = circuit.params_name
+        prog = lowered(circuit, self.n_qubits, self.precision, names, None, self.fuse)
+        if prog.n_gates == 0:
+            return
+        params, params_np = self._params_tensor(prog, pr)
+        custom = self._custom_tensor(prog, params_np)
+        ws_bytes = ctypes.c_size_t()
+        N.call('mqb_apply_workspace_size', prog.handle, batch, ctypes.byref(ws_bytes))
+        ws = torch.empty(ws_bytes.value, dtype=torch.uint8, device=self.device)
+        N.call('mqb_apply', prog.handle, _ptr(states), batch, _ptr(params), 0, _ptr(custom), _ptr(ws),
+               ws_bytes.value, _stream())
+
+    def _measure(self, state, gate, rng):
+        """ApplyMeasure (vector_state.tpp:440-462): draw, collapse, optional reset."""
+        q = gate.obj_qubits[0]
+        out = torch.zeros(1, dtype=torch.float64, device=self.device)
+        N.call('mqb_qubit_one_probability', self.n_qubits, self.precision, _ptr(state), q, _ptr(out), _stream())
+        one_amp = float(out.item())
+        collapse_to_one = rng.draw() < one_amp
+        prob = one_amp if collapse_to_one else 1.0 - one_amp
+        scale = 1.0 / math.sqrt(prob) if prob > 0 else 0.0
+        N.call('mqb_collapse', self.n_qubits, self.precision, _ptr(state), q, int(collapse_to_one), scale, _stream())
+        if gate.reset_to is not None and int(gate.reset_to) != int(collapse_to_one):
+            self._apply_segment(state, Circuit([G.X.on(q)]), ParameterResolver())
+        return int(collapse_to_one)
+
+    def _run(self, state, circuit, pr, rng):
+        if not circuit.has_measure_gate:
+            if len(circuit):
+                self._apply_segment(state, circuit, pr)
+            return {}
+        results = {}
+        segment = Circuit()
+        for g in circuit:
+            if isinstance(g, G.Measure):
+                if len(segment):
+                    self._apply_segment(state, segment, pr)
+                    segment = Circuit()
+                results[g.key] = self._measure(state, g, rng)
+            elif not isinstance(g, G.BarrierGate):
+                segment.append(g)
+        if len(segment):
+            self._apply_segment(state, segment, pr)
+        return results
+
+    def _check_pr(self, circuit, pr):
+        if circuit.params_name:
+            if pr is None:
+                raise ValueError("Applying a parameterized circuit needs a parameter_resolver.")
+            pr = to_pr(pr, circuit.params_name)
+            for k in circuit.params_name:
+                if k not in pr:
+                    raise ValueError(f"Parameter {k} is missing in the parameter resolver.")
+            if pr.is_complex:
+                warnings.warn("Simulator does not support complex number, the imaginary part will be ignored",
+                              UserWarning, stacklevel=3)
+            return pr
+        return ParameterResolver()
+
+    def apply_circuit(self, circuit, pr=None):
+        """Apply a circuit; measurements collapse the state and are returned as a MeasureResult."""
+        if not isinstance(circuit, Circuit):
+            raise TypeError(f"circuit requires a Circuit, but get {type(circuit)}")
+        if self.n_qubits < circuit.n_qubits:
+            raise ValueError(f"Circuit has {circuit.n_qubits} qubits, which is more than simulator qubits.")
+        pr = self._check_pr(circuit, pr)
+        res = self._run(self.state, circuit, pr, self._rng)
+        if res:
+            out = MeasureResult()
+            keys = circuit.all_measures.keys()
+            out.add_measure(keys)
+            out.collect_data([[res[k] for k in out.keys]])
+            return out
+        return None
+
+    def apply_gate(self, gate, pr=None, diff=False):
+        """Apply one gate; ``diff=True`` applies the gate's derivative matrix (vector_state.tpp:166-437)."""
+        if not isinstance(gate, G.BasicGate):
+            raise TypeError(f"gate requires a quantum gate, but get {type(gate)}")
+        if isinstance(gate, G.BarrierGate):
+            return None
+        if max(gate.obj_qubits + gate.ctrl_qubits) >= self.n_qubits:
+            raise ValueError(f"qubits of gate {gate} is higher than simulator qubits.")
+        if isinstance(gate, G.Measure):
+            return self._measure(self.state, gate, self._rng)
+        circ = Circuit([gate])
+        pr = self._check_pr(circ, pr)
+        if diff and gate.parameterized:
+            # derivative matrix on the controlled subspace, zero elsewhere (SetToZeroExcept)
+            names = [k for p in gate.get_parameters() for k in p.params_name]
+            dm = gate.diff_matrix(pr, names[0] if len(set(names)) == 1 else None)
+            qubits = gate.obj_qubits + gate.ctrl_qubits
+            k, c = len(gate.obj_qubits), len(gate.ctrl_qubits)
+            full = np.zeros((1 << (k + c), 1 << (k + c)), dtype=complex)
+            base = ((1 << c) - 1) << k
+            full[base:base + (1 << k), base:base + (1 << k)] = dm
+            circ = Circuit([G.UnivMathGate('diff', full).on(qubits)])
+            pr = ParameterResolver()
+        self._apply_segment(self.state, circ, pr)
+        return None
+
+    def apply_hamiltonian(self, hamiltonian):
+        if not isinstance(hamiltonian, Hamiltonian):
+            raise TypeError(f"hamiltonian requires a Hamiltonian, but get {type(hamiltonian)}")
+        self._check_ham(hamiltonian)
+        h = native_ham(hamiltonian, self.n_qubits, self.precision)
+        out = torch.empty_like(self.state)
+        N.call('mqb_apply_hamiltonian', h.handle, _ptr(self.state), _ptr(out), 1, _stream())
+        self._state = out
+
+    def _check_ham(self, ham):
+        if ham.n_qubits > self.n_qubits:
+            raise ValueError(f"Hamiltonian qubits is {ham.n_qubits}, not match with simulator qubits number "
+                             f"{self.n_qubits}")
+
+    # ------------------------------------------------------------------ expectations
+    def get_expectation(self, hamiltonian, circ_right=None, circ_left=None, simulator_left=None, pr=None):
+        """<psi| circ_left^dag H circ_right |psi> (GetExpectation, vector_state.tpp:712-768)."""
+        if not isinstance(hamiltonian, Hamiltonian):
+            raise TypeError(f"hamiltonian requires a Hamiltonian, but get {type(hamiltonian)}")
+        self._check_ham(hamiltonian)
+        circ_right = Circuit() if circ_right is None else circ_right
+        pr = ParameterResolver() if pr is None else to_pr(pr, circ_right.params_name)
+        ket = self.state.clone()
+        self._run(ket, circ_right, pr, Mt19937Uniform(self.seed + 1))
+        if circ_left is None and simulator_left is None:
+            bra = ket
+        else:
+            src = self if simulator_left is None else simulator_left
+            if isinstance(src, BackendBase) and not isinstance(src, MQVectorB200):
+                raise TypeError("simulator_left should be a mqvector_b200 simulator")
+            if src.n_qubits != self.n_qubits or src.dtype != self.dtype:
+                raise ValueError("simulator_left should have the same qubits and dtype")
+            bra = src.state.clone()
+            self._run(bra, circ_right if circ_left is None else circ_left, pr, Mt19937Uniform(self.seed + 2))
+        h = native_ham(hamiltonian, self.n_qubits, self.precision)
+        out = torch.zeros(2, dtype=torch.float64, device=self.device)
+        N.call('mqb_expectation', h.handle, _ptr(bra), _ptr(ket), 1, _ptr(out), _stream())
+        o = out.cpu().numpy()
+        return complex(o[0], o[1])
+
+    def expectation_with_grad_tensor(self, hams, circuit, params, param_names, grad_names=None, init_state=None,
+                                     ckpt_stride=None):
+        """Batched forward + adjoint gradient on device tensors.
+
+        Args:
+            hams: list of Hamiltonian.
+            circuit: parameterized circuit (no measurement).
+            params: float64 CUDA tensor [batch][len(param_names)].
+            param_names: parameter order of ``params``.
+            grad_names: names that need gradients (default: all).
+            init_state: None (|0...0>), [2^n] or [batch][2^n] tensor.
+            ckpt_stride: passes between stored states (None: choose from free memory).
+        Returns:
+            f: float64 [batch][n_hams][2] (re, im); grad: float64 [batch][n_hams][n_params].
+        """
+        prog = lowered(circuit, self.n_qubits, self.precision, param_names, grad_names, self.fuse)
+        nh = [native_ham(h, self.n_qubits, self.precision) for h in hams]
+        params = params.to(device=self.device, dtype=torch.float64).contiguous()
+        batch = params.shape[0]
+        custom = None
+        if prog.customs:
+            custom = self._custom_tensor(prog, params.detach().cpu().numpy())
+        init_batched = 0
+        init = None
+        if init_state is not None:
+            init = init_state.to(device=self.device, dtype=self.torch_dtype).contiguous()
+            init_batched = 1 if init.dim() == 2 else 0
+        ham_arr = (ctypes.c_void_p * len(nh))(*[h.handle.value for h in nh])
+        stride = self._choose_stride(prog, batch, len(nh)) if ckpt_stride is None else int(ckpt_stride)
+        ws_bytes = ctypes.c_size_t()
+        N.call('mqb_grad_workspace_size', prog.handle, batch, len(nh), stride, ctypes.byref(ws_bytes))
+        ws = torch.empty(ws_bytes.value, dtype=torch.uint8, device=self.device)
+        f = torch.empty((batch, len(nh), 2), dtype=torch.float64, device=self.device)
+        g = torch.empty((batch, len(nh), max(1, len(param_names))), dtype=torch.float64, device=self.device)
+        N.call('mqb_expectation_with_grad', prog.handle, ham_arr, len(nh), _ptr(init), init_batched, batch,
+               _ptr(params), params.shape[1] if params.dim() == 2 else 0, _ptr(custom), _ptr(f), _ptr(g), stride,
+               _ptr(ws), ws_bytes.value, _stream())
+        return f, g[:, :, :len(param_names)]
+
+    def _choose_stride(self, prog, batch, n_hams):
+        """Store the state after every pass when it fits in ~60% of free memory, else every sqrt(P) passes."""
+        free, _ = torch.cuda.mem_get_info(self.device)
+        for stride in (1, max(2, int(math.ceil(math.sqrt(max(1, prog.grad_passes(n_hams)[0]))))), 0):
+            ws = ctypes.c_size_t()
+            N.call('mqb_grad_workspace_size', prog.handle, batch, n_hams, stride, ctypes.byref(ws))
+            if ws.value <= 0.6 * free:
+                return stride
+        return 0
+
+    def get_expectation_with_grad(self, hams, circ_right, circ_left=None, simulator_left=None, parallel_worker=None,
+                                  pr_shift=False):
+        """Build the grad operator of ``hams`` on ``circ_right`` (mqsim.py:255-439)."""
+        if isinstance(hams, Hamiltonian):
+            hams = [hams]
+        elif not isinstance(hams, list):
+            raise TypeError(f"hams requires a Hamiltonian or a list of Hamiltonian, but get {type(hams)}")
+        for h in hams:
+            if not isinstance(h, Hamiltonian):
+                raise TypeError(f"hams's element requires a Hamiltonian, but get {type(h)}")
+            self._check_ham(h)
+        if not isinstance(circ_right, Circuit):
+            raise TypeError(f"circ_right requires a Circuit, but get {type(circ_right)}")
+        if circ_left is not None or simulator_left is not None:
+            raise NotImplementedError("the non-Hermitian adjoint (circ_left / simulator_left) is not part of the "
+                                      "mqvector_b200 backend")
+        if pr_shift:
+            raise NotImplementedError("parameter-shift gradients are not part of the mqvector_b200 backend")
+        if circ_right.has_measure_gate:
+            raise ValueError("circuit for variational algorithm cannot have measure gate")
+        if self.n_qubits < circ_right.n_qubits:
+            raise ValueError(f"Simulator has {self.n_qubits} qubits, but circuit has {circ_right.n_qubits} qubits.")
+        ans_names = circ_right.ansatz_params_name
+        enc_names = circ_right.encoder_params_name
+        if set(ans_names) & set(enc_names):
+            raise RuntimeError("Parameter cannot be both encoder and ansatz parameter.")
+        version = "both"
+        if not ans_names:
+            version = "encoder"
+        if not enc_names:
+            version = "ansatz"
+        names = enc_names + ans_names
+        sim = self
+
+        def grad_ops(*inputs_):
+            inputs = [np.array(x) if isinstance(x, list) else x for x in inputs_]
+            if version == "both" and len(inputs) != 2:
+                raise ValueError("Need two inputs!")
+            if version in ("encoder", "ansatz") and len(inputs) != 1:
+                raise ValueError("Need one input!")
+            if version in ("both", "encoder"):
+                enc = np.asarray(inputs[0], dtype=np.float64)
+                if enc.ndim == 1:
+                    enc = enc[None, :]
+                if enc.ndim != 2 or enc.shape[1] != len(enc_names):
+                    raise ValueError(f"encoder data requires a two dimension array with {len(enc_names)} columns, "
+                                     f"but get shape {enc.shape}")
+                ans = np.asarray(inputs[1], dtype=np.float64).reshape(-1) if version == "both" else np.zeros(0)
+            else:
+                enc = np.zeros((1, 0))
+                ans = np.asarray(inputs[0], dtype=np.float64).reshape(-1)
+            if ans.size != len(ans_names):
+                raise ValueError(f"ansatz data requires {len(ans_names)} values, but get {ans.size}")
+            params = np.concatenate([enc, np.broadcast_to(ans, (enc.shape[0], ans.size))], axis=1)
+            init = sim._state
+            f, g = sim.expectation_with_grad_tensor(hams, circ_right, torch.as_tensor(params), names, init_state=init)
+            f = f.cpu().numpy()
+            g = g.cpu().numpy()
+            fc = f[..., 0] + 1j * f[..., 1]
+            gc = g.astype(np.complex128)
+            if version == 'both':
+                return fc, gc[:, :, :len(enc_names)], gc[:, :, len(enc_names):]
+            return fc, gc
+
+        wrapper = GradOpsWrapper(grad_ops, hams, circ_right, circ_left, enc_names, ans_names, parallel_worker, self)
+        wrapper.set_str(f"{self.n_qubits} qubit{'' if self.n_qubits == 1 else 's'} {self.name} VQA Operator")
+        return wrapper
+
+    # ------------------------------------------------------------------ sampling
+    def sampling(self, circuit, pr=None, shots=1, seed=None):
+        """Sample measurement outcomes (mqsim.py:456-491; vector_state.tpp:1308-1373)."""
+        if not isinstance(circuit, Circuit):
+            raise TypeError(f"circuit requires a Circuit, but get {type(circuit)}")
+        if not circuit.has_measure_gate:
+            raise ValueError("circuit must have at least one measurement gate.")
+        if self.n_qubits < circuit.n_qubits:
+            raise ValueError(f"Circuit has {circuit.n_qubits} qubits, which is more than simulator qubits.")
+        if not isinstance(shots, (int, np.integer)) or shots < 1:
+            raise ValueError(f"sampling shots should be a positive integer, but get {shots}")
+        pr = self._check_pr(circuit, pr)
+        if seed is None:
+            seed = int(np.random.randint(1, 2 << 20))
+        res = MeasureResult()
+        res.add_measure(circuit.all_measures.keys())
+        key_map = res.keys_map
+        rng = Mt19937Uniform(seed)
+        samples = np.zeros((shots, len(key_map)), dtype=np.int64)
+        if circuit.is_measure_end:
+            sub = int(rng.draw(low=1.0, high=float(1 << 20)))
+            sim_rng = Mt19937Uniform(sub)
+            m_gates = [g for g in circuit if isinstance(g, G.Measure)]
+            other = Circuit([g for g in circuit if not isinstance(g, (G.Measure, G.BarrierGate))])
+            st = self.state.clone()
+            if len(other):
+                self._apply_segment(st, other, pr)
+            u = sim_rng.draw(shots)
+            if self.arithmetic_type == complex64:
+                u = u.astype(np.float32).astype(np.float64)
+            u.sort()
+            u_t = torch.as_tensor(u, device=self.device)
+            idx = torch.empty(shots, dtype=torch.int64, device=self.device)
+            scratch_bytes = ctypes.c_size_t()
+            N.call('mqb_sample_scratch_size', self.n_qubits, ctypes.byref(scratch_bytes))
+            scratch = torch.empty(scratch_bytes.value, dtype=torch.uint8, device=self.device)
+            N.call('mqb_sample_indices', self.n_qubits, self.precision, _ptr(st), _ptr(u_t), shots, _ptr(idx),
+                   _ptr(scratch), scratch_bytes.value, _stream())
+            r = idx.cpu().numpy()
+            for g in m_gates:
+                samples[:, key_map[g.key]] = (r >> g.obj_qubits[0]) & 1
+        else:
+            for s in range(shots):
+                sub = Mt19937Uniform(int(rng.draw(low=1.0, high=float(1 << 20))))
+                st = self.state.clone()
+                out = self._run(st, circuit, pr, sub)
+                for k, v in out.items():
+                    samples[s, key_map[k]] = v
+        res.collect_data(samples)
+        return res
