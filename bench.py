@@ -1,0 +1,383 @@
+"""Benchmark: batched complex64 adjoint gradients of a 26-qubit hardware-efficient ansatz on B200.
+
+Workload (one "step" = one batched gradient evaluation): 26 qubits, 12 layers of RY then RZ on
+every qubit followed by a CNOT ladder q_i -> q_{i+1} (624 parameters, 924 gates); the
+Hamiltonian H = sum_i a_i Z_i Z_{i+1} + sum_i b_i X_i (51 terms, a, b ~ N(0, 1)); a batch of B
+parameter sets (encoder samples) with angles ~ U[0, 2pi).  Every step computes <H> and the full
+624-entry gradient for every sample, complex64 state with FP64 reductions.  Synthetic data from
+numpy.random.default_rng(0): angles first, then Hamiltonian coefficients.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun every rank runs its own batch (replicas, weak scaling, no data-path collective);
+the timed region is bracketed by a barrier and a device synchronize and the max over ranks is
+reported.  ``--impl reference`` times the reference algorithm's CPU implementation (the oracle
+port of the mqvector CPU kernels) on the host cores, one bounded sample per step.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+METRIC = "grad evals/s at 26q c64-batched vs c128-plain, same B200, err≤1e-5; HBM GB/s"
+UNIT = "grad evals/s"
+
+
+def build_workload(n, layers, batch, seed=0):
+    from mindquantum_b200.core import gates as G
+    from mindquantum_b200.core.circuit import Circuit
+    from mindquantum_b200.core.operators import Hamiltonian, QubitOperator
+
+    circ = Circuit()
+    k = 0
+    for _ in range(layers):
+        for q in range(n):
+            circ += G.RY(f'p{k}').on(q)
+            k += 1
+        for q in range(n):
+            circ += G.RZ(f'p{k}').on(q)
+            k += 1
+        for q in range(n - 1):
+            circ += G.X.on(q + 1, q)
+    circ.as_encoder()
+    rng = np.random.default_rng(seed)
+    params = rng.uniform(0, 2 * np.pi, size=(batch, k))
+    a = rng.normal(size=n - 1)
+    b = rng.normal(size=n)
+    op = QubitOperator()
+    for i in range(n - 1):
+        op += QubitOperator(f'Z{i} Z{i + 1}', float(a[i]))
+    for i in range(n):
+        op += QubitOperator(f'X{i}', float(b[i]))
+    return circ, Hamiltonian(op), params
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+             'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+             'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--query-gpu={self.QUERY}', '--format=csv,noheader,nounits',
+                                          '-i', str(self.gpu), '-lms', '200'], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(',')])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() == 'active':
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json'), encoding='utf8') as f:
+            d = json.load(f)
+        return float(d['hbm_gbs']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback'
+
+
+def _traffic_from_profiles():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, 'profiles', 'fused_backward_26q_c64.json')
+    try:
+        with open(path, encoding='utf8') as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_reference_sample(n, layers_total, threads, steps=1, warmup=0, dtype=np.complex64):
+    """Time the oracle port of the reference CPU algorithm on a bounded sample of the workload.
+
+    One sample = forward + adjoint sweep of ONE layer of the ansatz at full register size; the
+    Hamiltonian application + <psi|H psi> (same for every layer count) is timed once.  The full
+    evaluation time is t_H + layers_total * t_layer.
+    """
+    from oracle import oracle as O
+
+    O.set_num_threads(threads)
+    circ1, ham, params = build_workload(n, 1, 1)
+    prd = dict(zip(circ1.params_name, params[0].tolist()))
+    herm = [g.hermitian() for g in reversed(list(circ1))]
+    p_map = {k: i for i, k in enumerate(circ1.params_name)}
+
+    psi = O.zero_state(n, dtype)
+    for g in circ1:
+        O.apply_gate(psi, n, g, prd)
+    t0 = time.perf_counter()
+    lam = O.apply_terms(psi, n, ham)
+    O.vdot(psi, lam, n)
+    t_h = time.perf_counter() - t0
+    del lam
+
+    def one_layer():
+        s = O.zero_state(n, dtype)
+        for g in circ1:
+            O.apply_gate(s, n, g, prd)
+        lam_ = s.copy()     # stands in for H|psi>: the adjoint sweep costs the same for any lambda
+        f_g = np.zeros(1 + len(p_map), dtype=complex)
+        for g in herm:
+            O.apply_gate(s, n, g, prd)
+            if O.gate_requires_grad(g):
+                title, jac = O.jacobi(g)
+                intrin = np.array(O.expect_diff_gate(s, lam_, n, g, prd))
+                pg = intrin @ jac
+                for name, idx in title.items():
+                    f_g[1 + p_map[name]] += pg[idx]
+            O.apply_gate(lam_, n, g, prd)
+        return f_g
+
+    for _ in range(warmup):
+        one_layer()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        one_layer()
+        times.append(time.perf_counter() - t0)
+    t_layer = float(np.median(times))
+    t_eval = t_h + layers_total * t_layer
+    return {"value": 1.0 / t_eval, "t_h": t_h, "t_layer": t_layer, "t_eval": t_eval, "times": times}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    r = cpu_reference_sample(args.qubits, args.layers, threads, steps=args.steps, warmup=args.warmup)
+    sample = (f"{args.qubits} qubits complex64, forward + adjoint sweep of 1 of {args.layers} layers per step plus one "
+              f"H application (51 terms); eval time = t_H + {args.layers} * t_layer")
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["t_layer"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+        "config": {"workload": f"HEA {args.qubits}q x {args.layers} layers, 624 params, 51-term H, per-sample grad",
+                   "n_qubits": args.qubits, "layers": args.layers, "batch": 1, "parallelism": "cpu"},
+        "impl": "reference",
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+
+    from mindquantum_b200 import _native as N
+    from mindquantum_b200 import complex64, complex128
+    from mindquantum_b200.simulator.mqvector_b200 import MQVectorB200
+    from mindquantum_b200.simulator import lowering
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        import datetime
+
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    dev = torch.device('cuda', local_rank)
+    n, layers, B = args.qubits, args.layers, args.batch
+    circ, ham, params_np = build_workload(n, layers, B, seed=rank)
+    names = circ.params_name
+    sim = MQVectorB200('mqvector_b200', n, dtype=complex64, device=dev)
+    params = torch.as_tensor(params_np, device=dev)
+    prog = lowering.lowered(circ, n, sim.precision, names, None, True)
+    stride = sim._choose_stride(prog, B, 1)  # pylint: disable=protected-access
+    n_passes, tile_bits = prog.grad_passes(1)
+
+    def step():
+        return sim.expectation_with_grad_tensor([ham], circ, params, names, ckpt_stride=stride)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            f, g = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * B * args.steps / (ms / 1e3)
+
+    # per-kernel event timing of the same steps (a separate timed run, so events do not perturb `value`)
+    with N.KernelTimer() as kt:
+        for _ in range(args.steps):
+            step()
+    launches = sum(kt.launches.values())
+    dom = max(kt.ms, key=lambda k: kt.ms[k])
+    S = (1 << n) * 8 * B
+    n_ham = kt.launches['hamiltonian'] // args.steps
+    # algorithmic bytes per step for each kernel kind
+    alg = {
+        'fused_forward': (2 * n_passes - 1) * S,                                 # pass 0 writes |0> tiles only
+        'fused_backward': n_passes * 3 * S + (0 if stride == 1 else n_passes * S),  # psi read, lambda read+write
+        'hamiltonian': (2 * S + 3 * S * (n_ham - 1)) if n_ham else 0,
+    }
+    peak, peak_kind = _peaks()
+    achieved = alg.get(dom, 0) * args.steps / (kt.ms[dom] / 1e3) / 1e9 if kt.ms[dom] else None
+    total_alg = sum(alg.values()) * args.steps
+    traffic = _traffic_from_profiles()
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": (traffic or {}).get('dram_bytes_per_launch'),
+                "alg_bytes_per_launch": alg.get(dom, 0) / max(1, kt.launches[dom] // args.steps),
+                "avg_launch_ms": kt.ms[dom] / max(1, kt.launches[dom]), "peak_source": peak_kind,
+                "step_hbm_gbs": total_alg / (ms / 1e3) / 1e9 if world == 1 else None,
+                "kernel_ms_per_step": {k: v / args.steps for k, v in kt.ms.items() if v}}
+
+    # end to end through the public API: numpy in, numpy out (host<->device copies inside)
+    ops = sim.get_expectation_with_grad(ham, circ)
+    ops(params_np)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fe, ge = ops(params_np)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * B * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(params_np.nbytes),
+           "d2h_bytes_per_step": int(fe.nbytes + ge.nbytes)}
+
+    extras = {}
+    if rank == 0 and not args.skip_extras:
+        # accuracy: the same parameter set in complex128 (fused, FP64 throughout)
+        s128 = MQVectorB200('mqvector_b200', n, dtype=complex128, device=dev)
+        p1 = params[:1]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f128, g128 = s128.expectation_with_grad_tensor([ham], circ, p1, names, ckpt_stride=0)
+        torch.cuda.synchronize()
+        t128 = time.perf_counter() - t0
+        extras["grad_err_vs_c128"] = float((g[:1] - g128).abs().max().item())
+        extras["f_err_vs_c128"] = float((f[:1, :, 0] - f128[:, :, 0]).abs().max().item())
+        extras["grad_max_abs"] = float(g128.abs().max().item())
+        extras["c128_fused"] = {"value": 1.0 / t128, "unit": UNIT, "batch": 1}
+        if not args.skip_plain:
+            # the plain complex128 single-circuit path: one kernel per gate, per-gate reductions
+            sp = MQVectorB200('mqvector_b200', n, dtype=complex128, device=dev, fuse=False)
+            sp.expectation_with_grad_tensor([ham], circ, p1, names, ckpt_stride=0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fp, gp = sp.expectation_with_grad_tensor([ham], circ, p1, names, ckpt_stride=0)
+            torch.cuda.synchronize()
+            tp = time.perf_counter() - t0
+            extras["c128_plain"] = {"value": 1.0 / tp, "unit": UNIT, "batch": 1,
+                                    "grad_err_vs_c128_fused": float((gp - g128).abs().max().item())}
+            extras["ratio_vs_c128_plain"] = value / world / extras["c128_plain"]["value"]
+            del sp
+        del s128
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        threads = os.cpu_count() or 1
+        r = cpu_reference_sample(n, layers, threads, steps=1, warmup=0)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{n} qubits complex64, forward + adjoint sweep of 1 of {layers} layers + one H "
+                         f"application; eval time = t_H + {layers} * t_layer = {r['t_eval']:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": f"HEA {n}q x {layers} layers (RY,RZ + CNOT ladder), {len(names)} params, "
+                                   f"51-term ZZ+X Hamiltonian, batched adjoint gradient",
+                       "n_qubits": n, "layers": layers, "params": len(names), "batch_per_gpu": B,
+                       "global_batch": B * world, "precision": "complex64 state, FP64 reductions",
+                       "passes": n_passes, "tile_bits": tile_bits, "ckpt_stride": stride,
+                       "l2": "inputs larger than L2 (512 MiB per state)", "parallelism": f"replicas x{world}"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "gpu_launches": launches, **extras,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--qubits', type=int, default=26)
+    ap.add_argument('--layers', type=int, default=12)
+    ap.add_argument('--batch', type=int, default=8)
+    ap.add_argument('--skip-extras', action='store_true')
+    ap.add_argument('--skip-plain', action='store_true')
+    ap.add_argument('--skip-cpu', action='store_true')
+    args = ap.parse_args()
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local_rank = int(os.environ.get('LOCAL_RANK', 0))
+    if args.impl == 'reference':
+        run_reference(args, rank)
+        return
+    run_b200(args, rank, world, local_rank)
+
+
+if __name__ == '__main__':
+    main()

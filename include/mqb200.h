@@ -112,6 +112,12 @@ typedef struct mqb_program_info {
 MQB_API const char *mqb_last_error(void);
 MQB_API int mqb_version(void);
 MQB_API int mqb_device_sm_count(int *out);
+/* Per-launch timing of the engine's kernels (CUDA events on the launching stream).  Kinds:
+ * 0 fused forward pass, 1 fused backward pass, 2 Hamiltonian pass, 3 matrix generation,
+ * 4 per-gate apply, 5 per-gate gradient, 6 gradient scatter, 7 copies.  mqb_timing_end
+ * synchronizes, writes total milliseconds and launch counts per kind and stops timing. */
+MQB_API int mqb_timing_begin(void);
+MQB_API int mqb_timing_end(double *ms, int64_t *launches, int n_kinds);
 /* sizeof of mqb_gate_desc, mqb_param_term, mqb_program_options, mqb_program_info (ABI check). */
 MQB_API int mqb_abi_struct_sizes(int64_t *out, int n);
 

@@ -70,6 +70,8 @@ _D = ctypes.c_double
 SIGNATURES = {
     'mqb_version': [],
     'mqb_device_sm_count': [_P],
+    'mqb_timing_begin': [],
+    'mqb_timing_end': [_P, _P, _I],
     'mqb_abi_struct_sizes': [_P, _I],
     'mqb_program_create': [_I, _I, _P, _I, _P, _I, _I, _P, _I64, _P, _P],
     'mqb_program_destroy': [_P],
@@ -134,3 +136,26 @@ def check(status, what=''):
 def call(name, *args):
     """Call an entry point and raise NativeError on a non-zero status."""
     check(getattr(lib(), name)(*args), name)
+
+
+TIMING_KINDS = ('fused_forward', 'fused_backward', 'hamiltonian', 'matgen', 'gate_apply', 'gate_grad', 'grad_scatter',
+                'copy')
+
+
+class KernelTimer:
+    """Context manager collecting per-kind kernel times (ms) and launch counts of libmqb200."""
+
+    def __enter__(self):
+        call('mqb_timing_begin')
+        self.ms = {}
+        self.launches = {}
+        return self
+
+    def __exit__(self, *exc):
+        n = len(TIMING_KINDS)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int64 * n)()
+        call('mqb_timing_end', ms, cnt, n)
+        self.ms = {k: ms[i] for i, k in enumerate(TIMING_KINDS)}
+        self.launches = {k: cnt[i] for i, k in enumerate(TIMING_KINDS)}
+        return False

@@ -76,6 +76,34 @@ T *upload(const std::vector<T> &v) {
 
 bool is_diag_gid(int gid) { return gid == GID_RZ || gid == GID_PS || gid == GID_GP || gid == GID_RZZ; }
 
+// Optional per-launch timing: CUDA events around every kernel launch of the engine, recorded on the
+// launching stream while enabled; mqb_timing_end synchronizes and reports the time per launch kind.
+enum TimedKind { TK_FWD = 0, TK_BWD, TK_HAM, TK_MATGEN, TK_PLAIN_APPLY, TK_PLAIN_GRAD, TK_SCATTER, TK_OTHER, TK_COUNT };
+struct TimedLaunch {
+    int kind;
+    cudaEvent_t a, b;
+};
+bool g_timing = false;
+std::vector<TimedLaunch> g_timed;
+
+struct TimeScope {
+    TimedLaunch t{};
+    cudaStream_t st;
+    bool on;
+    TimeScope(int kind, cudaStream_t s) : st(s), on(g_timing) {
+        if (!on) return;
+        t.kind = kind;
+        cudaEventCreate(&t.a);
+        cudaEventCreate(&t.b);
+        cudaEventRecord(t.a, st);
+    }
+    ~TimeScope() {
+        if (!on) return;
+        cudaEventRecord(t.b, st);
+        g_timed.push_back(t);
+    }
+};
+
 }  // namespace
 
 using namespace mqb;
@@ -174,10 +202,15 @@ static void run_forward_pass(const mqb_program &p, const Schedule &s, const Pass
         a.dst = dst;
         a.batch = batch;
         a.src_batch_stride = src_stride;
+        TimeScope ts(TK_FWD, st);
         ck(launch_fused_fwd<R>(a, sm, st), "fused forward pass");
         return;
     }
-    if (src != dst) ck(launch_copy_or_zero<R>(dst, src, p.n, batch, src_stride, st), "state copy");
+    if (src != dst) {
+        TimeScope ts(TK_OTHER, st);
+        ck(launch_copy_or_zero<R>(dst, src, p.n, batch, src_stride, st), "state copy");
+    }
+    TimeScope ts(TK_PLAIN_APPLY, st);
     ck(launch_plain_apply<R>(dst, p.n, batch, p.ops[ps.op_begin], mats, p.per_sample, cpool, false, sm, st),
        "gate kernel");
 }
@@ -198,6 +231,7 @@ static void run_matgen(const mqb_program &p, const double *params, int64_t param
     m.batch = batch;
     m.mats = mats;
     m.mats_stride = p.per_sample;
+    TimeScope ts(TK_MATGEN, st);
     ck(launch_matgen<R>(m, st), "matgen");
 }
 
@@ -239,6 +273,7 @@ static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R>
         a.batch = batch;
         a.out_batch_stride = dim;
         a.f_stride = f_stride;
+        TimeScope ts(TK_HAM, st);
         ck(launch_ham<R>(a, sm, st), "hamiltonian pass");
     }
 }
@@ -338,6 +373,7 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
             a.slot_map = s.d_slot_map + ps.slot_begin;
             a.n_local_slots = ps.n_slots;
             a.batch = batch;
+            TimeScope ts(TK_BWD, st);
             ck(launch_fused_bwd<R>(a, sm, st), "fused backward pass");
         } else {
             const DevOp &op = p.ops[ps.op_begin];
@@ -346,18 +382,28 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
                 psi_q = ckpt(q);
             } else {
                 V *src = loc(q + 1);
-                if (src != W) ck(launch_copy_or_zero<R>(W, src, p.n, batch, dim, st), "state copy");
+                if (src != W) {
+                    TimeScope ts(TK_OTHER, st);
+                    ck(launch_copy_or_zero<R>(W, src, p.n, batch, dim, st), "state copy");
+                }
+                TimeScope ts(TK_PLAIN_APPLY, st);
                 ck(launch_plain_apply<R>(W, p.n, batch, op, mats, p.per_sample, cpool, true, sm, st), "gate kernel");
                 psi_q = W;
             }
-            ck(launch_plain_grad<R>(psi_q, lam, p.n, batch, n_hams, op, mats, p.per_sample, gslots,
-                                    std::max(1, p.n_slots), sm, st),
-               "gradient kernel");
-            for (int h = 0; h < n_hams; ++h)
+            {
+                TimeScope ts(TK_PLAIN_GRAD, st);
+                ck(launch_plain_grad<R>(psi_q, lam, p.n, batch, n_hams, op, mats, p.per_sample, gslots,
+                                        std::max(1, p.n_slots), sm, st),
+                   "gradient kernel");
+            }
+            for (int h = 0; h < n_hams; ++h) {
+                TimeScope ts(TK_PLAIN_APPLY, st);
                 ck(launch_plain_apply<R>(lam + h * batch * dim, p.n, batch, op, mats, p.per_sample, cpool, true, sm, st),
                    "gate kernel");
+            }
         }
     }
+    TimeScope ts(TK_SCATTER, st);
     ck(launch_grad_scatter(gslots, batch, std::max(1, p.n_slots), n_hams, p.d_csr_ptr, p.d_csr_slot, p.d_csr_coeff,
                            p.n_params, grad, st),
        "gradient scatter");
@@ -448,6 +494,39 @@ extern "C" {
 const char *mqb_last_error(void) { return g_last_error.c_str(); }
 
 int mqb_version(void) { return 100; }
+
+int mqb_timing_begin(void) {
+    return guarded([&] {
+        for (auto &t : g_timed) {
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+        }
+        g_timed.clear();
+        g_timing = true;
+    });
+}
+
+int mqb_timing_end(double *ms, int64_t *launches, int n_kinds) {
+    return guarded([&] {
+        g_timing = false;
+        for (int k = 0; k < n_kinds; ++k) {
+            ms[k] = 0;
+            launches[k] = 0;
+        }
+        for (auto &t : g_timed) {
+            ck(cudaEventSynchronize(t.b), "cudaEventSynchronize");
+            float e = 0;
+            ck(cudaEventElapsedTime(&e, t.a, t.b), "cudaEventElapsedTime");
+            if (t.kind < n_kinds) {
+                ms[t.kind] += e;
+                launches[t.kind] += 1;
+            }
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+        }
+        g_timed.clear();
+    });
+}
 
 int mqb_device_sm_count(int *out) {
     return guarded([&] { *out = sm_count_cached(); });

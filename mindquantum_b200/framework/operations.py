@@ -28,9 +28,10 @@ class _ExpectationFunction(torch.autograd.Function):
                                                 init_state=sim._state)  # pylint: disable=protected-access
         ctx.n_enc = n_enc
         ctx.save_for_backward(g)
-        ctx.enc_dtype = enc.dtype if enc is not None else torch.float32
-        ctx.ans_dtype = ans.dtype if ans is not None else torch.float32
-        return f[..., 0].to(ctx.enc_dtype if n_enc else ctx.ans_dtype)
+        ctx.enc_dtype, ctx.enc_device = enc.dtype, enc.device
+        ctx.ans_dtype, ctx.ans_device = ans.dtype, ans.device
+        ref = enc if n_enc else ans
+        return f[..., 0].to(device=ref.device, dtype=ref.dtype)
 
     @staticmethod
     def backward(ctx, dout):  # pylint: disable=arguments-differ
@@ -38,8 +39,10 @@ class _ExpectationFunction(torch.autograd.Function):
         dout = dout.to(g.dtype).to(g.device)
         g_enc = g[:, :, :ctx.n_enc]
         g_ans = g[:, :, ctx.n_enc:]
-        enc_grad = torch.einsum('smp,sm->sp', g_enc, dout).to(ctx.enc_dtype) if ctx.n_enc else None
-        ans_grad = torch.einsum('smp,sm->p', g_ans, dout).to(ctx.ans_dtype) if g_ans.shape[2] else None
+        enc_grad = (torch.einsum('smp,sm->sp', g_enc, dout).to(device=ctx.enc_device, dtype=ctx.enc_dtype)
+                    if ctx.n_enc else None)
+        ans_grad = (torch.einsum('smp,sm->p', g_ans, dout).to(device=ctx.ans_device, dtype=ctx.ans_dtype)
+                    if g_ans.shape[2] else None)
         return enc_grad, ans_grad, None
 
 
