@@ -124,6 +124,8 @@ struct SchedDev {
     ~SchedDev() {
         cudaFree(s.d_pass_ops);
         cudaFree(s.d_slot_map);
+        cudaFree(s.d_stages);
+        cudaFree(s.d_stage_ops);
     }
 };
 
@@ -154,17 +156,22 @@ struct mqb_program {
     size_t elem() const { return precision == MQB_PREC_C64 ? 8 : 16; }
 };
 
-static std::unique_ptr<SchedDev> make_sched(const mqb_program &p, int K, bool fuse) {
+static std::unique_ptr<SchedDev> make_sched(const mqb_program &p, int K, bool fuse, int reg_bits) {
     auto sd = std::make_unique<SchedDev>();
     sd->s = build_schedule(p.n, K, contiguity_bits(p.precision), p.ops, fuse);
+    build_stages(sd->s, p.ops, reg_bits, p.precision);
     sd->s.d_pass_ops = upload(sd->s.pass_ops);
     sd->s.d_slot_map = upload(sd->s.slot_map);
+    sd->s.d_stages = upload(sd->s.stages);
+    sd->s.d_stage_ops = upload(sd->s.stage_ops);
     return sd;
 }
 
-static int grad_tile_bits(const mqb_program &p, int n_hams) {
-    if (p.tile_bits > 0) return std::min(p.tile_bits, default_tile_bits(p.precision, 1 + n_hams) + 1);
-    return default_tile_bits(p.precision, 1 + n_hams);
+// Tile size of the fused kernels: 2^RB registers x 2^8 threads, capped by the register size.
+static int tile_bits_for(const mqb_program &p, int reg_bits) {
+    int K = reg_bits + 8;
+    if (p.tile_bits > 0) K = std::min(K, std::max(reg_bits + 5, p.tile_bits));
+    return std::min(K, p.n);
 }
 
 static SchedDev &grad_schedule(mqb_program &p, int n_hams) {
@@ -172,7 +179,8 @@ static SchedDev &grad_schedule(mqb_program &p, int n_hams) {
     const int key = fused ? n_hams : 0;
     auto it = p.grad_sched.find(key);
     if (it != p.grad_sched.end()) return *it->second;
-    auto sd = make_sched(p, fused ? grad_tile_bits(p, n_hams) : p.n, fused);
+    const int rb = bwd_reg_bits(p.precision, n_hams);
+    auto sd = make_sched(p, fused ? tile_bits_for(p, rb) : p.n, fused, rb);
     SchedDev &ref = *sd;
     p.grad_sched[key] = std::move(sd);
     return ref;
@@ -190,10 +198,13 @@ static void run_forward_pass(const mqb_program &p, const Schedule &s, const Pass
     const int sm = sm_count_cached();
     const cplx<R> *cpool = static_cast<const cplx<R> *>(p.d_cpool);
     if (ps.fused) {
-        FwdArgs<R> a{};
+        Fwd2Args<R> a{};
         a.g = make_geom(p.n, ps.qbits);
-        a.pops = s.d_pass_ops + ps.op_begin;
-        a.n_pops = ps.op_end - ps.op_begin;
+        a.stages = s.d_stages + ps.stage_begin;
+        a.n_stages = ps.n_stages;
+        a.sops = s.d_stage_ops + ps.sop_begin;
+        a.n_ops = ps.n_sops;
+        a.reg_bits = ps.reg_bits;
         a.ops = p.d_ops;
         a.mats = mats;
         a.mats_stride = p.per_sample;
@@ -203,7 +214,7 @@ static void run_forward_pass(const mqb_program &p, const Schedule &s, const Pass
         a.batch = batch;
         a.src_batch_stride = src_stride;
         TimeScope ts(TK_FWD, st);
-        ck(launch_fused_fwd<R>(a, sm, st), "fused forward pass");
+        ck(launch_fused_fwd2<R>(a, sm, st), "fused forward pass");
         return;
     }
     if (src != dst) {
@@ -356,10 +367,13 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
         const Pass &ps = s.passes[q];
         const bool stored_q = L.ckpt_index[q] >= 0;
         if (ps.fused) {
-            BwdArgs<R> a{};
+            Bwd2Args<R> a{};
             a.g = make_geom(p.n, ps.qbits);
-            a.pops = s.d_pass_ops + ps.op_begin;
-            a.n_pops = ps.op_end - ps.op_begin;
+            a.stages = s.d_stages + ps.stage_begin;
+            a.n_stages = ps.n_stages;
+            a.sops = s.d_stage_ops + ps.sop_begin;
+            a.n_ops = ps.n_sops;
+            a.reg_bits = ps.reg_bits;
             a.ops = p.d_ops;
             a.mats = mats;
             a.mats_stride = p.per_sample;
@@ -374,7 +388,7 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
             a.n_local_slots = ps.n_slots;
             a.batch = batch;
             TimeScope ts(TK_BWD, st);
-            ck(launch_fused_bwd<R>(a, sm, st), "fused backward pass");
+            ck(launch_fused_bwd2<R>(a, sm, st), "fused backward pass");
         } else {
             const DevOp &op = p.ops[ps.op_begin];
             V *psi_q;
@@ -626,8 +640,8 @@ int mqb_program_create(int n_qubits, int precision, const mqb_gate_desc *gates, 
         p->d_csr_ptr = upload(ptr);
         p->d_csr_slot = upload(slot);
         p->d_csr_coeff = upload(coeff);
-        const int K = p->tile_bits > 0 ? p->tile_bits : default_tile_bits(precision, 1);
-        p->apply_sched = make_sched(*p, K, p->fuse != 0);
+        const int rb = fwd_reg_bits(precision);
+        p->apply_sched = make_sched(*p, tile_bits_for(*p, rb), p->fuse != 0, rb);
         *out = p.release();
     });
 }
@@ -640,7 +654,9 @@ int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, i
         std::vector<DevOp> ops;
         for (int k = 0; k < n_gates; ++k)
             ops.push_back(basic_op(gates[k], k, n_qubits, nullptr, 0, 0, const_matrices, n_const_entries));
-        const int K = tile_bits > 0 ? tile_bits : default_tile_bits(precision, 1);
+        const int rb = fwd_reg_bits(precision);
+        int K = std::min(n_qubits, rb + 8);
+        if (tile_bits > 0) K = std::min(n_qubits, tile_bits);
         Schedule s = build_schedule(n_qubits, K, contiguity_bits(precision), ops, fuse != 0);
         int pos = 0;
         for (size_t pi = 0; pi < s.passes.size(); ++pi) {

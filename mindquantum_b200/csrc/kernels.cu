@@ -3,12 +3,7 @@
 //   matgen      : per (sample, gate) gate matrices and their angle derivatives from the
 //                 parameter vector (the reference evaluates ParameterResolver::Combination and
 //                 builds a matrix per gate per call on the host, vector_state.tpp:236-343).
-//   fused_fwd   : one read + write of the state applies every gate of a pass on 2^K-amplitude
-//                 tiles held in shared memory (replaces one sweep per gate).
-//   fused_bwd   : the adjoint sweep of one pass: uncompute psi, accumulate
-//                 Re<lambda_h| dU/dangle |psi> in FP64 for every gradient angle, uncompute every
-//                 lambda_h - for all gates of the pass in one read + write of psi and the lambdas
-//                 (replaces GradientHelper::LeftSizeGrad's per-gate sweeps, gradient.h:160-197).
+//   (the fused tile passes live in fused.cu)
 //   ham         : lambda = H psi and/or <bra|H|ket> for a group of Pauli terms whose flip masks fit
 //                 in one tile; terms with a common flip mask share one partner read
 //                 (replaces ApplyTerms / ExpectationOfTerms' pass per term, cpu_vector_core_policy.cpp:133-261).
@@ -341,126 +336,6 @@ cudaError_t launch_matgen(const MatgenArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// ------------------------------------------------------------------------------------------ fused forward
-template <typename V, bool ADJ>
-__device__ __forceinline__ V mat_el(const V *M, int dim, int r, int c) {
-    return ADJ ? cconj(M[c * dim + r]) : M[r * dim + c];
-}
-
-// Apply one op of a pass on the tile in shared memory (all threads participate).
-template <typename V, bool ADJ>
-__device__ __forceinline__ void tile_apply_op(V *tile, const PassOp &po, const V *M, uint64_t base, int K) {
-    const int T = blockDim.x;
-    if (po.kind == KIND_DIAG) {
-        V d[8];
-        const int nd = 1 << po.m;
-        for (int r = 0; r < nd; ++r) d[r] = ADJ ? cconj(M[r]) : M[r];
-        int fixed = 0;   // index bits of targets outside the tile
-        for (int k = 0; k < po.m; ++k)
-            if (po.lt[k] < 0) fixed |= int((base >> po.gt[k]) & 1) << k;
-        for (int L = threadIdx.x; L < (1 << K); L += T) {
-            if ((uint32_t(L) & po.lctrl) != po.lctrl) continue;
-            int r = fixed;
-            for (int k = 0; k < po.m; ++k)
-                if (po.lt[k] >= 0) r |= ((L >> po.lt[k]) & 1) << k;
-            tile[L] = cmul(tile[L], d[r]);
-        }
-        return;
-    }
-    if (po.m == 1) {
-        const int t0 = po.lt[0];
-        const V m00 = mat_el<V, ADJ>(M, 2, 0, 0), m01 = mat_el<V, ADJ>(M, 2, 0, 1);
-        const V m10 = mat_el<V, ADJ>(M, 2, 1, 0), m11 = mat_el<V, ADJ>(M, 2, 1, 1);
-        for (int p = threadIdx.x; p < (1 << (K - 1)); p += T) {
-            const uint32_t i0 = ins0(uint32_t(p), t0);
-            if ((i0 & po.lctrl) != po.lctrl) continue;
-            const uint32_t i1 = i0 | (1u << t0);
-            const V a = tile[i0], b = tile[i1];
-            tile[i0] = cmadd(m00, a, cmul(m01, b));
-            tile[i1] = cmadd(m10, a, cmul(m11, b));
-        }
-        return;
-    }
-    const int m = po.m;
-    const int nd = 1 << m;
-    int sorted[kMaxFusedM];
-    for (int k = 0; k < m; ++k) sorted[k] = po.lt[k];
-    for (int i = 1; i < m; ++i)
-        for (int j = i; j > 0 && sorted[j - 1] > sorted[j]; --j) {
-            const int tmp = sorted[j];
-            sorted[j] = sorted[j - 1];
-            sorted[j - 1] = tmp;
-        }
-    uint32_t off[8];
-    for (int r = 0; r < nd; ++r) {
-        uint32_t o = 0;
-        for (int k = 0; k < m; ++k)
-            if (r >> k & 1) o |= 1u << po.lt[k];
-        off[r] = o;
-    }
-    for (int p = threadIdx.x; p < (1 << (K - m)); p += T) {
-        uint32_t i0 = uint32_t(p);
-        for (int k = 0; k < m; ++k) i0 = ins0(i0, sorted[k]);
-        if ((i0 & po.lctrl) != po.lctrl) continue;
-        V v[8], o[8];
-        for (int r = 0; r < nd; ++r) v[r] = tile[i0 | off[r]];
-        for (int r = 0; r < nd; ++r) {
-            V acc = czero<V>();
-            for (int col = 0; col < nd; ++col) acc = cmadd(mat_el<V, ADJ>(M, nd, r, col), v[col], acc);
-            o[r] = acc;
-        }
-        for (int r = 0; r < nd; ++r) tile[i0 | off[r]] = o[r];
-    }
-}
-
-size_t fused_fwd_smem(const TileGeom &g, int n_pops, int elem_bytes) {
-    size_t s = (size_t(1) << g.K) * elem_bytes;
-    s = (s + 15) & ~size_t(15);
-    s += (size_t(1) << (g.K - g.c)) * sizeof(uint64_t);
-    s = (s + 15) & ~size_t(15);
-    s += size_t(n_pops) * sizeof(PassOp);
-    return s;
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kThreads) fused_fwd_kernel(const FwdArgs<R> a) {
-    using V = cplx<R>;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const TileGeom &g = a.g;
-    const int K = g.K, c = g.c;
-    V *tile = reinterpret_cast<V *>(smem);
-    size_t o = align16((size_t(1) << K) * sizeof(V));
-    uint64_t *tab = reinterpret_cast<uint64_t *>(smem + o);
-    o = align16(o + (size_t(1) << (K - c)) * sizeof(uint64_t));
-    PassOp *sops = reinterpret_cast<PassOp *>(smem + o);
-    build_table(tab, g);
-    for (int i = threadIdx.x; i < a.n_pops; i += blockDim.x) sops[i] = a.pops[i];
-    __syncthreads();
-    const int64_t n_tiles = int64_t(1) << g.n_out;
-    const int64_t dim = int64_t(1) << g.n;
-    for (int64_t w = blockIdx.x; w < a.batch * n_tiles; w += gridDim.x) {
-        const int64_t b = w >> g.n_out;
-        const uint64_t t = uint64_t(w) & uint64_t(n_tiles - 1);
-        const uint64_t base = tile_base(g, t);
-        if (a.src)
-            load_tile(tile, a.src + b * a.src_batch_stride, base, tab, K, c);
-        else
-            zero_tile(tile, base, K);
-        __syncthreads();
-        const V *mb = a.mats + b * a.mats_stride;
-        for (int k = 0; k < a.n_pops; ++k) {
-            const PassOp &po = sops[k];
-            if ((base & po.octrl) != po.octrl) continue;
-            const DevOp &op = a.ops[po.op];
-            const V *M = op.per_sample ? mb + op.mat_off : a.cpool + op.mat_off;
-            tile_apply_op<V, false>(tile, po, M, base, K);
-            __syncthreads();
-        }
-        store_tile(tile, a.dst + b * dim, base, tab, K, c);
-        __syncthreads();
-    }
-}
-
 template <typename KernelT>
 static int blocks_for(KernelT kern, size_t smem, int sm_count, int64_t work) {
     int per_sm = 0;
@@ -468,272 +343,6 @@ static int blocks_for(KernelT kern, size_t smem, int sm_count, int64_t work) {
         per_sm = 1;
     const int64_t want = int64_t(sm_count) * per_sm;
     return int(std::max<int64_t>(1, std::min<int64_t>(want, work)));
-}
-
-template <typename R>
-cudaError_t launch_fused_fwd(const FwdArgs<R> &a, int sm_count, cudaStream_t s) {
-    if (a.g.c < 1 || a.g.K > kMaxTileBits || a.g.K < 1) return cudaErrorInvalidValue;  // 16-byte tile accesses need a contiguous low qubit
-    const size_t smem = fused_fwd_smem(a.g, a.n_pops, sizeof(cplx<R>));
-    auto kern = fused_fwd_kernel<R>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    const int64_t work = a.batch << a.g.n_out;
-    kern<<<blocks_for(kern, smem, sm_count, work), kThreads, smem, s>>>(a);
-    return cudaGetLastError();
-}
-
-// ------------------------------------------------------------------------------------------ fused backward
-size_t fused_bwd_smem(const TileGeom &g, int n_pops, int n_hams, int n_local_slots, int elem_bytes) {
-    size_t s = (size_t(1) << g.K) * elem_bytes * (1 + n_hams);
-    s = (s + 15) & ~size_t(15);
-    s += (size_t(1) << (g.K - g.c)) * sizeof(uint64_t);
-    s = (s + 15) & ~size_t(15);
-    s += size_t(n_pops) * sizeof(PassOp);
-    s = (s + 15) & ~size_t(15);
-    s += size_t(kThreads / 32) * std::max(1, n_local_slots) * n_hams * sizeof(double);
-    return s;
-}
-
-// One op of the backward sweep on the psi and lambda tiles.  Each thread owns whole groups, so
-// psi <- U^dag psi, the gradient partials and lambda <- U^dag lambda of a group need no barrier.
-template <typename V, int NH>
-__device__ __forceinline__ void tile_bwd_op(V *psi, V *lam, int K, const PassOp &po, const DevOp &op, const V *M,
-                                            const V *dM, uint64_t base, double (&acc)[3][NH]) {
-    const int T = blockDim.x;
-    const int TS = 1 << K;
-    const int na = op.grad_mask ? op.n_angles : 0;
-    if (po.kind == KIND_DIAG) {
-        const int nd = 1 << po.m;
-        int fixed = 0;
-        for (int k = 0; k < po.m; ++k)
-            if (po.lt[k] < 0) fixed |= int((base >> po.gt[k]) & 1) << k;
-        for (int L = threadIdx.x; L < TS; L += T) {
-            if ((uint32_t(L) & po.lctrl) != po.lctrl) continue;
-            int r = fixed;
-            for (int k = 0; k < po.m; ++k)
-                if (po.lt[k] >= 0) r |= ((L >> po.lt[k]) & 1) << k;
-            const V dr = cconj(M[r]);
-            const V w = cmul(dr, psi[L]);
-            psi[L] = w;
-            V y[3];
-#pragma unroll
-            for (int an = 0; an < 3; ++an)
-                if (an < na && (op.grad_mask >> an & 1)) y[an] = cmul(dM[an * nd + r], w);
-#pragma unroll
-            for (int h = 0; h < NH; ++h) {
-                V l = lam[h * TS + L];
-#pragma unroll
-                for (int an = 0; an < 3; ++an)
-                    if (an < na && (op.grad_mask >> an & 1))
-                        acc[an][h] += double(l.x) * double(y[an].x) + double(l.y) * double(y[an].y);
-                lam[h * TS + L] = cmul(dr, l);
-            }
-        }
-        return;
-    }
-    if (po.m == 1) {
-        const int t0 = po.lt[0];
-        // U^dag entries
-        const V a00 = cconj(M[0]), a01 = cconj(M[2]), a10 = cconj(M[1]), a11 = cconj(M[3]);
-        V d[3][4];
-#pragma unroll
-        for (int an = 0; an < 3; ++an)
-            if (an < na && (op.grad_mask >> an & 1))
-#pragma unroll
-                for (int e = 0; e < 4; ++e) d[an][e] = dM[an * 4 + e];
-        for (int p = threadIdx.x; p < (TS >> 1); p += T) {
-            const uint32_t i0 = ins0(uint32_t(p), t0);
-            if ((i0 & po.lctrl) != po.lctrl) continue;
-            const uint32_t i1 = i0 | (1u << t0);
-            const V v0 = psi[i0], v1 = psi[i1];
-            const V w0 = cmadd(a00, v0, cmul(a01, v1)), w1 = cmadd(a10, v0, cmul(a11, v1));
-            psi[i0] = w0;
-            psi[i1] = w1;
-            V y0[3], y1[3];
-#pragma unroll
-            for (int an = 0; an < 3; ++an)
-                if (an < na && (op.grad_mask >> an & 1)) {
-                    y0[an] = cmadd(d[an][0], w0, cmul(d[an][1], w1));
-                    y1[an] = cmadd(d[an][2], w0, cmul(d[an][3], w1));
-                }
-#pragma unroll
-            for (int h = 0; h < NH; ++h) {
-                const V l0 = lam[h * TS + i0], l1 = lam[h * TS + i1];
-#pragma unroll
-                for (int an = 0; an < 3; ++an)
-                    if (an < na && (op.grad_mask >> an & 1))
-                        acc[an][h] += double(l0.x) * double(y0[an].x) + double(l0.y) * double(y0[an].y) +
-                                      double(l1.x) * double(y1[an].x) + double(l1.y) * double(y1[an].y);
-                lam[h * TS + i0] = cmadd(a00, l0, cmul(a01, l1));
-                lam[h * TS + i1] = cmadd(a10, l0, cmul(a11, l1));
-            }
-        }
-        return;
-    }
-    const int m = po.m;
-    const int nd = 1 << m;
-    int sorted[kMaxFusedM];
-    for (int k = 0; k < m; ++k) sorted[k] = po.lt[k];
-    for (int i = 1; i < m; ++i)
-        for (int j = i; j > 0 && sorted[j - 1] > sorted[j]; --j) {
-            const int tmp = sorted[j];
-            sorted[j] = sorted[j - 1];
-            sorted[j - 1] = tmp;
-        }
-    uint32_t off[8];
-    for (int r = 0; r < nd; ++r) {
-        uint32_t o = 0;
-        for (int k = 0; k < m; ++k)
-            if (r >> k & 1) o |= 1u << po.lt[k];
-        off[r] = o;
-    }
-    for (int p = threadIdx.x; p < (TS >> m); p += T) {
-        uint32_t i0 = uint32_t(p);
-        for (int k = 0; k < m; ++k) i0 = ins0(i0, sorted[k]);
-        if ((i0 & po.lctrl) != po.lctrl) continue;
-        V v[8], w[8];
-        for (int r = 0; r < nd; ++r) v[r] = psi[i0 | off[r]];
-        for (int r = 0; r < nd; ++r) {
-            V s = czero<V>();
-            for (int col = 0; col < nd; ++col) s = cmadd(cconj(M[col * nd + r]), v[col], s);
-            w[r] = s;
-        }
-        for (int r = 0; r < nd; ++r) psi[i0 | off[r]] = w[r];
-#pragma unroll
-        for (int an = 0; an < 3; ++an) {
-            if (!(an < na && (op.grad_mask >> an & 1))) continue;
-            const V *D = dM + an * nd * nd;
-            V y[8];
-            for (int r = 0; r < nd; ++r) {
-                V s = czero<V>();
-                for (int col = 0; col < nd; ++col) s = cmadd(D[r * nd + col], w[col], s);
-                y[r] = s;
-            }
-#pragma unroll
-            for (int h = 0; h < NH; ++h) {
-                double sacc = 0;
-                for (int r = 0; r < nd; ++r) {
-                    const V l = lam[h * TS + (i0 | off[r])];
-                    sacc += double(l.x) * double(y[r].x) + double(l.y) * double(y[r].y);
-                }
-                acc[an][h] += sacc;
-            }
-        }
-#pragma unroll
-        for (int h = 0; h < NH; ++h) {
-            V l[8];
-            for (int r = 0; r < nd; ++r) l[r] = lam[h * TS + (i0 | off[r])];
-            for (int r = 0; r < nd; ++r) {
-                V s = czero<V>();
-                for (int col = 0; col < nd; ++col) s = cmadd(cconj(M[col * nd + r]), l[col], s);
-                lam[h * TS + (i0 | off[r])] = s;
-            }
-        }
-    }
-}
-
-template <typename R, int NH>
-__global__ void __launch_bounds__(kThreads) fused_bwd_kernel(const BwdArgs<R> a) {
-    using V = cplx<R>;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const TileGeom &g = a.g;
-    const int K = g.K, c = g.c;
-    const int TS = 1 << K;
-    V *psi = reinterpret_cast<V *>(smem);
-    V *lam = psi + TS;
-    size_t o = align16(size_t(TS) * sizeof(V) * (1 + NH));
-    uint64_t *tab = reinterpret_cast<uint64_t *>(smem + o);
-    o = align16(o + (size_t(1) << (K - c)) * sizeof(uint64_t));
-    PassOp *sops = reinterpret_cast<PassOp *>(smem + o);
-    o = align16(o + size_t(a.n_pops) * sizeof(PassOp));
-    double *wacc = reinterpret_cast<double *>(smem + o);   // [warps][n_local_slots][NH]
-    const int nw = blockDim.x / 32;
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const int nls = a.n_local_slots;
-    build_table(tab, g);
-    for (int i = threadIdx.x; i < a.n_pops; i += blockDim.x) sops[i] = a.pops[i];
-    for (int i = threadIdx.x; i < nw * nls * NH; i += blockDim.x) wacc[i] = 0;
-    __syncthreads();
-    const int64_t n_tiles = int64_t(1) << g.n_out;
-    const int64_t dim = int64_t(1) << g.n;
-    const int64_t total = a.batch * n_tiles;
-    for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
-        const int64_t b = w >> g.n_out;
-        const uint64_t t = uint64_t(w) & uint64_t(n_tiles - 1);
-        const uint64_t base = tile_base(g, t);
-        load_tile(psi, a.psi_src + b * dim, base, tab, K, c);
-        for (int h = 0; h < NH; ++h) load_tile(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, K, c);
-        __syncthreads();
-        const V *mb = a.mats + b * a.mats_stride;
-        for (int k = a.n_pops - 1; k >= 0; --k) {
-            const PassOp &po = sops[k];
-            if ((base & po.octrl) != po.octrl) continue;
-            const DevOp &op = a.ops[po.op];
-            const V *M = op.per_sample ? mb + op.mat_off : a.cpool + op.mat_off;
-            const V *dM = mb + op.dmat_off;
-            double acc[3][NH];
-#pragma unroll
-            for (int an = 0; an < 3; ++an)
-#pragma unroll
-                for (int h = 0; h < NH; ++h) acc[an][h] = 0;
-            tile_bwd_op<V, NH>(psi, lam, K, po, op, M, dM, base, acc);
-            if (po.lslot >= 0) {
-                int r = 0;
-                for (int an = 0; an < op.n_angles; ++an) {
-                    if (!(op.grad_mask >> an & 1)) continue;
-#pragma unroll
-                    for (int h = 0; h < NH; ++h) {
-                        const double v = warp_sum(acc[an][h]);
-                        if (lane == 0) wacc[(warp * nls + po.lslot + r) * NH + h] += v;
-                    }
-                    ++r;
-                }
-            }
-            __syncthreads();
-        }
-        for (int h = 0; h < NH; ++h) store_tile(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, K, c);
-        if (a.psi_dst) store_tile(psi, a.psi_dst + b * dim, base, tab, K, c);
-        // flush the gradient partials when the next tile of this block belongs to another sample
-        const int64_t nxt = w + gridDim.x;
-        const bool flush = (nxt >= total) || ((nxt >> g.n_out) != b);
-        __syncthreads();
-        if (flush) {
-            for (int i = threadIdx.x; i < nls * NH; i += blockDim.x) {
-                double s = 0;
-                for (int ww = 0; ww < nw; ++ww) {
-                    s += wacc[ww * nls * NH + i];
-                    wacc[ww * nls * NH + i] = 0;
-                }
-                const int ls = i / NH, h = i % NH;
-                if (s != 0) atomicAdd(&a.gslots[(b * a.n_slots + a.slot_map[ls]) * a.n_hams + h], s);
-            }
-            __syncthreads();
-        }
-    }
-}
-
-template <typename R>
-cudaError_t launch_fused_bwd(const BwdArgs<R> &a, int sm_count, cudaStream_t s) {
-    if (a.g.c < 1 || a.g.K > kMaxTileBits || a.g.K < 1) return cudaErrorInvalidValue;  // 16-byte tile accesses need a contiguous low qubit
-    const size_t smem = fused_bwd_smem(a.g, a.n_pops, a.n_hams, a.n_local_slots, sizeof(cplx<R>));
-    const int64_t work = a.batch << a.g.n_out;
-#define MQB_BWD_CASE(NHV)                                                                                 \
-    case NHV: {                                                                                           \
-        auto kern = fused_bwd_kernel<R, NHV>;                                                             \
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-        if (e != cudaSuccess) return e;                                                                   \
-        kern<<<blocks_for(kern, smem, sm_count, work), kThreads, smem, s>>>(a);                           \
-        return cudaGetLastError();                                                                        \
-    }
-    switch (a.n_hams) {
-        MQB_BWD_CASE(1)
-        MQB_BWD_CASE(2)
-        MQB_BWD_CASE(3)
-        MQB_BWD_CASE(4)
-        default:
-            return cudaErrorInvalidValue;
-    }
-#undef MQB_BWD_CASE
 }
 
 // ------------------------------------------------------------------------------------------ Hamiltonian
@@ -1348,8 +957,6 @@ cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale
 // ------------------------------------------------------------------------------------------ instantiations
 #define MQB_INSTANTIATE(R)                                                                                         \
     template cudaError_t launch_matgen<R>(const MatgenArgs &, cudaStream_t);                                       \
-    template cudaError_t launch_fused_fwd<R>(const FwdArgs<R> &, int, cudaStream_t);                               \
-    template cudaError_t launch_fused_bwd<R>(const BwdArgs<R> &, int, cudaStream_t);                               \
     template cudaError_t launch_ham<R>(const HamArgs<R> &, int, cudaStream_t);                                     \
     template cudaError_t launch_plain_apply<R>(cplx<R> *, int, int64_t, const DevOp &, const cplx<R> *, int64_t,   \
                                                const cplx<R> *, bool, int, cudaStream_t);                          \

@@ -34,10 +34,13 @@ struct MatgenArgs {
 };
 
 template <typename R>
-struct FwdArgs {
+struct Fwd2Args {
     TileGeom g;
-    const PassOp *pops;
-    int n_pops;
+    const StageDesc *stages;
+    int n_stages;
+    const StageOp *sops;
+    int n_ops;
+    int reg_bits;
     const DevOp *ops;
     const cplx<R> *mats;
     int64_t mats_stride;
@@ -49,10 +52,13 @@ struct FwdArgs {
 };
 
 template <typename R>
-struct BwdArgs {
+struct Bwd2Args {
     TileGeom g;
-    const PassOp *pops;
-    int n_pops;
+    const StageDesc *stages;
+    int n_stages;
+    const StageOp *sops;
+    int n_ops;
+    int reg_bits;
     const DevOp *ops;
     const cplx<R> *mats;
     int64_t mats_stride;
@@ -88,9 +94,9 @@ struct HamArgs {
 template <typename R>
 cudaError_t launch_matgen(const MatgenArgs &a, cudaStream_t s);
 template <typename R>
-cudaError_t launch_fused_fwd(const FwdArgs<R> &a, int sm_count, cudaStream_t s);
+cudaError_t launch_fused_fwd2(const Fwd2Args<R> &a, int sm_count, cudaStream_t s);
 template <typename R>
-cudaError_t launch_fused_bwd(const BwdArgs<R> &a, int sm_count, cudaStream_t s);
+cudaError_t launch_fused_bwd2(const Bwd2Args<R> &a, int sm_count, cudaStream_t s);
 template <typename R>
 cudaError_t launch_ham(const HamArgs<R> &a, int sm_count, cudaStream_t s);
 template <typename R>
@@ -120,8 +126,8 @@ cudaError_t launch_one_prob(const cplx<R> *st, int n, int q, double *out, cudaSt
 template <typename R>
 cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale, cudaStream_t s);
 
-size_t fused_fwd_smem(const TileGeom &g, int n_pops, int elem_bytes);
-size_t fused_bwd_smem(const TileGeom &g, int n_pops, int n_hams, int n_local_slots, int elem_bytes);
+size_t fused2_smem(const TileGeom &g, int n_tiles_in_smem, int n_stages, int n_stage_ops, int n_local_slots,
+                   int n_hams, int elem_bytes, int threads);
 size_t ham_smem(const TileGeom &g, int elem_bytes);
 
 }  // namespace mqb

@@ -14,8 +14,8 @@
 
 namespace mqb {
 
-constexpr int kMaxFusedM = 3;        // dense gates with <= 3 targets run inside fused tiles
-constexpr int kMaxTileBits = 14;     // upper bound of the tile size 2^K
+constexpr int kMaxFusedM = 2;        // gates with <= 2 targets run inside fused tiles
+constexpr int kMaxTileBits = 13;     // upper bound of the tile size 2^K
 constexpr int kMaxPassOps = 256;     // ops of one fused pass (staged in shared memory)
 constexpr int kMaxPassSlots = 96;    // gradient slots of one fused pass (accumulated in shared memory)
 constexpr int kMaxGroupClasses = 64; // flip classes of one Hamiltonian pass
@@ -56,6 +56,32 @@ struct PassOp {
     uint64_t octrl;           // control bits outside the tile (global mask)
 };
 
+// A register stage of a fused pass: every thread holds 2^RB amplitudes of the tile in registers,
+// those whose tile-local index differs in the stage's register bits; the stage's gates act on
+// register bits only (diagonal gates may act on any bit).  Stages exchange data through the
+// tile in shared memory.
+constexpr int kMaxRegBits = 5;
+constexpr int kMaxThreadBits = 8;
+struct StageDesc {
+    int8_t rbits[kMaxRegBits];     // register position -> tile-local bit
+    int8_t tbits[kMaxThreadBits];  // thread-index bit -> tile-local bit
+    int8_t pad[3];
+    int32_t op_begin, op_end;      // range in Schedule::stage_ops
+};
+enum StageOpKind : int32_t { SK_DENSE1 = 0, SK_DENSE2 = 1, SK_DIAG1 = 2, SK_DIAG2 = 3 };
+struct StageOp {
+    int32_t op;          // program op index
+    int32_t kind;        // StageOpKind
+    int32_t p0, p1;      // dense: register positions of matrix bit 0 / bit 1
+    int32_t dsrc[2];     // diag target k: 0 register position, 1 thread (local bit), 2 outside (global qubit)
+    int32_t dval[2];     // position / local bit / global qubit
+    uint32_t rctrl;      // control bits among register positions
+    uint32_t tctrl;      // control bits among thread bits (tile-local mask)
+    uint64_t octrl;      // control bits outside the tile (global mask)
+    int32_t lslot;       // pass-local gradient slot of the first gradient angle (-1: none)
+    int32_t pad;
+};
+
 // A pass: one sweep over the state(s).
 struct Pass {
     int fused = 1;                 // 1: fused tile pass over ops [op_begin, op_end) of pass_ops; 0: single op
@@ -66,6 +92,9 @@ struct Pass {
     int op_begin = 0, op_end = 0;  // fused: range in Schedule::pass_ops; single: op index in op_begin
     int prog_op_begin = 0, prog_op_end = 0;  // program ops covered (execution order)
     int slot_begin = 0, n_slots = 0;         // fused: range in Schedule::slot_map (pass-local gradient slots)
+    int stage_begin = 0, n_stages = 0;       // fused: range in Schedule::stages
+    int sop_begin = 0, n_sops = 0;           // fused: range in Schedule::stage_ops (StageDesc ranges are relative)
+    int reg_bits = 0, thread_bits = 0;       // fused: registers / threads of the tile kernel
 };
 
 struct Schedule {
@@ -73,8 +102,12 @@ struct Schedule {
     std::vector<Pass> passes;
     std::vector<PassOp> pass_ops;
     std::vector<int32_t> slot_map;  // pass-local slot -> global gradient slot
+    std::vector<StageDesc> stages;
+    std::vector<StageOp> stage_ops;
     PassOp *d_pass_ops = nullptr;   // device copies
     int32_t *d_slot_map = nullptr;
+    StageDesc *d_stages = nullptr;
+    StageOp *d_stage_ops = nullptr;
 };
 
 // Kernel-facing description of a fused pass (passed by value).
@@ -107,12 +140,23 @@ struct HamGroup {
 
 // Builders (scheduler.cpp)
 Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool fuse);
+// Split every fused pass of `s` into register stages with `reg_bits` register bits per thread.
+void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int precision);
+inline uint32_t smem_swizzle(uint32_t L, int precision) {
+    // XOR-fold the index into its low 4 (complex64) / 3 (complex128) bits: linear over GF(2) and
+    // a bijection, so bank conflicts of the stage exchanges depend only on the thread bits' residues
+    if (precision == MQB_PREC_C64) return L ^ ((L >> 4) & 15u) ^ ((L >> 8) & 15u) ^ ((L >> 12) & 15u);
+    return L ^ ((L >> 3) & 7u) ^ ((L >> 6) & 7u) ^ ((L >> 9) & 7u) ^ ((L >> 12) & 7u);
+}
 void build_ham_groups(int n, int K, int c, const std::vector<uint64_t> &mx, const std::vector<uint64_t> &my,
                       const std::vector<uint64_t> &mz, const std::vector<int> &ny, const std::vector<double> &coeff,
                       std::vector<HamGroup> &groups, std::vector<HamClass> &classes, std::vector<HamTerm> &terms);
 TileGeom make_geom(int n, const std::vector<int> &qbits);
 int contiguity_bits(int precision);
 int default_tile_bits(int precision, int n_states_in_tile);
+// Register bits of the fused kernels: forward passes, and backward passes with n_hams lambdas.
+int fwd_reg_bits(int precision);
+int bwd_reg_bits(int precision, int n_hams);
 
 }  // namespace mqb
 

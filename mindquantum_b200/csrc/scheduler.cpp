@@ -21,6 +21,13 @@ static inline int popc(uint64_t x) { return __builtin_popcountll(x); }
 
 int contiguity_bits(int precision) { return precision == MQB_PREC_C64 ? 4 : 3; }
 
+int fwd_reg_bits(int precision) { return precision == MQB_PREC_C64 ? 5 : 4; }
+
+int bwd_reg_bits(int precision, int n_hams) {
+    if (n_hams <= 1) return precision == MQB_PREC_C64 ? 4 : 3;
+    return precision == MQB_PREC_C64 ? 3 : 2;
+}
+
 int default_tile_bits(int precision, int n_states_in_tile) {
     // keep the shared-memory tiles of all states at <= 64 KB so 2-3 blocks fit per SM
     const size_t amp = precision == MQB_PREC_C64 ? 8 : 16;
@@ -69,6 +76,7 @@ Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool
     // contiguity bit so 16-byte vector accesses never straddle two tile runs
     if (c > K - kMaxFusedM) c = std::max(1, K - kMaxFusedM);
     if (n > K && K < kMaxFusedM + 1) fuse = false;
+    if (K < 6) fuse = false;
     s.K = K;
     const int L = int(ops.size());
     std::vector<char> done(L, 0);
@@ -188,6 +196,138 @@ Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool
         s.passes.push_back(p);
     }
     return s;
+}
+
+// Greedy register-stage grouping of one fused pass (same blocking rule as the pass scan, over
+// tile-local bits), then padding of the register set and a bank-conflict-aware thread-bit order.
+void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int precision) {
+    s.stages.clear();
+    s.stage_ops.clear();
+    const int res_mod = precision == MQB_PREC_C64 ? 4 : 3;
+    for (Pass &p : s.passes) {
+        if (!p.fused) continue;
+        const int K = p.K;
+        // 2^TB threads (32..256) holding 2^RB amplitudes each
+        const int RB = std::max(1, std::min(reg_bits, K - 5));
+        const int TB = K - RB;
+        p.reg_bits = RB;
+        p.thread_bits = TB;
+        p.stage_begin = int(s.stages.size());
+        p.sop_begin = int(s.stage_ops.size());
+        const int npo = p.op_end - p.op_begin;
+        std::vector<char> done(npo, 0);
+        int n_done = 0;
+        while (n_done < npo) {
+            uint32_t R = 0, blocked = 0;
+            std::vector<int> members;
+            for (int i = 0; i < npo; ++i) {
+                if (done[i]) continue;
+                const PassOp &po = s.pass_ops[p.op_begin + i];
+                uint32_t touch = po.lctrl, dense = 0;
+                for (int k = 0; k < po.m; ++k)
+                    if (po.lt[k] >= 0) touch |= 1u << po.lt[k];
+                if (po.kind == KIND_DENSE) dense = touch & ~po.lctrl;
+                if (touch & blocked) {
+                    blocked |= touch;
+                    continue;
+                }
+                if (popc(R | dense) <= RB) {
+                    R |= dense;
+                    members.push_back(i);
+                } else {
+                    blocked |= touch;
+                }
+            }
+            // padding: add local bits so that the thread bits keep one bit of every residue class
+            auto thread_residue_count = [&](uint32_t Rm, int r) {
+                int cnt = 0;
+                for (int b = 0; b < K; ++b)
+                    if (!(Rm >> b & 1) && b % res_mod == r) ++cnt;
+                return cnt;
+            };
+            while (popc(R) < RB) {
+                int best = -1, best_score = -1;
+                for (int b = 0; b < K; ++b) {
+                    if (R >> b & 1) continue;
+                    const int score = thread_residue_count(R, b % res_mod);
+                    if (score > best_score) {
+                        best_score = score;
+                        best = b;
+                    }
+                }
+                R |= 1u << best;
+            }
+            StageDesc sd{};
+            std::vector<int> rl;
+            for (int b = 0; b < K; ++b)
+                if (R >> b & 1) rl.push_back(b);
+            // register positions: dense targets first in op order are not needed; ascending is fine
+            for (int i = 0; i < RB; ++i) sd.rbits[i] = int8_t(rl[i]);
+            std::vector<int> tl;
+            for (int b = 0; b < K; ++b)
+                if (!(R >> b & 1)) tl.push_back(b);
+            // lanes first: one thread bit of each residue class, then the rest ascending
+            std::vector<int> order;
+            std::vector<char> used(tl.size(), 0);
+            for (int r = 0; r < res_mod; ++r)
+                for (size_t i = 0; i < tl.size(); ++i)
+                    if (!used[i] && tl[i] % res_mod == r) {
+                        order.push_back(tl[i]);
+                        used[i] = 1;
+                        break;
+                    }
+            for (size_t i = 0; i < tl.size(); ++i)
+                if (!used[i]) order.push_back(tl[i]);
+            for (int i = 0; i < TB; ++i) sd.tbits[i] = int8_t(order[i]);
+            int pos_of[32];
+            for (int i = 0; i < 32; ++i) pos_of[i] = -1;
+            for (int i = 0; i < RB; ++i) pos_of[rl[i]] = i;
+            sd.op_begin = int(s.stage_ops.size()) - p.sop_begin;
+            for (int i : members) {
+                const PassOp &po = s.pass_ops[p.op_begin + i];
+                StageOp so{};
+                so.op = po.op;
+                so.lslot = po.lslot;
+                so.octrl = po.octrl;
+                so.rctrl = 0;
+                so.tctrl = 0;
+                for (int b = 0; b < K; ++b) {
+                    if (!(po.lctrl >> b & 1)) continue;
+                    if (pos_of[b] >= 0)
+                        so.rctrl |= 1u << pos_of[b];
+                    else
+                        so.tctrl |= 1u << b;
+                }
+                if (po.kind == KIND_DENSE) {
+                    so.kind = po.m == 1 ? SK_DENSE1 : SK_DENSE2;
+                    so.p0 = pos_of[po.lt[0]];
+                    so.p1 = po.m == 2 ? pos_of[po.lt[1]] : 0;
+                } else {
+                    so.kind = po.m == 1 ? SK_DIAG1 : SK_DIAG2;
+                    for (int k = 0; k < po.m; ++k) {
+                        if (po.lt[k] >= 0 && pos_of[po.lt[k]] >= 0) {
+                            so.dsrc[k] = 0;
+                            so.dval[k] = pos_of[po.lt[k]];
+                        } else if (po.lt[k] >= 0) {
+                            so.dsrc[k] = 1;
+                            so.dval[k] = po.lt[k];
+                        } else {
+                            so.dsrc[k] = 2;
+                            so.dval[k] = po.gt[k];
+                        }
+                    }
+                }
+                s.stage_ops.push_back(so);
+                done[i] = 1;
+                ++n_done;
+            }
+            sd.op_end = int(s.stage_ops.size()) - p.sop_begin;
+            s.stages.push_back(sd);
+        }
+        p.n_stages = int(s.stages.size()) - p.stage_begin;
+        p.n_sops = int(s.stage_ops.size()) - p.sop_begin;
+    }
+    (void)ops;
 }
 
 void build_ham_groups(int n, int K, int c, const std::vector<uint64_t> &mx, const std::vector<uint64_t> &my,
