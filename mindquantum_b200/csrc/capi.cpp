@@ -205,7 +205,7 @@ static void run_forward_pass(const mqb_program &p, const Schedule &s, const Pass
         a.sops = s.d_stage_ops + ps.sop_begin;
         a.n_ops = ps.n_sops;
         a.reg_bits = ps.reg_bits;
-        a.ops = p.d_ops;
+        a.mtab_entries = ps.mtab_entries;
         a.mats = mats;
         a.mats_stride = p.per_sample;
         a.cpool = cpool;
@@ -374,7 +374,7 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
             a.sops = s.d_stage_ops + ps.sop_begin;
             a.n_ops = ps.n_sops;
             a.reg_bits = ps.reg_bits;
-            a.ops = p.d_ops;
+            a.mtab_entries = ps.mtab_entries;
             a.mats = mats;
             a.mats_stride = p.per_sample;
             a.cpool = cpool;

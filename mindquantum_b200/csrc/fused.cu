@@ -401,6 +401,18 @@ __device__ __forceinline__ void bwd_dispatch2(V (&v)[1 << RB], V (&l)[NH][1 << R
 #undef MQB_B2
 }
 
+// Copy the matrices (and derivative matrices) of every gate of the pass into shared memory.
+template <typename V>
+__device__ __forceinline__ void load_mtab(V *mtab, const StageOp *sops, int n_ops, const V *mb, const V *cpool) {
+    // one warp per gate: the loads of different gates are in flight together
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int k = threadIdx.x >> 5; k < n_ops; k += nw) {
+        const StageOp &so = sops[k];
+        const V *src = (so.msrc_ps ? mb : cpool) + so.msrc;
+        for (int e = lane; e < so.mcount; e += 32) mtab[so.moff + e] = src[e];
+    }
+}
+
 template <int RB>
 __device__ __forceinline__ uint32_t reg_offset(int j, const uint32_t (&pr)[RB]) {
     uint32_t o = 0;
@@ -413,8 +425,10 @@ __device__ __forceinline__ uint32_t reg_offset(int j, const uint32_t (&pr)[RB]) 
 }  // namespace
 
 size_t fused2_smem(const TileGeom &g, int n_tiles_in_smem, int n_stages, int n_stage_ops, int n_local_slots,
-                   int n_hams, int elem_bytes, int threads) {
+                   int n_hams, int elem_bytes, int threads, int mtab_entries) {
     size_t s = (size_t(1) << g.K) * elem_bytes * n_tiles_in_smem;
+    s = (s + 15) & ~size_t(15);
+    s += size_t(mtab_entries) * elem_bytes;
     s = (s + 15) & ~size_t(15);
     s += (size_t(1) << (g.K - g.c)) * sizeof(uint64_t);
     s = (s + 15) & ~size_t(15);
@@ -436,6 +450,8 @@ __global__ void __launch_bounds__(256) fused_fwd2_kernel(const Fwd2Args<R> a) {
     const int TB = K - RB;
     V *tile = reinterpret_cast<V *>(smem);
     size_t o = align16((size_t(1) << K) * sizeof(V));
+    V *mtab = reinterpret_cast<V *>(smem + o);
+    o = align16(o + size_t(a.mtab_entries) * sizeof(V));
     uint64_t *tab = reinterpret_cast<uint64_t *>(smem + o);
     o = align16(o + (size_t(1) << (K - c)) * sizeof(uint64_t));
     StageDesc *sst = reinterpret_cast<StageDesc *>(smem + o);
@@ -448,16 +464,20 @@ __global__ void __launch_bounds__(256) fused_fwd2_kernel(const Fwd2Args<R> a) {
     const int64_t n_tiles = int64_t(1) << g.n_out;
     const int64_t dim = int64_t(1) << g.n;
     const int tid = threadIdx.x;
+    int64_t cached_b = -1;
     for (int64_t w = blockIdx.x; w < a.batch * n_tiles; w += gridDim.x) {
         const int64_t b = w >> g.n_out;
         const uint64_t t = uint64_t(w) & uint64_t(n_tiles - 1);
         const uint64_t base = tile_base(g, t);
+        if (b != cached_b) {
+            load_mtab(mtab, sops, a.n_ops, a.mats + b * a.mats_stride, a.cpool);
+            cached_b = b;
+        }
         if (a.src)
             stage_in(tile, a.src + b * a.src_batch_stride, base, tab, K, c);
         else
             stage_zero(tile, base, K);
         __syncthreads();
-        const V *mb = a.mats + b * a.mats_stride;
         for (int s = 0; s < a.n_stages; ++s) {
             const StageDesc &sd = sst[s];
             uint32_t Lt = 0;
@@ -474,8 +494,7 @@ __global__ void __launch_bounds__(256) fused_fwd2_kernel(const Fwd2Args<R> a) {
                 const StageOp &so = sops[k];
                 if ((base & so.octrl) != so.octrl) continue;
                 const bool on = (Lt & so.tctrl) == so.tctrl;
-                const DevOp &op = a.ops[so.op];
-                const V *M = op.per_sample ? mb + op.mat_off : a.cpool + op.mat_off;
+                const V *M = mtab + so.moff;
                 if (so.kind == SK_DENSE1) {
                     dispatch_dense1<V, RB, false>(v, so.p0, M, so.rctrl, on);
                 } else if (so.kind == SK_DENSE2) {
@@ -508,6 +527,8 @@ __global__ void __launch_bounds__(256) fused_bwd2_kernel(const Bwd2Args<R> a) {
     V *psi = reinterpret_cast<V *>(smem);
     V *lam = psi + TS;
     size_t o = align16(size_t(TS) * sizeof(V) * (1 + NH));
+    V *mtab = reinterpret_cast<V *>(smem + o);
+    o = align16(o + size_t(a.mtab_entries) * sizeof(V));
     uint64_t *tab = reinterpret_cast<uint64_t *>(smem + o);
     o = align16(o + (size_t(1) << (K - c)) * sizeof(uint64_t));
     StageDesc *sst = reinterpret_cast<StageDesc *>(smem + o);
@@ -527,15 +548,19 @@ __global__ void __launch_bounds__(256) fused_bwd2_kernel(const Bwd2Args<R> a) {
     const int64_t dim = int64_t(1) << g.n;
     const int64_t total = a.batch * n_tiles;
     const int tid = threadIdx.x;
+    int64_t cached_b = -1;
     for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
         const int64_t b = w >> g.n_out;
         const uint64_t t = uint64_t(w) & uint64_t(n_tiles - 1);
         const uint64_t base = tile_base(g, t);
+        if (b != cached_b) {
+            load_mtab(mtab, sops, a.n_ops, a.mats + b * a.mats_stride, a.cpool);
+            cached_b = b;
+        }
         stage_in(psi, a.psi_src + b * dim, base, tab, K, c);
 #pragma unroll
         for (int h = 0; h < NH; ++h) stage_in(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, K, c);
         __syncthreads();
-        const V *mb = a.mats + b * a.mats_stride;
         for (int s = a.n_stages - 1; s >= 0; --s) {
             const StageDesc &sd = sst[s];
             uint32_t Lt = 0;
@@ -558,30 +583,29 @@ __global__ void __launch_bounds__(256) fused_bwd2_kernel(const Bwd2Args<R> a) {
                 const StageOp &so = sops[k];
                 if ((base & so.octrl) != so.octrl) continue;   // uniform over the block
                 const bool on = (Lt & so.tctrl) == so.tctrl;
-                const DevOp &op = a.ops[so.op];
-                const V *M = op.per_sample ? mb + op.mat_off : a.cpool + op.mat_off;
-                const V *dM = mb + op.dmat_off;
-                const int na = op.grad_mask ? op.n_angles : 0;
+                const V *M = mtab + so.moff;
+                const V *dM = M + so.mat_size;
+                const int na = so.n_angles;
                 double acc[3][NH];
 #pragma unroll
                 for (int an = 0; an < 3; ++an)
 #pragma unroll
                     for (int h = 0; h < NH; ++h) acc[an][h] = 0;
                 if (so.kind == SK_DENSE1) {
-                    bwd_dispatch1<V, RB, NH>(v, l, so.p0, M, dM, na, op.grad_mask, so.rctrl, on, acc);
+                    bwd_dispatch1<V, RB, NH>(v, l, so.p0, M, dM, na, so.grad_mask, so.rctrl, on, acc);
                 } else if (so.kind == SK_DENSE2) {
                     const bool swap = so.p0 > so.p1;
                     V m[16];
                     load_mat4(m, M, swap);
                     bwd_dispatch2<V, RB, NH>(v, l, swap ? so.p1 : so.p0, swap ? so.p0 : so.p1, m, dM, swap, na,
-                                             op.grad_mask, so.rctrl, on, acc);
+                                             so.grad_mask, so.rctrl, on, acc);
                 } else {
-                    bwd_diag<V, RB, NH>(v, l, so, M, dM, na, op.grad_mask, Lt, base, on, acc);
+                    bwd_diag<V, RB, NH>(v, l, so, M, dM, na, so.grad_mask, Lt, base, on, acc);
                 }
                 if (so.lslot >= 0) {
                     int r = 0;
-                    for (int an = 0; an < op.n_angles; ++an) {
-                        if (!(op.grad_mask >> an & 1)) continue;
+                    for (int an = 0; an < so.n_angles; ++an) {
+                        if (!(so.grad_mask >> an & 1)) continue;
 #pragma unroll
                         for (int h = 0; h < NH; ++h) {
                             double x = 0;
@@ -641,7 +665,7 @@ cudaError_t launch_fused_fwd2(const Fwd2Args<R> &a, int sm_count, cudaStream_t s
     if (a.g.c < 1 || a.g.K > kMaxTileBits || RB < 1 || RB > kMaxRegBits || TB < 5 || TB > kMaxThreadBits)
         return cudaErrorInvalidValue;
     const int threads = 1 << TB;
-    const size_t smem = fused2_smem(a.g, 1, a.n_stages, a.n_ops, 0, 0, sizeof(cplx<R>), threads);
+    const size_t smem = fused2_smem(a.g, 1, a.n_stages, a.n_ops, 0, 0, sizeof(cplx<R>), threads, a.mtab_entries);
     const int64_t work = a.batch << a.g.n_out;
 #define MQB_F2(RBV)                                                                                         \
     case RBV: {                                                                                             \
@@ -668,7 +692,8 @@ cudaError_t launch_fused_bwd2(const Bwd2Args<R> &a, int sm_count, cudaStream_t s
         return cudaErrorInvalidValue;
     const int threads = 1 << TB;
     const size_t smem =
-        fused2_smem(a.g, 1 + a.n_hams, a.n_stages, a.n_ops, a.n_local_slots, a.n_hams, sizeof(cplx<R>), threads);
+        fused2_smem(a.g, 1 + a.n_hams, a.n_stages, a.n_ops, a.n_local_slots, a.n_hams, sizeof(cplx<R>), threads,
+                    a.mtab_entries);
     const int64_t work = a.batch << a.g.n_out;
 #define MQB_B2K(RBV, NHV)                                                                                   \
     case RBV * 8 + NHV: {                                                                                   \

@@ -41,7 +41,7 @@ struct Fwd2Args {
     const StageOp *sops;
     int n_ops;
     int reg_bits;
-    const DevOp *ops;
+    int mtab_entries;          // complex entries of the shared-memory matrix table
     const cplx<R> *mats;
     int64_t mats_stride;
     const cplx<R> *cpool;
@@ -59,7 +59,7 @@ struct Bwd2Args {
     const StageOp *sops;
     int n_ops;
     int reg_bits;
-    const DevOp *ops;
+    int mtab_entries;          // complex entries of the shared-memory matrix table
     const cplx<R> *mats;
     int64_t mats_stride;
     const cplx<R> *cpool;
@@ -127,7 +127,7 @@ template <typename R>
 cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale, cudaStream_t s);
 
 size_t fused2_smem(const TileGeom &g, int n_tiles_in_smem, int n_stages, int n_stage_ops, int n_local_slots,
-                   int n_hams, int elem_bytes, int threads);
+                   int n_hams, int elem_bytes, int threads, int mtab_entries);
 size_t ham_smem(const TileGeom &g, int elem_bytes);
 
 }  // namespace mqb

@@ -79,7 +79,14 @@ struct StageOp {
     uint32_t tctrl;      // control bits among thread bits (tile-local mask)
     uint64_t octrl;      // control bits outside the tile (global mask)
     int32_t lslot;       // pass-local gradient slot of the first gradient angle (-1: none)
-    int32_t pad;
+    int32_t n_angles;    // gradient angles of the gate when it has any, else 0
+    int32_t grad_mask;
+    int32_t mat_size;    // complex entries of one matrix (4 / 16 dense, 2 / 4 diagonal)
+    int32_t moff;        // offset of M in the pass's shared-memory matrix table (dM_a follows at moff + (1+a) mat_size)
+    int32_t mcount;      // entries copied into the table (M, then dM_0..)
+    int64_t msrc;        // source offset: per-sample block (msrc_ps) or constant pool
+    int32_t msrc_ps;     // 1: per-sample matrices, 0: constant pool
+    int32_t pad2;
 };
 
 // A pass: one sweep over the state(s).
@@ -94,6 +101,7 @@ struct Pass {
     int slot_begin = 0, n_slots = 0;         // fused: range in Schedule::slot_map (pass-local gradient slots)
     int stage_begin = 0, n_stages = 0;       // fused: range in Schedule::stages
     int sop_begin = 0, n_sops = 0;           // fused: range in Schedule::stage_ops (StageDesc ranges are relative)
+    int mtab_entries = 0;                    // fused: complex entries of the pass's shared-memory matrix table
     int reg_bits = 0, thread_bits = 0;       // fused: registers / threads of the tile kernel
 };
 

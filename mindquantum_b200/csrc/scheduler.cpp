@@ -214,6 +214,7 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
         p.thread_bits = TB;
         p.stage_begin = int(s.stages.size());
         p.sop_begin = int(s.stage_ops.size());
+        int mtab = 0;
         const int npo = p.op_end - p.op_begin;
         std::vector<char> done(npo, 0);
         int n_done = 0;
@@ -285,9 +286,18 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
             sd.op_begin = int(s.stage_ops.size()) - p.sop_begin;
             for (int i : members) {
                 const PassOp &po = s.pass_ops[p.op_begin + i];
+                const DevOp &dop = ops[po.op];
                 StageOp so{};
                 so.op = po.op;
                 so.lslot = po.lslot;
+                so.grad_mask = dop.grad_mask;
+                so.n_angles = dop.grad_mask ? dop.n_angles : 0;
+                so.mat_size = dop.mat_size;
+                so.moff = mtab;
+                so.mcount = dop.mat_size * (1 + so.n_angles);
+                so.msrc = dop.mat_off;
+                so.msrc_ps = dop.per_sample;
+                mtab += so.mcount;
                 so.octrl = po.octrl;
                 so.rctrl = 0;
                 so.tctrl = 0;
@@ -326,8 +336,8 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
         }
         p.n_stages = int(s.stages.size()) - p.stage_begin;
         p.n_sops = int(s.stage_ops.size()) - p.sop_begin;
+        p.mtab_entries = mtab;
     }
-    (void)ops;
 }
 
 void build_ham_groups(int n, int K, int c, const std::vector<uint64_t> &mx, const std::vector<uint64_t> &my,
