@@ -129,10 +129,12 @@ MQB_API int mqb_program_destroy(mqb_program *prog);
 MQB_API int mqb_program_get_info(const mqb_program *prog, mqb_program_info *info);
 /* Host-only, no CUDA call: the pass schedule the engine builds for a gate table.  Arrays hold
  * n_gates entries: order = gate indices in execution order, pass_of = pass of each executed gate,
- * qmask / fused = tile qubit mask and kind (1 fused tile pass, 0 single-gate pass) of each pass. */
+ * qmask / fused / n_stages = tile qubit mask, kind (1 fused tile pass, 0 single-gate pass) and
+ * register stages of each pass (n_stages may be NULL). */
 MQB_API int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, int n_gates,
                               const double *const_matrices, int64_t n_const_entries, int tile_bits, int fuse,
-                              int *n_passes, int32_t *order, int32_t *pass_of, uint64_t *qmask, int32_t *fused);
+                              int *n_passes, int32_t *order, int32_t *pass_of, uint64_t *qmask, int32_t *fused,
+                              int32_t *n_stages);
 /* Passes and tile bits of the schedule mqb_expectation_with_grad uses for n_hams Hamiltonians. */
 MQB_API int mqb_program_grad_passes(mqb_program *prog, int n_hams, int *n_passes, int *tile_bits);
 

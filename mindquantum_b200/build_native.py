@@ -60,7 +60,14 @@ def build(force=False, verbose=False):
         [_nvcc(), *ARCH, '-shared', '-cudart', 'static', '-ccbin', 'g++',
          *[os.path.join(bdir, o) for o in ('kernels.o', 'fused.o', 'capi.o', 'scheduler.o')], '-o', LIB + '.tmp'],
     ]
+    headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, 'mqb200.h')]
+    newest_header = max(os.path.getmtime(h) for h in headers)
     for cmd in steps:
+        out = cmd[cmd.index('-o') + 1]
+        if '-c' in cmd and not force and os.path.exists(out):
+            src = cmd[cmd.index('-c') + 1]
+            if os.path.getmtime(out) >= max(os.path.getmtime(src), newest_header):
+                continue   # object up to date
         if verbose:
             print(' '.join(cmd))
         res = subprocess.run(cmd, capture_output=True, text=True, env=env)

@@ -158,6 +158,9 @@ struct mqb_program {
 
 static std::unique_ptr<SchedDev> make_sched(const mqb_program &p, int K, bool fuse, int reg_bits) {
     auto sd = std::make_unique<SchedDev>();
+    // the register kernels need 2^5..2^8 threads of 2^reg_bits amplitudes: smaller registers use
+    // the per-gate kernels
+    if (K < reg_bits + 5) fuse = false;
     sd->s = build_schedule(p.n, K, contiguity_bits(p.precision), p.ops, fuse);
     build_stages(sd->s, p.ops, reg_bits, p.precision);
     sd->s.d_pass_ops = upload(sd->s.pass_ops);
@@ -473,6 +476,18 @@ static DevOp basic_op(const mqb_gate_desc &d, int k, int n_qubits, const mqb_par
         op.grad_mask = 0;
         op.kind = diag ? KIND_DIAG : KIND_DENSE;
         op.mat_size = diag ? dimm : dimm * dimm;
+        op.sub = SUB_GENERIC;
+        if (!diag && dimm == 2) {
+            bool real = true;
+            for (int e = 0; e < 4; ++e) real = real && m[2 * e + 1] == 0;
+            const bool anti = m[0] == 0 && m[1] == 0 && m[6] == 0 && m[7] == 0;
+            if (anti && m[2] == 1 && m[3] == 0 && m[4] == 1 && m[5] == 0)
+                op.sub = SUB_SWAP;
+            else if (anti)
+                op.sub = SUB_PERM;
+            else if (real)
+                op.sub = SUB_REAL;
+        }
         return op;
     }
     if (d.gate_id == GID_RPS) {
@@ -494,6 +509,7 @@ static DevOp basic_op(const mqb_gate_desc &d, int k, int n_qubits, const mqb_par
     } else {
         op.kind = KIND_DENSE;
         op.mat_size = 1 << (2 * d.n_obj);
+        if (d.gate_id == GID_RY) op.sub = SUB_REAL;   // RY and its derivative are real matrices
     }
     const int expect_obj =
         (d.gate_id == GID_RZZ || (d.gate_id >= GID_RXX && d.gate_id <= GID_SWAPALPHA) || d.gate_id == GID_FSIM) ? 2 : 1;
@@ -648,7 +664,7 @@ int mqb_program_create(int n_qubits, int precision, const mqb_gate_desc *gates, 
 
 int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, int n_gates, const double *const_matrices,
                       int64_t n_const_entries, int tile_bits, int fuse, int *n_passes, int32_t *order, int32_t *pass_of,
-                      uint64_t *qmask, int32_t *fused) {
+                      uint64_t *qmask, int32_t *fused, int32_t *n_stages) {
     return guarded([&] {
         if (n_qubits < 1 || n_qubits > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
         std::vector<DevOp> ops;
@@ -656,8 +672,9 @@ int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, i
             ops.push_back(basic_op(gates[k], k, n_qubits, nullptr, 0, 0, const_matrices, n_const_entries));
         const int rb = fwd_reg_bits(precision);
         int K = std::min(n_qubits, rb + 8);
-        if (tile_bits > 0) K = std::min(n_qubits, tile_bits);
-        Schedule s = build_schedule(n_qubits, K, contiguity_bits(precision), ops, fuse != 0);
+        if (tile_bits > 0) K = std::min(n_qubits, std::max(rb + 5, tile_bits));
+        Schedule s = build_schedule(n_qubits, K, contiguity_bits(precision), ops, fuse != 0 && K >= rb + 5);
+        build_stages(s, ops, rb, precision);
         int pos = 0;
         for (size_t pi = 0; pi < s.passes.size(); ++pi) {
             const Pass &ps = s.passes[pi];
@@ -665,6 +682,7 @@ int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, i
             for (int q : ps.qbits) qm |= uint64_t(1) << q;
             qmask[pi] = qm;
             fused[pi] = ps.fused;
+            if (n_stages) n_stages[pi] = ps.n_stages;
             if (ps.fused) {
                 for (int i = ps.op_begin; i < ps.op_end; ++i) {
                     order[pos] = s.pass_ops[i].op;

@@ -126,38 +126,119 @@ __device__ __forceinline__ void stage_out(const V *tile, V *dst, uint64_t base, 
 }
 
 // ----------------------------------------------------------------------------------- register ops
-// Forward / adjoint dense single-qubit gate on register position P.
-template <typename V, int RB, int P, bool ADJ>
-__device__ __forceinline__ void reg_dense1(V (&v)[1 << RB], const V *M, uint32_t rctrl, bool on) {
-    V m00 = M[0], m01 = M[1], m10 = M[2], m11 = M[3];
+// All register kernels index the thread's amplitude array with compile-time indices; the gate's
+// register position P is a template parameter reached through a switch.  CTRL selects the path
+// with controls among the register bits (rctrl != 0); the uncontrolled path has no predicates.
+template <typename V>
+__device__ __forceinline__ V rmul(float a, V x) {  // real scalar (float) times complex
+    V r;
+    r.x = a * x.x;
+    r.y = a * x.y;
+    return r;
+}
+template <typename V>
+__device__ __forceinline__ V rmul(double a, V x) {
+    V r;
+    r.x = a * x.x;
+    r.y = a * x.y;
+    return r;
+}
+template <typename V>
+__device__ __forceinline__ V rmadd(decltype(V::x) a, V x, V c) {  // a x + c, a real
+    V r;
+    r.x = fma(a, x.x, c.x);
+    r.y = fma(a, x.y, c.y);
+    return r;
+}
+
+// Matrix entries (row-major 2x2) of U or U^dag.
+template <typename V, bool ADJ>
+__device__ __forceinline__ void mat2(const V *M, V &m00, V &m01, V &m10, V &m11) {
     if (ADJ) {
-        const V t01 = m01;
-        m00 = cconj(m00);
-        m01 = cconj(m10);
-        m10 = cconj(t01);
-        m11 = cconj(m11);
-    }
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (j >> P & 1) continue;
-        constexpr int bit = 1 << P;
-        const bool act = on && ((uint32_t(j) & rctrl) == rctrl);
-        const V a = v[j], b = v[j | bit];
-        const V na = cmadd(m00, a, cmul(m01, b)), nb = cmadd(m10, a, cmul(m11, b));
-        v[j] = act ? na : a;
-        v[j | bit] = act ? nb : b;
+        m00 = cconj(M[0]);
+        m01 = cconj(M[2]);
+        m10 = cconj(M[1]);
+        m11 = cconj(M[3]);
+    } else {
+        m00 = M[0];
+        m01 = M[1];
+        m10 = M[2];
+        m11 = M[3];
     }
 }
 
-// Dense two-qubit gate on register positions P0 < P1; matrix index bit 0 <-> position of `lo_is_bit0`.
+template <typename V, int RB, int P, bool CTRL>
+__device__ __forceinline__ void fw_dense1(V (&v)[1 << RB], V m00, V m01, V m10, V m11, uint32_t rctrl) {
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (j >> P & 1) continue;
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
+        constexpr int bit = 1 << P;
+        const V a = v[j], b = v[j | bit];
+        v[j] = cmadd(m00, a, cmul(m01, b));
+        v[j | bit] = cmadd(m10, a, cmul(m11, b));
+    }
+}
+
+template <typename V, int RB, int P, bool CTRL>
+__device__ __forceinline__ void fw_real1(V (&v)[1 << RB], decltype(V::x) m00, decltype(V::x) m01,
+                                         decltype(V::x) m10, decltype(V::x) m11, uint32_t rctrl) {
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (j >> P & 1) continue;
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
+        constexpr int bit = 1 << P;
+        const V a = v[j], b = v[j | bit];
+        v[j] = rmadd(m00, a, rmul(m01, b));
+        v[j | bit] = rmadd(m10, a, rmul(m11, b));
+    }
+}
+
+template <typename V, int RB, int P, bool CTRL>
+__device__ __forceinline__ void fw_perm1(V (&v)[1 << RB], V m01, V m10, bool unit, uint32_t rctrl) {
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (j >> P & 1) continue;
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
+        constexpr int bit = 1 << P;
+        const V a = v[j], b = v[j | bit];
+        if (unit) {
+            v[j] = b;
+            v[j | bit] = a;
+        } else {
+            v[j] = cmul(m01, b);
+            v[j | bit] = cmul(m10, a);
+        }
+    }
+}
+
+template <typename V, int RB, int P, bool CTRL>
+__device__ __forceinline__ void fw_diag1(V (&v)[1 << RB], V d0, V d1, uint32_t rctrl) {
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
+        v[j] = cmul(v[j], (j >> P & 1) ? d1 : d0);
+    }
+}
+
+template <typename V, int RB, bool CTRL>
+__device__ __forceinline__ void fw_scale(V (&v)[1 << RB], V d, uint32_t rctrl) {
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
+        v[j] = cmul(v[j], d);
+    }
+}
+
+// Dense two-qubit gate on register positions P0 < P1 (matrix already in position order).
 template <typename V, int RB, int P0, int P1, bool ADJ>
-__device__ __forceinline__ void reg_dense2(V (&v)[1 << RB], const V (&m)[16], uint32_t rctrl, bool on) {
+__device__ __forceinline__ void reg_dense2(V (&v)[1 << RB], const V (&m)[16], uint32_t rctrl) {
 #pragma unroll
     for (int j = 0; j < (1 << RB); ++j) {
         if ((j >> P0 & 1) || (j >> P1 & 1)) continue;
-        const bool act = on && ((uint32_t(j) & rctrl) == rctrl);
+        if ((uint32_t(j) & rctrl) != rctrl) continue;
         const int id[4] = {j, j | (1 << P0), j | (1 << P1), j | (1 << P0) | (1 << P1)};
-        V x[4], y[4];
+        V x[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) x[r] = v[id[r]];
 #pragma unroll
@@ -167,10 +248,8 @@ __device__ __forceinline__ void reg_dense2(V (&v)[1 << RB], const V (&m)[16], ui
             s.y = 0;
 #pragma unroll
             for (int col = 0; col < 4; ++col) s = cmadd(ADJ ? cconj(m[col * 4 + r]) : m[r * 4 + col], x[col], s);
-            y[r] = s;
+            v[id[r]] = s;
         }
-#pragma unroll
-        for (int r = 0; r < 4; ++r) v[id[r]] = act ? y[r] : x[r];
     }
 }
 
@@ -187,33 +266,6 @@ __device__ __forceinline__ void load_mat4(V (&m)[16], const V *M, bool swap) {
         }
 }
 
-template <typename V, int RB, bool ADJ>
-__device__ __forceinline__ void dispatch_dense1(V (&v)[1 << RB], int p, const V *M, uint32_t rctrl, bool on) {
-    switch (p) {
-        case 0: reg_dense1<V, RB, 0, ADJ>(v, M, rctrl, on); break;
-        case 1: if constexpr (RB > 1) reg_dense1<V, RB, 1, ADJ>(v, M, rctrl, on); break;
-        case 2: if constexpr (RB > 2) reg_dense1<V, RB, 2, ADJ>(v, M, rctrl, on); break;
-        case 3: if constexpr (RB > 3) reg_dense1<V, RB, 3, ADJ>(v, M, rctrl, on); break;
-        case 4: if constexpr (RB > 4) reg_dense1<V, RB, 4, ADJ>(v, M, rctrl, on); break;
-        default: break;
-    }
-}
-
-template <typename V, int RB, bool ADJ>
-__device__ __forceinline__ void dispatch_dense2(V (&v)[1 << RB], int lo, int hi, const V (&m)[16], uint32_t rctrl,
-                                                bool on) {
-#define MQB_D2(A, B)                                                  \
-    case (A * 8 + B):                                                 \
-        if constexpr (RB > B) reg_dense2<V, RB, A, B, ADJ>(v, m, rctrl, on); \
-        break;
-    switch (lo * 8 + hi) {
-        MQB_D2(0, 1) MQB_D2(0, 2) MQB_D2(0, 3) MQB_D2(0, 4) MQB_D2(1, 2) MQB_D2(1, 3) MQB_D2(1, 4) MQB_D2(2, 3)
-        MQB_D2(2, 4) MQB_D2(3, 4)
-        default: break;
-    }
-#undef MQB_D2
-}
-
 template <typename V>
 __device__ __forceinline__ int diag_bit(int src, int val, int j, uint32_t Lt, uint64_t base) {
     if (src == 0) return (j >> val) & 1;
@@ -221,59 +273,139 @@ __device__ __forceinline__ int diag_bit(int src, int val, int j, uint32_t Lt, ui
     return int((base >> val) & 1u);
 }
 
-// Diagonal gate (one or two targets): v[j] *= d[index bits of j]
+// Diagonal gate with two targets (generic).
 template <typename V, int RB, bool ADJ>
-__device__ __forceinline__ void reg_diag(V (&v)[1 << RB], const StageOp &so, const V *D, uint32_t Lt, uint64_t base,
-                                         bool on) {
-    const bool two = so.kind == SK_DIAG2;
-    V d0 = D[0], d1 = D[1], d2 = d0, d3 = d1;
-    if (two) {
-        d2 = D[2];
-        d3 = D[3];
-    }
-    if (ADJ) {
-        d0 = cconj(d0);
-        d1 = cconj(d1);
-        d2 = cconj(d2);
-        d3 = cconj(d3);
-    }
+__device__ __forceinline__ void reg_diag2(V (&v)[1 << RB], const StageOp &so, const V *D, uint32_t Lt, uint64_t base) {
+    V d[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) d[r] = ADJ ? cconj(D[r]) : D[r];
 #pragma unroll
     for (int j = 0; j < (1 << RB); ++j) {
-        const bool act = on && ((uint32_t(j) & so.rctrl) == so.rctrl);
+        if ((uint32_t(j) & so.rctrl) != so.rctrl) continue;
         const int b0 = diag_bit<V>(so.dsrc[0], so.dval[0], j, Lt, base);
-        const int b1 = two ? diag_bit<V>(so.dsrc[1], so.dval[1], j, Lt, base) : 0;
-        const V d = b1 ? (b0 ? d3 : d2) : (b0 ? d1 : d0);
-        const V r = cmul(v[j], d);
-        v[j] = act ? r : v[j];
+        const int b1 = diag_bit<V>(so.dsrc[1], so.dval[1], j, Lt, base);
+        const V dd = b1 ? (b0 ? d[3] : d[2]) : (b0 ? d[1] : d[0]);
+        v[j] = cmul(v[j], dd);
     }
 }
 
-// Adjoint step of one gate on psi and lambda registers with FP64 gradient partials.
-template <typename V, int RB, int NH, int P>
-__device__ __forceinline__ void bwd_dense1(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M, const V *dM, int na,
-                                           int gmask, uint32_t rctrl, bool on, double (&acc)[3][NH]) {
-    const V a00 = cconj(M[0]), a01 = cconj(M[2]), a10 = cconj(M[1]), a11 = cconj(M[3]);
-    V d[3][4];
-#pragma unroll
-    for (int an = 0; an < 3; ++an)
-        if (an < na && (gmask >> an & 1))
-#pragma unroll
-            for (int e = 0; e < 4; ++e) d[an][e] = dM[an * 4 + e];
+#define MQB_POS_SWITCH(p, CALL5)  \
+    switch (p) {                  \
+        case 0: CALL5(0); break;  \
+        case 1: CALL5(1); break;  \
+        case 2: CALL5(2); break;  \
+        case 3: CALL5(3); break;  \
+        case 4: CALL5(4); break;  \
+        default: break;           \
+    }
+
+// One gate of a forward stage.
+template <typename V, int RB, bool ADJ>
+__device__ __forceinline__ void fwd_gate(V (&v)[1 << RB], const StageOp &so, const V *M, uint32_t Lt, uint64_t base) {
+    using R = decltype(V::x);
+    const bool ctrl = so.rctrl != 0;
+    switch (so.kind) {
+        case SK_DENSE1: {
+            V m00, m01, m10, m11;
+            mat2<V, ADJ>(M, m00, m01, m10, m11);
+#define MQB_C(P)                                                                                    \
+    if constexpr (RB > P) {                                                                         \
+        if (ctrl) fw_dense1<V, RB, P, true>(v, m00, m01, m10, m11, so.rctrl);                       \
+        else fw_dense1<V, RB, P, false>(v, m00, m01, m10, m11, so.rctrl);                           \
+    }
+            MQB_POS_SWITCH(so.p0, MQB_C)
+#undef MQB_C
+        } break;
+        case SK_REAL1: {
+            const R m00 = M[0].x, m11 = M[3].x;
+            const R m01 = ADJ ? M[2].x : M[1].x, m10 = ADJ ? M[1].x : M[2].x;
+#define MQB_C(P)                                                                                    \
+    if constexpr (RB > P) {                                                                         \
+        if (ctrl) fw_real1<V, RB, P, true>(v, m00, m01, m10, m11, so.rctrl);                        \
+        else fw_real1<V, RB, P, false>(v, m00, m01, m10, m11, so.rctrl);                            \
+    }
+            MQB_POS_SWITCH(so.p0, MQB_C)
+#undef MQB_C
+        } break;
+        case SK_PERM1:
+        case SK_SWAP1: {
+            const bool unit = so.kind == SK_SWAP1;
+            const V m01 = ADJ ? cconj(M[2]) : M[1], m10 = ADJ ? cconj(M[1]) : M[2];
+#define MQB_C(P)                                                                                    \
+    if constexpr (RB > P) {                                                                         \
+        if (ctrl) fw_perm1<V, RB, P, true>(v, m01, m10, unit, so.rctrl);                            \
+        else fw_perm1<V, RB, P, false>(v, m01, m10, unit, so.rctrl);                                \
+    }
+            MQB_POS_SWITCH(so.p0, MQB_C)
+#undef MQB_C
+        } break;
+        case SK_DIAG1: {
+            const V d0 = ADJ ? cconj(M[0]) : M[0], d1 = ADJ ? cconj(M[1]) : M[1];
+            if (so.dsrc[0] == 0) {
+#define MQB_C(P)                                                                                    \
+    if constexpr (RB > P) {                                                                         \
+        if (ctrl) fw_diag1<V, RB, P, true>(v, d0, d1, so.rctrl);                                    \
+        else fw_diag1<V, RB, P, false>(v, d0, d1, so.rctrl);                                        \
+    }
+                MQB_POS_SWITCH(so.dval[0], MQB_C)
+#undef MQB_C
+            } else {
+                const V d = diag_bit<V>(so.dsrc[0], so.dval[0], 0, Lt, base) ? d1 : d0;
+                if (ctrl)
+                    fw_scale<V, RB, true>(v, d, so.rctrl);
+                else
+                    fw_scale<V, RB, false>(v, d, so.rctrl);
+            }
+        } break;
+        case SK_DIAG2:
+            reg_diag2<V, RB, ADJ>(v, so, M, Lt, base);
+            break;
+        case SK_DENSE2: {
+            const bool swap = so.p0 > so.p1;
+            const int lo = swap ? so.p1 : so.p0, hi = swap ? so.p0 : so.p1;
+            V m[16];
+            load_mat4(m, M, swap);
+#define MQB_D2(A, B)                                                      \
+    case (A * 8 + B):                                                     \
+        if constexpr (RB > B) reg_dense2<V, RB, A, B, ADJ>(v, m, so.rctrl); \
+        break;
+            switch (lo * 8 + hi) {
+                MQB_D2(0, 1) MQB_D2(0, 2) MQB_D2(0, 3) MQB_D2(0, 4) MQB_D2(1, 2) MQB_D2(1, 3) MQB_D2(1, 4)
+                MQB_D2(2, 3) MQB_D2(2, 4) MQB_D2(3, 4)
+                default: break;
+            }
+#undef MQB_D2
+        } break;
+        default:
+            break;
+    }
+}
+
+// ------------------------------------------------------------------- adjoint step with gradients
+// psi <- U^dag psi, partial[a][h] += Re<lambda_h| dU_a |psi>, lambda_h <- U^dag lambda_h; the
+// partials of one gate accumulate in the state's precision over the thread's amplitudes and are
+// reduced in FP64 across threads.
+template <typename V, int RB, int NH, int P, bool CTRL>
+__device__ __forceinline__ void bw_dense1(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M, const V *dM, int gm,
+                                          uint32_t rctrl, decltype(V::x) (&acc)[3][NH]) {
+    V a00, a01, a10, a11;
+    mat2<V, true>(M, a00, a01, a10, a11);
 #pragma unroll
     for (int j = 0; j < (1 << RB); ++j) {
         if (j >> P & 1) continue;
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
         constexpr int bit = 1 << P;
-        const bool act = on && ((uint32_t(j) & rctrl) == rctrl);
-        if (!act) continue;
         const V w0 = cmadd(a00, v[j], cmul(a01, v[j | bit])), w1 = cmadd(a10, v[j], cmul(a11, v[j | bit]));
         v[j] = w0;
         v[j | bit] = w1;
 #pragma unroll
         for (int an = 0; an < 3; ++an) {
-            if (!(an < na && (gmask >> an & 1))) continue;
-            const V y0 = cmadd(d[an][0], w0, cmul(d[an][1], w1)), y1 = cmadd(d[an][2], w0, cmul(d[an][3], w1));
+            if (!(gm >> an & 1)) continue;
+            const V *d = dM + an * 4;
+            const V y0 = cmadd(d[0], w0, cmul(d[1], w1)), y1 = cmadd(d[2], w0, cmul(d[3], w1));
 #pragma unroll
-            for (int h = 0; h < NH; ++h) acc[an][h] += redot(l[h][j], y0) + redot(l[h][j | bit], y1);
+            for (int h = 0; h < NH; ++h)
+                acc[an][h] += l[h][j].x * y0.x + l[h][j].y * y0.y + l[h][j | bit].x * y1.x + l[h][j | bit].y * y1.y;
         }
 #pragma unroll
         for (int h = 0; h < NH; ++h) {
@@ -284,15 +416,91 @@ __device__ __forceinline__ void bwd_dense1(V (&v)[1 << RB], V (&l)[NH][1 << RB],
     }
 }
 
+template <typename V, int RB, int NH, int P, bool CTRL>
+__device__ __forceinline__ void bw_real1(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M, const V *dM, int gm,
+                                         uint32_t rctrl, decltype(V::x) (&acc)[3][NH]) {
+    using R = decltype(V::x);
+    const R a00 = M[0].x, a01 = M[2].x, a10 = M[1].x, a11 = M[3].x;   // U^dag = U^T
+    R d00 = 0, d01 = 0, d10 = 0, d11 = 0;
+    if (gm & 1) {
+        d00 = dM[0].x;
+        d01 = dM[1].x;
+        d10 = dM[2].x;
+        d11 = dM[3].x;
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (j >> P & 1) continue;
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
+        constexpr int bit = 1 << P;
+        const V w0 = rmadd(a00, v[j], rmul(a01, v[j | bit])), w1 = rmadd(a10, v[j], rmul(a11, v[j | bit]));
+        v[j] = w0;
+        v[j | bit] = w1;
+        if (gm & 1) {
+            const V y0 = rmadd(d00, w0, rmul(d01, w1)), y1 = rmadd(d10, w0, rmul(d11, w1));
+#pragma unroll
+            for (int h = 0; h < NH; ++h)
+                acc[0][h] += l[h][j].x * y0.x + l[h][j].y * y0.y + l[h][j | bit].x * y1.x + l[h][j | bit].y * y1.y;
+        }
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+            const V x0 = l[h][j], x1 = l[h][j | bit];
+            l[h][j] = rmadd(a00, x0, rmul(a01, x1));
+            l[h][j | bit] = rmadd(a10, x0, rmul(a11, x1));
+        }
+    }
+}
+
+template <typename V, int RB, int NH, int P, bool CTRL>
+__device__ __forceinline__ void bw_diag1(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M, const V *dM, int gm,
+                                         uint32_t rctrl, decltype(V::x) (&acc)[3][NH]) {
+    const V c0 = cconj(M[0]), c1 = cconj(M[1]);
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
+        const int b = j >> P & 1;
+        const V w = cmul(v[j], b ? c1 : c0);
+        v[j] = w;
+#pragma unroll
+        for (int an = 0; an < 3; ++an) {
+            if (!(gm >> an & 1)) continue;
+            const V y = cmul(dM[an * 2 + b], w);
+#pragma unroll
+            for (int h = 0; h < NH; ++h) acc[an][h] += l[h][j].x * y.x + l[h][j].y * y.y;
+        }
+#pragma unroll
+        for (int h = 0; h < NH; ++h) l[h][j] = cmul(l[h][j], b ? c1 : c0);
+    }
+}
+
+// diagonal gate whose target is constant over the thread's registers (thread or outside bit)
+template <typename V, int RB, int NH, bool CTRL>
+__device__ __forceinline__ void bw_scale(V (&v)[1 << RB], V (&l)[NH][1 << RB], V c, const V *dMb, int nd, int gm,
+                                         uint32_t rctrl, decltype(V::x) (&acc)[3][NH]) {
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (CTRL && (uint32_t(j) & rctrl) != rctrl) continue;
+        const V w = cmul(v[j], c);
+        v[j] = w;
+#pragma unroll
+        for (int an = 0; an < 3; ++an) {
+            if (!(gm >> an & 1)) continue;
+            const V y = cmul(dMb[an * nd], w);
+#pragma unroll
+            for (int h = 0; h < NH; ++h) acc[an][h] += l[h][j].x * y.x + l[h][j].y * y.y;
+        }
+#pragma unroll
+        for (int h = 0; h < NH; ++h) l[h][j] = cmul(l[h][j], c);
+    }
+}
+
 template <typename V, int RB, int NH, int P0, int P1>
-__device__ __forceinline__ void bwd_dense2(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V (&m)[16], const V *dMbase,
-                                           bool swap, int na, int gmask, uint32_t rctrl, bool on,
-                                           double (&acc)[3][NH]) {
+__device__ __forceinline__ void bw_dense2(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V (&m)[16], const V *dMbase,
+                                          bool swap, int gm, uint32_t rctrl, decltype(V::x) (&acc)[3][NH]) {
 #pragma unroll
     for (int j = 0; j < (1 << RB); ++j) {
         if ((j >> P0 & 1) || (j >> P1 & 1)) continue;
-        const bool act = on && ((uint32_t(j) & rctrl) == rctrl);
-        if (!act) continue;
+        if ((uint32_t(j) & rctrl) != rctrl) continue;
         const int id[4] = {j, j | (1 << P0), j | (1 << P1), j | (1 << P0) | (1 << P1)};
         V w[4];
 #pragma unroll
@@ -308,23 +516,19 @@ __device__ __forceinline__ void bwd_dense2(V (&v)[1 << RB], V (&l)[NH][1 << RB],
         for (int r = 0; r < 4; ++r) v[id[r]] = w[r];
 #pragma unroll
         for (int an = 0; an < 3; ++an) {
-            if (!(an < na && (gmask >> an & 1))) continue;
+            if (!(gm >> an & 1)) continue;
             V dm[16];
             load_mat4(dm, dMbase + an * 16, swap);
-            V y[4];
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                V s;
-                s.x = 0;
-                s.y = 0;
+                V y;
+                y.x = 0;
+                y.y = 0;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) s = cmadd(dm[r * 4 + c], w[c], s);
-                y[r] = s;
+                for (int c = 0; c < 4; ++c) y = cmadd(dm[r * 4 + c], w[c], y);
+#pragma unroll
+                for (int h = 0; h < NH; ++h) acc[an][h] += l[h][id[r]].x * y.x + l[h][id[r]].y * y.y;
             }
-#pragma unroll
-            for (int h = 0; h < NH; ++h)
-#pragma unroll
-                for (int r = 0; r < 4; ++r) acc[an][h] += redot(l[h][id[r]], y[r]);
         }
 #pragma unroll
         for (int h = 0; h < NH; ++h) {
@@ -345,27 +549,24 @@ __device__ __forceinline__ void bwd_dense2(V (&v)[1 << RB], V (&l)[NH][1 << RB],
 }
 
 template <typename V, int RB, int NH>
-__device__ __forceinline__ void bwd_diag(V (&v)[1 << RB], V (&l)[NH][1 << RB], const StageOp &so, const V *D,
-                                         const V *dM, int na, int gmask, uint32_t Lt, uint64_t base, bool on,
-                                         double (&acc)[3][NH]) {
-    const bool two = so.kind == SK_DIAG2;
-    const int nd = two ? 4 : 2;
+__device__ __forceinline__ void bw_diag2(V (&v)[1 << RB], V (&l)[NH][1 << RB], const StageOp &so, const V *D,
+                                         const V *dM, int gm, uint32_t Lt, uint64_t base,
+                                         decltype(V::x) (&acc)[3][NH]) {
 #pragma unroll
     for (int j = 0; j < (1 << RB); ++j) {
-        const bool act = on && ((uint32_t(j) & so.rctrl) == so.rctrl);
-        if (!act) continue;
+        if ((uint32_t(j) & so.rctrl) != so.rctrl) continue;
         const int b0 = diag_bit<V>(so.dsrc[0], so.dval[0], j, Lt, base);
-        const int b1 = two ? diag_bit<V>(so.dsrc[1], so.dval[1], j, Lt, base) : 0;
+        const int b1 = diag_bit<V>(so.dsrc[1], so.dval[1], j, Lt, base);
         const int r = b0 | (b1 << 1);
         const V dc = cconj(D[r]);
         const V w = cmul(dc, v[j]);
         v[j] = w;
 #pragma unroll
         for (int an = 0; an < 3; ++an) {
-            if (!(an < na && (gmask >> an & 1))) continue;
-            const V y = cmul(dM[an * nd + r], w);
+            if (!(gm >> an & 1)) continue;
+            const V y = cmul(dM[an * 4 + r], w);
 #pragma unroll
-            for (int h = 0; h < NH; ++h) acc[an][h] += redot(l[h][j], y);
+            for (int h = 0; h < NH; ++h) acc[an][h] += l[h][j].x * y.x + l[h][j].y * y.y;
         }
 #pragma unroll
         for (int h = 0; h < NH; ++h) l[h][j] = cmul(dc, l[h][j]);
@@ -373,32 +574,88 @@ __device__ __forceinline__ void bwd_diag(V (&v)[1 << RB], V (&l)[NH][1 << RB], c
 }
 
 template <typename V, int RB, int NH>
-__device__ __forceinline__ void bwd_dispatch1(V (&v)[1 << RB], V (&l)[NH][1 << RB], int p, const V *M, const V *dM,
-                                              int na, int gmask, uint32_t rctrl, bool on, double (&acc)[3][NH]) {
-    switch (p) {
-        case 0: bwd_dense1<V, RB, NH, 0>(v, l, M, dM, na, gmask, rctrl, on, acc); break;
-        case 1: if constexpr (RB > 1) bwd_dense1<V, RB, NH, 1>(v, l, M, dM, na, gmask, rctrl, on, acc); break;
-        case 2: if constexpr (RB > 2) bwd_dense1<V, RB, NH, 2>(v, l, M, dM, na, gmask, rctrl, on, acc); break;
-        case 3: if constexpr (RB > 3) bwd_dense1<V, RB, NH, 3>(v, l, M, dM, na, gmask, rctrl, on, acc); break;
-        case 4: if constexpr (RB > 4) bwd_dense1<V, RB, NH, 4>(v, l, M, dM, na, gmask, rctrl, on, acc); break;
-        default: break;
+__device__ __forceinline__ void bwd_gate(V (&v)[1 << RB], V (&l)[NH][1 << RB], const StageOp &so, const V *M,
+                                         uint32_t Lt, uint64_t base, decltype(V::x) (&acc)[3][NH]) {
+    const V *dM = M + so.mat_size;
+    const int gm = so.n_angles ? so.grad_mask : 0;
+    const bool ctrl = so.rctrl != 0;
+    switch (so.kind) {
+        case SK_DENSE1: {
+#define MQB_C(P)                                                                                    \
+    if constexpr (RB > P) {                                                                         \
+        if (ctrl) bw_dense1<V, RB, NH, P, true>(v, l, M, dM, gm, so.rctrl, acc);                    \
+        else bw_dense1<V, RB, NH, P, false>(v, l, M, dM, gm, so.rctrl, acc);                        \
     }
-}
-
-template <typename V, int RB, int NH>
-__device__ __forceinline__ void bwd_dispatch2(V (&v)[1 << RB], V (&l)[NH][1 << RB], int lo, int hi, const V (&m)[16],
-                                              const V *dM, bool swap, int na, int gmask, uint32_t rctrl, bool on,
-                                              double (&acc)[3][NH]) {
-#define MQB_B2(A, B)                                                                                \
-    case (A * 8 + B):                                                                               \
-        if constexpr (RB > B) bwd_dense2<V, RB, NH, A, B>(v, l, m, dM, swap, na, gmask, rctrl, on, acc); \
+            MQB_POS_SWITCH(so.p0, MQB_C)
+#undef MQB_C
+        } break;
+        case SK_REAL1: {
+#define MQB_C(P)                                                                                    \
+    if constexpr (RB > P) {                                                                         \
+        if (ctrl) bw_real1<V, RB, NH, P, true>(v, l, M, dM, gm, so.rctrl, acc);                     \
+        else bw_real1<V, RB, NH, P, false>(v, l, M, dM, gm, so.rctrl, acc);                         \
+    }
+            MQB_POS_SWITCH(so.p0, MQB_C)
+#undef MQB_C
+        } break;
+        case SK_PERM1:
+        case SK_SWAP1: {
+            // constant gates: no gradient, uncompute psi and every lambda
+            const bool unit = so.kind == SK_SWAP1;
+            const V m01 = cconj(M[2]), m10 = cconj(M[1]);
+#define MQB_C(P)                                                                                    \
+    if constexpr (RB > P) {                                                                         \
+        if (ctrl) {                                                                                 \
+            fw_perm1<V, RB, P, true>(v, m01, m10, unit, so.rctrl);                                  \
+            _Pragma("unroll") for (int h = 0; h < NH; ++h) fw_perm1<V, RB, P, true>(l[h], m01, m10, unit, so.rctrl); \
+        } else {                                                                                    \
+            fw_perm1<V, RB, P, false>(v, m01, m10, unit, so.rctrl);                                 \
+            _Pragma("unroll") for (int h = 0; h < NH; ++h) fw_perm1<V, RB, P, false>(l[h], m01, m10, unit, so.rctrl); \
+        }                                                                                           \
+    }
+            MQB_POS_SWITCH(so.p0, MQB_C)
+#undef MQB_C
+        } break;
+        case SK_DIAG1: {
+            if (so.dsrc[0] == 0) {
+#define MQB_C(P)                                                                                    \
+    if constexpr (RB > P) {                                                                         \
+        if (ctrl) bw_diag1<V, RB, NH, P, true>(v, l, M, dM, gm, so.rctrl, acc);                     \
+        else bw_diag1<V, RB, NH, P, false>(v, l, M, dM, gm, so.rctrl, acc);                         \
+    }
+                MQB_POS_SWITCH(so.dval[0], MQB_C)
+#undef MQB_C
+            } else {
+                const int b = diag_bit<V>(so.dsrc[0], so.dval[0], 0, Lt, base);
+                const V c = cconj(M[b]);
+                if (ctrl)
+                    bw_scale<V, RB, NH, true>(v, l, c, dM + b, 2, gm, so.rctrl, acc);
+                else
+                    bw_scale<V, RB, NH, false>(v, l, c, dM + b, 2, gm, so.rctrl, acc);
+            }
+        } break;
+        case SK_DIAG2:
+            bw_diag2<V, RB, NH>(v, l, so, M, dM, gm, Lt, base, acc);
+            break;
+        case SK_DENSE2: {
+            const bool swap = so.p0 > so.p1;
+            const int lo = swap ? so.p1 : so.p0, hi = swap ? so.p0 : so.p1;
+            V m[16];
+            load_mat4(m, M, swap);
+#define MQB_B2(A, B)                                                                          \
+    case (A * 8 + B):                                                                         \
+        if constexpr (RB > B) bw_dense2<V, RB, NH, A, B>(v, l, m, dM, swap, gm, so.rctrl, acc); \
         break;
-    switch (lo * 8 + hi) {
-        MQB_B2(0, 1) MQB_B2(0, 2) MQB_B2(0, 3) MQB_B2(0, 4) MQB_B2(1, 2) MQB_B2(1, 3) MQB_B2(1, 4) MQB_B2(2, 3)
-        MQB_B2(2, 4) MQB_B2(3, 4)
-        default: break;
-    }
+            switch (lo * 8 + hi) {
+                MQB_B2(0, 1) MQB_B2(0, 2) MQB_B2(0, 3) MQB_B2(0, 4) MQB_B2(1, 2) MQB_B2(1, 3) MQB_B2(1, 4)
+                MQB_B2(2, 3) MQB_B2(2, 4) MQB_B2(3, 4)
+                default: break;
+            }
 #undef MQB_B2
+        } break;
+        default:
+            break;
+    }
 }
 
 // Copy the matrices (and derivative matrices) of every gate of the pass into shared memory.
@@ -441,7 +698,7 @@ size_t fused2_smem(const TileGeom &g, int n_tiles_in_smem, int n_stages, int n_s
 }
 
 template <typename R, int RB>
-__global__ void __launch_bounds__(256) fused_fwd2_kernel(const Fwd2Args<R> a) {
+__global__ void __launch_bounds__(256, 2) fused_fwd2_kernel(const Fwd2Args<R> a) {
     using V = cplx<R>;
     constexpr int NR = 1 << RB;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -493,18 +750,8 @@ __global__ void __launch_bounds__(256) fused_fwd2_kernel(const Fwd2Args<R> a) {
             for (int k = sd.op_begin; k < sd.op_end; ++k) {
                 const StageOp &so = sops[k];
                 if ((base & so.octrl) != so.octrl) continue;
-                const bool on = (Lt & so.tctrl) == so.tctrl;
-                const V *M = mtab + so.moff;
-                if (so.kind == SK_DENSE1) {
-                    dispatch_dense1<V, RB, false>(v, so.p0, M, so.rctrl, on);
-                } else if (so.kind == SK_DENSE2) {
-                    const bool swap = so.p0 > so.p1;
-                    V m[16];
-                    load_mat4(m, M, swap);
-                    dispatch_dense2<V, RB, false>(v, swap ? so.p1 : so.p0, swap ? so.p0 : so.p1, m, so.rctrl, on);
-                } else {
-                    reg_diag<V, RB, false>(v, so, M, Lt, base, on);
-                }
+                if ((Lt & so.tctrl) != so.tctrl) continue;
+                fwd_gate<V, RB, false>(v, so, mtab + so.moff, Lt, base);
             }
 #pragma unroll
             for (int j = 0; j < NR; ++j) tile[pLt ^ reg_offset<RB>(j, pr)] = v[j];
@@ -516,7 +763,7 @@ __global__ void __launch_bounds__(256) fused_fwd2_kernel(const Fwd2Args<R> a) {
 }
 
 template <typename R, int RB, int NH>
-__global__ void __launch_bounds__(256) fused_bwd2_kernel(const Bwd2Args<R> a) {
+__global__ void __launch_bounds__(256, 2) fused_bwd2_kernel(const Bwd2Args<R> a) {
     using V = cplx<R>;
     constexpr int NR = 1 << RB;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -582,26 +829,12 @@ __global__ void __launch_bounds__(256) fused_bwd2_kernel(const Bwd2Args<R> a) {
             for (int k = sd.op_end - 1; k >= sd.op_begin; --k) {
                 const StageOp &so = sops[k];
                 if ((base & so.octrl) != so.octrl) continue;   // uniform over the block
-                const bool on = (Lt & so.tctrl) == so.tctrl;
-                const V *M = mtab + so.moff;
-                const V *dM = M + so.mat_size;
-                const int na = so.n_angles;
-                double acc[3][NH];
+                R acc[3][NH];
 #pragma unroll
                 for (int an = 0; an < 3; ++an)
 #pragma unroll
                     for (int h = 0; h < NH; ++h) acc[an][h] = 0;
-                if (so.kind == SK_DENSE1) {
-                    bwd_dispatch1<V, RB, NH>(v, l, so.p0, M, dM, na, so.grad_mask, so.rctrl, on, acc);
-                } else if (so.kind == SK_DENSE2) {
-                    const bool swap = so.p0 > so.p1;
-                    V m[16];
-                    load_mat4(m, M, swap);
-                    bwd_dispatch2<V, RB, NH>(v, l, swap ? so.p1 : so.p0, swap ? so.p0 : so.p1, m, dM, swap, na,
-                                             so.grad_mask, so.rctrl, on, acc);
-                } else {
-                    bwd_diag<V, RB, NH>(v, l, so, M, dM, na, so.grad_mask, Lt, base, on, acc);
-                }
+                if ((Lt & so.tctrl) == so.tctrl) bwd_gate<V, RB, NH>(v, l, so, mtab + so.moff, Lt, base, acc);
                 if (so.lslot >= 0) {
                     int r = 0;
                     for (int an = 0; an < so.n_angles; ++an) {
@@ -611,7 +844,7 @@ __global__ void __launch_bounds__(256) fused_bwd2_kernel(const Bwd2Args<R> a) {
                             double x = 0;
 #pragma unroll
                             for (int q = 0; q < 3; ++q)
-                                if (q == an) x = acc[q][h];
+                                if (q == an) x = double(acc[q][h]);
                             x = warp_sum(x);
                             if (lane == 0) wacc[(warp * nls + so.lslot + r) * NH + h] += x;
                         }
@@ -675,8 +908,9 @@ cudaError_t launch_fused_fwd2(const Fwd2Args<R> &a, int sm_count, cudaStream_t s
         kern<<<blocks_for2(kern, threads, smem, sm_count, work), threads, smem, s>>>(a);                    \
         return cudaGetLastError();                                                                          \
     }
+    // register bits used by the scheduler: 5 (complex64) / 4 (complex128)
     switch (RB) {
-        MQB_F2(1) MQB_F2(2) MQB_F2(3) MQB_F2(4) MQB_F2(5)
+        MQB_F2(sizeof(R) == 4 ? 5 : 4)
         default:
             return cudaErrorInvalidValue;
     }
@@ -703,11 +937,10 @@ cudaError_t launch_fused_bwd2(const Bwd2Args<R> &a, int sm_count, cudaStream_t s
         kern<<<blocks_for2(kern, threads, smem, sm_count, work), threads, smem, s>>>(a);                    \
         return cudaGetLastError();                                                                          \
     }
+    // register bits used by the scheduler: one lambda 4 (complex64) / 3 (complex128), more lambdas 3 / 2
+    constexpr int RB1 = sizeof(R) == 4 ? 4 : 3, RBN = sizeof(R) == 4 ? 3 : 2;
     switch (RB * 8 + a.n_hams) {
-        MQB_B2K(1, 1) MQB_B2K(2, 1) MQB_B2K(3, 1) MQB_B2K(4, 1)
-        MQB_B2K(1, 2) MQB_B2K(2, 2) MQB_B2K(3, 2) MQB_B2K(4, 2)
-        MQB_B2K(1, 3) MQB_B2K(2, 3) MQB_B2K(3, 3)
-        MQB_B2K(1, 4) MQB_B2K(2, 4) MQB_B2K(3, 4)
+        MQB_B2K(RB1, 1) MQB_B2K(RBN, 2) MQB_B2K(RBN, 3) MQB_B2K(RBN, 4)
         default:
             return cudaErrorInvalidValue;
     }

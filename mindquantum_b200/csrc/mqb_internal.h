@@ -41,8 +41,10 @@ struct DevOp {
     int32_t custom_off;          // GID_CUSTOM: offset of M in the caller's per-sample custom block
     uint64_t px, py, pz;         // GID_RPS masks
     int32_t pny;
-    int32_t pad;
+    int32_t sub;                 // dense single-qubit structure: SUB_GENERIC, SUB_REAL, SUB_PERM, SUB_SWAP
 };
+// Structure of a dense single-qubit matrix, used to pick a cheaper register kernel.
+enum DenseSub : int32_t { SUB_GENERIC = 0, SUB_REAL = 1, SUB_PERM = 2, SUB_SWAP = 3 };
 
 // An op as seen inside one fused pass (targets remapped to tile-local bits).
 struct PassOp {
@@ -68,7 +70,7 @@ struct StageDesc {
     int8_t pad[3];
     int32_t op_begin, op_end;      // range in Schedule::stage_ops
 };
-enum StageOpKind : int32_t { SK_DENSE1 = 0, SK_DENSE2 = 1, SK_DIAG1 = 2, SK_DIAG2 = 3 };
+enum StageOpKind : int32_t { SK_DENSE1 = 0, SK_DENSE2 = 1, SK_DIAG1 = 2, SK_DIAG2 = 3, SK_REAL1 = 4, SK_PERM1 = 5, SK_SWAP1 = 6 };
 struct StageOp {
     int32_t op;          // program op index
     int32_t kind;        // StageOpKind

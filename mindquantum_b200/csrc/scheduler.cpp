@@ -207,8 +207,8 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
     for (Pass &p : s.passes) {
         if (!p.fused) continue;
         const int K = p.K;
-        // 2^TB threads (32..256) holding 2^RB amplitudes each
-        const int RB = std::max(1, std::min(reg_bits, K - 5));
+        // 2^TB threads (32..256) holding 2^RB amplitudes each; passes are only fused when K >= reg_bits + 5
+        const int RB = reg_bits;
         const int TB = K - RB;
         p.reg_bits = RB;
         p.thread_bits = TB;
@@ -310,6 +310,9 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
                 }
                 if (po.kind == KIND_DENSE) {
                     so.kind = po.m == 1 ? SK_DENSE1 : SK_DENSE2;
+                    if (po.m == 1 && dop.sub == SUB_REAL) so.kind = SK_REAL1;
+                    if (po.m == 1 && dop.sub == SUB_PERM) so.kind = SK_PERM1;
+                    if (po.m == 1 && dop.sub == SUB_SWAP) so.kind = SK_SWAP1;
                     so.p0 = pos_of[po.lt[0]];
                     so.p1 = po.m == 2 ? pos_of[po.lt[1]] : 0;
                 } else {

@@ -186,12 +186,14 @@ def plan_schedule(circuit, n_qubits, precision, tile_bits=0, fuse=True):
     pass_of = np.zeros(max(1, n), np.int32)
     qmask = np.zeros(max(1, n), np.uint64)
     fused = np.zeros(max(1, n), np.int32)
+    stages = np.zeros(max(1, n), np.int32)
     n_passes = ctypes.c_int()
     N.call('mqb_plan_schedule', n_qubits, precision, gate_arr, n, pool_f.ctypes.data_as(ctypes.c_void_p),
            pool_arr.size, tile_bits, 1 if fuse else 0, ctypes.byref(n_passes), order.ctypes.data_as(ctypes.c_void_p),
            pass_of.ctypes.data_as(ctypes.c_void_p), qmask.ctypes.data_as(ctypes.c_void_p),
-           fused.ctypes.data_as(ctypes.c_void_p))
+           fused.ctypes.data_as(ctypes.c_void_p), stages.ctypes.data_as(ctypes.c_void_p))
     k = n_passes.value
+    plan_schedule.last_stages = stages[:k]
     return order[:n], pass_of[:n], qmask[:k], fused[:k]
 
 

@@ -106,9 +106,10 @@ def test_schedule_is_a_valid_reordering(n, K, prec):
         if not fused[p]:
             continue
         qm = int(qmask[p])
-        kk = min(K, n)
+        rb = 5 if prec == 0 else 4           # register bits of the forward tile kernel
+        kk = min(n, max(K, rb + 5))
         assert bin(qm).count('1') == kk
-        ce = kk if n <= K else min(c_bits, max(0, K - 3))
+        ce = kk if n <= kk else min(c_bits, max(1, kk - 2))
         assert qm & ((1 << ce) - 1) == (1 << ce) - 1
         dense, _ = _targets_and_touched(gates[gi])
         for q in dense:
@@ -155,13 +156,13 @@ def test_invalid_gate_tables_are_rejected_on_the_host():
     out = [np.zeros(1, np.int32), np.zeros(1, np.int32), np.zeros(1, np.uint64), np.zeros(1, np.int32)]
     n_p = ctypes.c_int()
     st = N.lib().mqb_plan_schedule(4, 0, arr, 1, None, 0, 0, 1, ctypes.byref(n_p),
-                                   *[o.ctypes.data_as(ctypes.c_void_p) for o in out])
+                                   *[o.ctypes.data_as(ctypes.c_void_p) for o in out], None)
     assert st == -1 and b'out of range' in N.lib().mqb_last_error()
     d.obj[0] = 1
     d.ctrl_mask = 2
     arr = (N.GateDesc * 1)(d)
     st = N.lib().mqb_plan_schedule(4, 0, arr, 1, None, 0, 0, 1, ctypes.byref(n_p),
-                                   *[o.ctypes.data_as(ctypes.c_void_p) for o in out])
+                                   *[o.ctypes.data_as(ctypes.c_void_p) for o in out], None)
     assert st == -1 and b'overlap' in N.lib().mqb_last_error()
 
 
