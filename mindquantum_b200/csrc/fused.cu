@@ -908,9 +908,12 @@ cudaError_t launch_fused_fwd2(const Fwd2Args<R> &a, int sm_count, cudaStream_t s
         kern<<<blocks_for2(kern, threads, smem, sm_count, work), threads, smem, s>>>(a);                    \
         return cudaGetLastError();                                                                          \
     }
-    // register bits used by the scheduler: 5 (complex64) / 4 (complex128)
+    // register bits used by the scheduler: apply passes 5 (complex64) / 4 (complex128); the forward
+    // passes of a gradient run with the backward layout (4, 3 / 3, 2)
     switch (RB) {
         MQB_F2(sizeof(R) == 4 ? 5 : 4)
+        MQB_F2(sizeof(R) == 4 ? 4 : 3)
+        MQB_F2(sizeof(R) == 4 ? 3 : 2)
         default:
             return cudaErrorInvalidValue;
     }
