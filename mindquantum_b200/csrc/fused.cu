@@ -75,22 +75,32 @@ __device__ __forceinline__ void build_table(uint64_t *tab, const TileGeom &g) {
     }
 }
 
-// global (coalesced 16-byte vectors) -> swizzled shared tile
-template <typename V>
-__device__ __forceinline__ void stage_in(V *tile, const V *src, uint64_t base, const uint64_t *tab, int K, int c) {
+// global (coalesced 16-byte vectors) -> swizzled shared tile.  Every thread moves NV vectors;
+// all of its global loads are issued before the first shared store so their latencies overlap.
+template <typename V, int NV>
+__device__ __forceinline__ void stage_in(V *tile, const V *src, uint64_t base, const uint64_t *tab, int c) {
     constexpr int APV = 16 / sizeof(V);
-    const int nvec = (1 << K) / APV;
+    constexpr int CH = NV < 8 ? NV : 8;   // vectors in flight per thread (bounded register use)
     const uint32_t lowmask = (1u << c) - 1u;
-    for (int v = threadIdx.x; v < nvec; v += blockDim.x) {
-        const uint32_t L = uint32_t(v) * APV;
-        const uint64_t gi = base + tab[L >> c] + (L & lowmask);
-        const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(src + gi));
-        if (APV == 2) {
-            const V *pv = reinterpret_cast<const V *>(&raw);
-            tile[swz<V>(L)] = pv[0];
-            tile[swz<V>(L + 1)] = pv[1];
-        } else {
-            *reinterpret_cast<uint4 *>(&tile[swz<V>(L)]) = raw;
+#pragma unroll
+    for (int i0 = 0; i0 < NV; i0 += CH) {
+        uint4 buf[CH];
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+            const uint32_t L = (threadIdx.x + uint32_t(i0 + i) * blockDim.x) * APV;
+            const uint64_t gi = base + tab[L >> c] + (L & lowmask);
+            buf[i] = __ldcs(reinterpret_cast<const uint4 *>(src + gi));
+        }
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+            const uint32_t L = (threadIdx.x + uint32_t(i0 + i) * blockDim.x) * APV;
+            if (APV == 2) {
+                const V *pv = reinterpret_cast<const V *>(&buf[i]);
+                tile[swz<V>(L)] = pv[0];
+                tile[swz<V>(L + 1)] = pv[1];
+            } else {
+                *reinterpret_cast<uint4 *>(&tile[swz<V>(L)]) = buf[i];
+            }
         }
     }
 }
@@ -105,13 +115,13 @@ __device__ __forceinline__ void stage_zero(V *tile, uint64_t base, int K) {
     }
 }
 
-template <typename V>
-__device__ __forceinline__ void stage_out(const V *tile, V *dst, uint64_t base, const uint64_t *tab, int K, int c) {
+template <typename V, int NV>
+__device__ __forceinline__ void stage_out(const V *tile, V *dst, uint64_t base, const uint64_t *tab, int c) {
     constexpr int APV = 16 / sizeof(V);
-    const int nvec = (1 << K) / APV;
     const uint32_t lowmask = (1u << c) - 1u;
-    for (int v = threadIdx.x; v < nvec; v += blockDim.x) {
-        const uint32_t L = uint32_t(v) * APV;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        const uint32_t L = (threadIdx.x + uint32_t(i) * blockDim.x) * APV;
         const uint64_t gi = base + tab[L >> c] + (L & lowmask);
         uint4 raw;
         if (APV == 2) {
@@ -121,7 +131,7 @@ __device__ __forceinline__ void stage_out(const V *tile, V *dst, uint64_t base, 
         } else {
             raw = *reinterpret_cast<const uint4 *>(&tile[swz<V>(L)]);
         }
-        *reinterpret_cast<uint4 *>(dst + gi) = raw;
+        __stcs(reinterpret_cast<uint4 *>(dst + gi), raw);
     }
 }
 
@@ -701,6 +711,7 @@ template <typename R, int RB>
 __global__ void __launch_bounds__(256, 2) fused_fwd2_kernel(const Fwd2Args<R> a) {
     using V = cplx<R>;
     constexpr int NR = 1 << RB;
+    constexpr int NV = NR / (16 / int(sizeof(V)));   // 16-byte vectors per thread per tile
     extern __shared__ __align__(16) unsigned char smem[];
     const TileGeom &g = a.g;
     const int K = g.K, c = g.c;
@@ -731,7 +742,7 @@ __global__ void __launch_bounds__(256, 2) fused_fwd2_kernel(const Fwd2Args<R> a)
             cached_b = b;
         }
         if (a.src)
-            stage_in(tile, a.src + b * a.src_batch_stride, base, tab, K, c);
+            stage_in<V, NV>(tile, a.src + b * a.src_batch_stride, base, tab, c);
         else
             stage_zero(tile, base, K);
         __syncthreads();
@@ -757,15 +768,16 @@ __global__ void __launch_bounds__(256, 2) fused_fwd2_kernel(const Fwd2Args<R> a)
             for (int j = 0; j < NR; ++j) tile[pLt ^ reg_offset<RB>(j, pr)] = v[j];
             __syncthreads();
         }
-        stage_out(tile, a.dst + b * dim, base, tab, K, c);
+        stage_out<V, NV>(tile, a.dst + b * dim, base, tab, c);
         __syncthreads();
     }
 }
 
 template <typename R, int RB, int NH>
-__global__ void __launch_bounds__(256, 2) fused_bwd2_kernel(const Bwd2Args<R> a) {
+__global__ void __launch_bounds__(256, 1) fused_bwd2_kernel(const Bwd2Args<R> a) {
     using V = cplx<R>;
     constexpr int NR = 1 << RB;
+    constexpr int NV = NR / (16 / int(sizeof(V)));   // 16-byte vectors per thread per tile
     extern __shared__ __align__(16) unsigned char smem[];
     const TileGeom &g = a.g;
     const int K = g.K, c = g.c;
@@ -804,9 +816,9 @@ __global__ void __launch_bounds__(256, 2) fused_bwd2_kernel(const Bwd2Args<R> a)
             load_mtab(mtab, sops, a.n_ops, a.mats + b * a.mats_stride, a.cpool);
             cached_b = b;
         }
-        stage_in(psi, a.psi_src + b * dim, base, tab, K, c);
+        stage_in<V, NV>(psi, a.psi_src + b * dim, base, tab, c);
 #pragma unroll
-        for (int h = 0; h < NH; ++h) stage_in(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, K, c);
+        for (int h = 0; h < NH; ++h) stage_in<V, NV>(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, c);
         __syncthreads();
         for (int s = a.n_stages - 1; s >= 0; --s) {
             const StageDesc &sd = sst[s];
@@ -862,8 +874,8 @@ __global__ void __launch_bounds__(256, 2) fused_bwd2_kernel(const Bwd2Args<R> a)
             __syncthreads();
         }
 #pragma unroll
-        for (int h = 0; h < NH; ++h) stage_out(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, K, c);
-        if (a.psi_dst) stage_out(psi, a.psi_dst + b * dim, base, tab, K, c);
+        for (int h = 0; h < NH; ++h) stage_out<V, NV>(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, c);
+        if (a.psi_dst) stage_out<V, NV>(psi, a.psi_dst + b * dim, base, tab, c);
         const int64_t nxt = w + gridDim.x;
         const bool flush = (nxt >= total) || ((nxt >> g.n_out) != b);
         __syncthreads();
