@@ -141,6 +141,17 @@ MQB_API int mqb_program_grad_passes(mqb_program *prog, int n_hams, int *n_passes
 /* Workspace (bytes) that mqb_apply needs for `batch` samples. */
 MQB_API int mqb_apply_workspace_size(const mqb_program *prog, int64_t batch, size_t *bytes);
 
+/* The same as mqb_apply, without a workspace argument and without allocating: for callers that
+ * cannot allocate device memory while they apply a circuit (a framework recording a CUDA graph
+ * that forbids allocations during capture, a runtime whose device memory is a fixed pool, a thin
+ * binding that only owns the state buffers).  No counterpart in the reference.  The gate matrices
+ * go to a fixed 4 MiB array inside the library (held on every GPU that loads it until exit);
+ * batches whose matrices need more are rejected with MQB_ERR_WORKSPACE.  The first call on a
+ * device looks the array up and should come before any stream capture.  All calls share the
+ * array, so calls whose work overlaps on the GPU race. */
+MQB_API int mqb_apply_static(mqb_program *prog, void *states, int64_t batch, const double *params,
+                             int64_t param_stride, const double *custom, void *stream);
+
 /* Apply the program in place to `batch` states.  params: device [batch][n_params] float64
  * (row stride param_stride, 0 = broadcast one row); custom: device [batch][custom_entries]
  * complex128 (NULL if the program has no custom parameterized gate). */

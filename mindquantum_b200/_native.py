@@ -80,6 +80,7 @@ SIGNATURES = {
     'mqb_program_grad_passes': [_P, _I, _P, _P],
     'mqb_apply_workspace_size': [_P, _I64, _P],
     'mqb_apply': [_P, _P, _I64, _P, _I64, _P, _P, _SZ, _P],
+    'mqb_apply_static': [_P, _P, _I64, _P, _I64, _P, _P],
     'mqb_ham_create': [_I, _I, _P, _P, _P, _P, _P, _I, _P],
     'mqb_ham_destroy': [_P],
     'mqb_apply_hamiltonian': [_P, _P, _P, _I64, _P],

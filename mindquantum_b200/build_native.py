@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
 LIB = os.path.join(HERE, 'libmqb200.so')
-SOURCES = ['kernels.cu', 'fused.cu', 'capi.cpp', 'scheduler.cpp']
+SOURCES = ['kernels.cu', 'fused.cu', 'capi.cpp', 'scheduler.cpp', 'noalloc.cu']
 HEADERS = ['kernels.cuh', 'mqb_internal.h', 'mqb_gate_ids.h']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
@@ -55,10 +55,12 @@ def build(force=False, verbose=False):
          '-o', os.path.join(bdir, 'fused.o')],
         [_nvcc(), *ARCH, '-lineinfo', *common, '-x', 'cu', '-c', os.path.join(CSRC, 'capi.cpp'),
          '-o', os.path.join(bdir, 'capi.o')],
+        [_nvcc(), *ARCH, '-lineinfo', *common, '-c', os.path.join(CSRC, 'noalloc.cu'),
+         '-o', os.path.join(bdir, 'noalloc.o')],
         [_nvcc(), *common, '-x', 'c++', '-c', os.path.join(CSRC, 'scheduler.cpp'),
          '-o', os.path.join(bdir, 'scheduler.o')],
         [_nvcc(), *ARCH, '-shared', '-cudart', 'static', '-ccbin', 'g++',
-         *[os.path.join(bdir, o) for o in ('kernels.o', 'fused.o', 'capi.o', 'scheduler.o')], '-o', LIB + '.tmp'],
+         *[os.path.join(bdir, o) for o in ('kernels.o', 'fused.o', 'capi.o', 'scheduler.o', 'noalloc.o')], '-o', LIB + '.tmp'],
     ]
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, 'mqb200.h')]
     newest_header = max(os.path.getmtime(h) for h in headers)

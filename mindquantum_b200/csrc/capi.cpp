@@ -108,6 +108,10 @@ struct TimeScope {
 
 using namespace mqb;
 
+namespace mqb {
+void set_last_error(const char *msg) { g_last_error = msg; }
+}  // namespace mqb
+
 struct mqb_hamiltonian {
     int n = 0, precision = 0;
     std::vector<HamGroup> groups;
