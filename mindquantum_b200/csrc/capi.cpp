@@ -130,6 +130,8 @@ struct SchedDev {
         cudaFree(s.d_slot_map);
         cudaFree(s.d_stages);
         cudaFree(s.d_stage_ops);
+        cudaFree(s.d_f_stages);
+        cudaFree(s.d_f_stage_ops);
     }
 };
 
@@ -166,11 +168,14 @@ static std::unique_ptr<SchedDev> make_sched(const mqb_program &p, int K, bool fu
     // the per-gate kernels
     if (K < reg_bits + 5) fuse = false;
     sd->s = build_schedule(p.n, K, contiguity_bits(p.precision), p.ops, fuse);
-    build_stages(sd->s, p.ops, reg_bits, p.precision);
+    build_stages(sd->s, p.ops, reg_bits, p.precision, false);
+    build_stages(sd->s, p.ops, fwd_reg_bits(p.precision), p.precision, true);
     sd->s.d_pass_ops = upload(sd->s.pass_ops);
     sd->s.d_slot_map = upload(sd->s.slot_map);
     sd->s.d_stages = upload(sd->s.stages);
     sd->s.d_stage_ops = upload(sd->s.stage_ops);
+    sd->s.d_f_stages = upload(sd->s.f_stages);
+    sd->s.d_f_stage_ops = upload(sd->s.f_stage_ops);
     return sd;
 }
 
@@ -207,12 +212,12 @@ static void run_forward_pass(const mqb_program &p, const Schedule &s, const Pass
     if (ps.fused) {
         Fwd2Args<R> a{};
         a.g = make_geom(p.n, ps.qbits);
-        a.stages = s.d_stages + ps.stage_begin;
-        a.n_stages = ps.n_stages;
-        a.sops = s.d_stage_ops + ps.sop_begin;
-        a.n_ops = ps.n_sops;
-        a.reg_bits = ps.reg_bits;
-        a.mtab_entries = ps.mtab_entries;
+        a.stages = s.d_f_stages + ps.f_stage_begin;
+        a.n_stages = ps.f_n_stages;
+        a.sops = s.d_f_stage_ops + ps.f_sop_begin;
+        a.n_ops = ps.f_n_sops;
+        a.reg_bits = ps.f_reg_bits;
+        a.mtab_entries = ps.f_mtab_entries;
         a.mats = mats;
         a.mats_stride = p.per_sample;
         a.cpool = cpool;
@@ -678,7 +683,7 @@ int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, i
         int K = std::min(n_qubits, rb + 8);
         if (tile_bits > 0) K = std::min(n_qubits, std::max(rb + 5, tile_bits));
         Schedule s = build_schedule(n_qubits, K, contiguity_bits(precision), ops, fuse != 0 && K >= rb + 5);
-        build_stages(s, ops, rb, precision);
+        build_stages(s, ops, rb, precision, true);
         int pos = 0;
         for (size_t pi = 0; pi < s.passes.size(); ++pi) {
             const Pass &ps = s.passes[pi];
@@ -686,7 +691,7 @@ int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, i
             for (int q : ps.qbits) qm |= uint64_t(1) << q;
             qmask[pi] = qm;
             fused[pi] = ps.fused;
-            if (n_stages) n_stages[pi] = ps.n_stages;
+            if (n_stages) n_stages[pi] = ps.f_n_stages;
             if (ps.fused) {
                 for (int i = ps.op_begin; i < ps.op_end; ++i) {
                     order[pos] = s.pass_ops[i].op;

@@ -222,6 +222,34 @@ __device__ __forceinline__ void fw_perm1(V (&v)[1 << RB], V m01, V m10, bool uni
     }
 }
 
+// X on register position P controlled by register position C (CNOT inside the registers): a
+// compile-time permutation of the thread's registers, i.e. register renaming.
+template <typename V, int RB, int P, int C>
+__device__ __forceinline__ void fw_cswap(V (&v)[1 << RB]) {
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if ((j >> P & 1) || !(j >> C & 1)) continue;
+        const V a = v[j];
+        v[j] = v[j | (1 << P)];
+        v[j | (1 << P)] = a;
+    }
+}
+
+template <typename V, int RB>
+__device__ __forceinline__ void dispatch_cswap(V (&v)[1 << RB], int p, int c) {
+#define MQB_CS(P, C)                                                   \
+    case (P * 8 + C):                                                  \
+        if constexpr (RB > P && RB > C) fw_cswap<V, RB, P, C>(v);     \
+        break;
+    switch (p * 8 + c) {
+        MQB_CS(0, 1) MQB_CS(0, 2) MQB_CS(0, 3) MQB_CS(0, 4) MQB_CS(1, 0) MQB_CS(1, 2) MQB_CS(1, 3) MQB_CS(1, 4)
+        MQB_CS(2, 0) MQB_CS(2, 1) MQB_CS(2, 3) MQB_CS(2, 4) MQB_CS(3, 0) MQB_CS(3, 1) MQB_CS(3, 2) MQB_CS(3, 4)
+        MQB_CS(4, 0) MQB_CS(4, 1) MQB_CS(4, 2) MQB_CS(4, 3)
+        default: break;
+    }
+#undef MQB_CS
+}
+
 template <typename V, int RB, int P, bool CTRL>
 __device__ __forceinline__ void fw_diag1(V (&v)[1 << RB], V d0, V d1, uint32_t rctrl) {
 #pragma unroll
@@ -339,6 +367,10 @@ __device__ __forceinline__ void fwd_gate(V (&v)[1 << RB], const StageOp &so, con
         } break;
         case SK_PERM1:
         case SK_SWAP1: {
+            if (so.kind == SK_SWAP1 && so.rc1 >= 0) {   // one control among the register bits
+                dispatch_cswap<V, RB>(v, so.p0, so.rc1);
+                break;
+            }
             const bool unit = so.kind == SK_SWAP1;
             const V m01 = ADJ ? cconj(M[2]) : M[1], m10 = ADJ ? cconj(M[1]) : M[2];
 #define MQB_C(P)                                                                                    \
@@ -611,6 +643,12 @@ __device__ __forceinline__ void bwd_gate(V (&v)[1 << RB], V (&l)[NH][1 << RB], c
         case SK_PERM1:
         case SK_SWAP1: {
             // constant gates: no gradient, uncompute psi and every lambda
+            if (so.kind == SK_SWAP1 && so.rc1 >= 0) {   // self-inverse register permutation
+                dispatch_cswap<V, RB>(v, so.p0, so.rc1);
+#pragma unroll
+                for (int h = 0; h < NH; ++h) dispatch_cswap<V, RB>(l[h], so.p0, so.rc1);
+                break;
+            }
             const bool unit = so.kind == SK_SWAP1;
             const V m01 = cconj(M[2]), m10 = cconj(M[1]);
 #define MQB_C(P)                                                                                    \
@@ -774,7 +812,7 @@ __global__ void __launch_bounds__(256, 2) fused_fwd2_kernel(const Fwd2Args<R> a)
 }
 
 template <typename R, int RB, int NH>
-__global__ void __launch_bounds__(256, 1) fused_bwd2_kernel(const Bwd2Args<R> a) {
+__global__ void __launch_bounds__(256, 2) fused_bwd2_kernel(const Bwd2Args<R> a) {
     using V = cplx<R>;
     constexpr int NR = 1 << RB;
     constexpr int NV = NR / (16 / int(sizeof(V)));   // 16-byte vectors per thread per tile

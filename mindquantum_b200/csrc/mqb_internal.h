@@ -88,7 +88,7 @@ struct StageOp {
     int32_t mcount;      // entries copied into the table (M, then dM_0..)
     int64_t msrc;        // source offset: per-sample block (msrc_ps) or constant pool
     int32_t msrc_ps;     // 1: per-sample matrices, 0: constant pool
-    int32_t pad2;
+    int32_t rc1;         // the register position of the only control when rctrl has one bit, else -1
 };
 
 // A pass: one sweep over the state(s).
@@ -104,6 +104,8 @@ struct Pass {
     int stage_begin = 0, n_stages = 0;       // fused: range in Schedule::stages
     int sop_begin = 0, n_sops = 0;           // fused: range in Schedule::stage_ops (StageDesc ranges are relative)
     int mtab_entries = 0;                    // fused: complex entries of the pass's shared-memory matrix table
+    // the forward kernel's own stage layout of the same pass (more register bits, no lambdas)
+    int f_stage_begin = 0, f_n_stages = 0, f_sop_begin = 0, f_n_sops = 0, f_mtab_entries = 0, f_reg_bits = 0;
     int reg_bits = 0, thread_bits = 0;       // fused: registers / threads of the tile kernel
 };
 
@@ -112,8 +114,12 @@ struct Schedule {
     std::vector<Pass> passes;
     std::vector<PassOp> pass_ops;
     std::vector<int32_t> slot_map;  // pass-local slot -> global gradient slot
-    std::vector<StageDesc> stages;
+    std::vector<StageDesc> stages;      // backward layout
     std::vector<StageOp> stage_ops;
+    std::vector<StageDesc> f_stages;    // forward layout
+    std::vector<StageOp> f_stage_ops;
+    StageDesc *d_f_stages = nullptr;
+    StageOp *d_f_stage_ops = nullptr;
     PassOp *d_pass_ops = nullptr;   // device copies
     int32_t *d_slot_map = nullptr;
     StageDesc *d_stages = nullptr;
@@ -150,8 +156,9 @@ struct HamGroup {
 
 // Builders (scheduler.cpp)
 Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool fuse);
-// Split every fused pass of `s` into register stages with `reg_bits` register bits per thread.
-void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int precision);
+// Split every fused pass of `s` into register stages with `reg_bits` register bits per thread:
+// the backward layout (Schedule::stages) or, with `forward`, the forward layout (f_stages).
+void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int precision, bool forward = false);
 inline uint32_t smem_swizzle(uint32_t L, int precision) {
     // XOR-fold the index into its low 4 (complex64) / 3 (complex128) bits: linear over GF(2) and
     // a bijection, so bank conflicts of the stage exchanges depend only on the thread bits' residues

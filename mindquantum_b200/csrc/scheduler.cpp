@@ -200,20 +200,20 @@ Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool
 
 // Greedy register-stage grouping of one fused pass (same blocking rule as the pass scan, over
 // tile-local bits), then padding of the register set and a bank-conflict-aware thread-bit order.
-void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int precision) {
-    s.stages.clear();
-    s.stage_ops.clear();
+void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int precision, bool forward) {
+    std::vector<StageDesc> &stages = forward ? s.f_stages : s.stages;
+    std::vector<StageOp> &stage_ops = forward ? s.f_stage_ops : s.stage_ops;
+    stages.clear();
+    stage_ops.clear();
     const int res_mod = precision == MQB_PREC_C64 ? 4 : 3;
     for (Pass &p : s.passes) {
         if (!p.fused) continue;
         const int K = p.K;
         // 2^TB threads (32..256) holding 2^RB amplitudes each; passes are only fused when K >= reg_bits + 5
-        const int RB = reg_bits;
+        const int RB = std::min(reg_bits, K - 5);
         const int TB = K - RB;
-        p.reg_bits = RB;
-        p.thread_bits = TB;
-        p.stage_begin = int(s.stages.size());
-        p.sop_begin = int(s.stage_ops.size());
+        const int stage_begin = int(stages.size());
+        const int sop_begin = int(stage_ops.size());
         int mtab = 0;
         const int npo = p.op_end - p.op_begin;
         std::vector<char> done(npo, 0);
@@ -283,7 +283,7 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
             int pos_of[32];
             for (int i = 0; i < 32; ++i) pos_of[i] = -1;
             for (int i = 0; i < RB; ++i) pos_of[rl[i]] = i;
-            sd.op_begin = int(s.stage_ops.size()) - p.sop_begin;
+            sd.op_begin = int(stage_ops.size()) - sop_begin;
             for (int i : members) {
                 const PassOp &po = s.pass_ops[p.op_begin + i];
                 const DevOp &dop = ops[po.op];
@@ -298,6 +298,7 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
                 so.msrc = dop.mat_off;
                 so.msrc_ps = dop.per_sample;
                 mtab += so.mcount;
+                so.rc1 = -1;
                 so.octrl = po.octrl;
                 so.rctrl = 0;
                 so.tctrl = 0;
@@ -308,6 +309,7 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
                     else
                         so.tctrl |= 1u << b;
                 }
+                if (popc(so.rctrl) == 1) so.rc1 = __builtin_ctz(so.rctrl);
                 if (po.kind == KIND_DENSE) {
                     so.kind = po.m == 1 ? SK_DENSE1 : SK_DENSE2;
                     if (po.m == 1 && dop.sub == SUB_REAL) so.kind = SK_REAL1;
@@ -330,16 +332,29 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
                         }
                     }
                 }
-                s.stage_ops.push_back(so);
+                stage_ops.push_back(so);
                 done[i] = 1;
                 ++n_done;
             }
-            sd.op_end = int(s.stage_ops.size()) - p.sop_begin;
-            s.stages.push_back(sd);
+            sd.op_end = int(stage_ops.size()) - sop_begin;
+            stages.push_back(sd);
         }
-        p.n_stages = int(s.stages.size()) - p.stage_begin;
-        p.n_sops = int(s.stage_ops.size()) - p.sop_begin;
-        p.mtab_entries = mtab;
+        if (forward) {
+            p.f_reg_bits = RB;
+            p.f_stage_begin = stage_begin;
+            p.f_n_stages = int(stages.size()) - stage_begin;
+            p.f_sop_begin = sop_begin;
+            p.f_n_sops = int(stage_ops.size()) - sop_begin;
+            p.f_mtab_entries = mtab;
+        } else {
+            p.reg_bits = RB;
+            p.thread_bits = TB;
+            p.stage_begin = stage_begin;
+            p.n_stages = int(stages.size()) - stage_begin;
+            p.sop_begin = sop_begin;
+            p.n_sops = int(stage_ops.size()) - sop_begin;
+            p.mtab_entries = mtab;
+        }
     }
 }
 
