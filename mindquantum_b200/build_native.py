@@ -8,13 +8,15 @@ CUDA runtime statically, so the .so has no dependency beyond the NVIDIA driver.
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
 LIB = os.path.join(HERE, 'libmqb200.so')
-SOURCES = ['kernels.cu', 'fused.cu', 'capi.cpp', 'scheduler.cpp', 'noalloc.cu']
-HEADERS = ['kernels.cuh', 'mqb_internal.h', 'mqb_gate_ids.h']
+FUSED = ['fused_fwd_c64.cu', 'fused_fwd_c128.cu', 'fused_bwd_c64.cu', 'fused_bwd_c128.cu']
+SOURCES = ['kernels.cu', *FUSED, 'capi.cpp', 'scheduler.cpp', 'noalloc.cu']
+HEADERS = ['kernels.cuh', 'mqb_internal.h', 'mqb_gate_ids.h', 'fused_impl.cuh', 'regops.cuh']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 
@@ -48,34 +50,40 @@ def build(force=False, verbose=False):
     env.pop('CXX', None)
     common = ['-O3', '-std=c++17', '-Xcompiler', '-fPIC', '-Xcompiler', '-fvisibility=hidden',
               '-Xcompiler', '-fvisibility-inlines-hidden', '-ccbin', 'g++', f'-I{INCLUDE}']
-    steps = [
-        [_nvcc(), *ARCH, '-lineinfo', *common, '-c', os.path.join(CSRC, 'kernels.cu'),
-         '-o', os.path.join(bdir, 'kernels.o')],
-        [_nvcc(), *ARCH, '-lineinfo', *common, '-c', os.path.join(CSRC, 'fused.cu'),
-         '-o', os.path.join(bdir, 'fused.o')],
-        [_nvcc(), *ARCH, '-lineinfo', *common, '-x', 'cu', '-c', os.path.join(CSRC, 'capi.cpp'),
-         '-o', os.path.join(bdir, 'capi.o')],
-        [_nvcc(), *ARCH, '-lineinfo', *common, '-c', os.path.join(CSRC, 'noalloc.cu'),
-         '-o', os.path.join(bdir, 'noalloc.o')],
-        [_nvcc(), *common, '-x', 'c++', '-c', os.path.join(CSRC, 'scheduler.cpp'),
-         '-o', os.path.join(bdir, 'scheduler.o')],
-        [_nvcc(), *ARCH, '-shared', '-cudart', 'static', '-ccbin', 'g++',
-         *[os.path.join(bdir, o) for o in ('kernels.o', 'fused.o', 'capi.o', 'scheduler.o', 'noalloc.o')], '-o', LIB + '.tmp'],
-    ]
+
+    def obj(name):
+        return os.path.join(bdir, os.path.splitext(name)[0] + '.o')
+
+    compiles = [[_nvcc(), *ARCH, '-lineinfo', *common, '-c', os.path.join(CSRC, f), '-o', obj(f)]
+                for f in ('kernels.cu', *FUSED, 'noalloc.cu')]
+    compiles.append([_nvcc(), *ARCH, '-lineinfo', *common, '-x', 'cu', '-c', os.path.join(CSRC, 'capi.cpp'),
+                     '-o', obj('capi.cpp')])
+    compiles.append([_nvcc(), *common, '-x', 'c++', '-c', os.path.join(CSRC, 'scheduler.cpp'),
+                     '-o', obj('scheduler.cpp')])
+    link = [_nvcc(), *ARCH, '-shared', '-cudart', 'static', '-ccbin', 'g++',
+            *[obj(f) for f in SOURCES], '-o', LIB + '.tmp']
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, 'mqb200.h')]
     newest_header = max(os.path.getmtime(h) for h in headers)
-    for cmd in steps:
+
+    def stale(cmd):
         out = cmd[cmd.index('-o') + 1]
-        if '-c' in cmd and not force and os.path.exists(out):
-            src = cmd[cmd.index('-c') + 1]
-            if os.path.getmtime(out) >= max(os.path.getmtime(src), newest_header):
-                continue   # object up to date
+        src = cmd[cmd.index('-c') + 1]
+        return force or not os.path.exists(out) or os.path.getmtime(out) < max(os.path.getmtime(src), newest_header)
+
+    def run(cmd):
         if verbose:
-            print(' '.join(cmd))
+            print(' '.join(cmd), flush=True)
         res = subprocess.run(cmd, capture_output=True, text=True, env=env)
         if res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
-            raise RuntimeError('building libmqb200.so failed')
+        return res.returncode
+
+    todo = [c for c in compiles if stale(c)]
+    # the fused translation units dominate the build time: compile everything in parallel
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as pool:
+        codes = list(pool.map(run, todo))
+    if any(codes) or run(link) != 0:
+        raise RuntimeError('building libmqb200.so failed')
     os.replace(LIB + '.tmp', LIB)
     return LIB
 

@@ -519,6 +519,7 @@ static DevOp basic_op(const mqb_gate_desc &d, int k, int n_qubits, const mqb_par
         op.kind = KIND_DENSE;
         op.mat_size = 1 << (2 * d.n_obj);
         if (d.gate_id == GID_RY) op.sub = SUB_REAL;   // RY and its derivative are real matrices
+        if (d.gate_id == GID_RX) op.sub = SUB_RXL;    // RX: real diagonal, imaginary off-diagonal
     }
     const int expect_obj =
         (d.gate_id == GID_RZZ || (d.gate_id >= GID_RXX && d.gate_id <= GID_SWAPALPHA) || d.gate_id == GID_FSIM) ? 2 : 1;

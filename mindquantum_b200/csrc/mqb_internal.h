@@ -41,10 +41,11 @@ struct DevOp {
     int32_t custom_off;          // GID_CUSTOM: offset of M in the caller's per-sample custom block
     uint64_t px, py, pz;         // GID_RPS masks
     int32_t pny;
-    int32_t sub;                 // dense single-qubit structure: SUB_GENERIC, SUB_REAL, SUB_PERM, SUB_SWAP
+    int32_t sub;                 // dense single-qubit structure: SUB_GENERIC, SUB_REAL, SUB_PERM, SUB_SWAP, SUB_RXL
 };
 // Structure of a dense single-qubit matrix, used to pick a cheaper register kernel.
-enum DenseSub : int32_t { SUB_GENERIC = 0, SUB_REAL = 1, SUB_PERM = 2, SUB_SWAP = 3 };
+// SUB_RXL: [[a, ib], [ib, a]] with a, b real, and so are its derivatives (RX).
+enum DenseSub : int32_t { SUB_GENERIC = 0, SUB_REAL = 1, SUB_PERM = 2, SUB_SWAP = 3, SUB_RXL = 4 };
 
 // An op as seen inside one fused pass (targets remapped to tile-local bits).
 struct PassOp {
@@ -70,7 +71,32 @@ struct StageDesc {
     int8_t pad[3];
     int32_t op_begin, op_end;      // range in Schedule::stage_ops
 };
-enum StageOpKind : int32_t { SK_DENSE1 = 0, SK_DENSE2 = 1, SK_DIAG1 = 2, SK_DIAG2 = 3, SK_REAL1 = 4, SK_PERM1 = 5, SK_SWAP1 = 6 };
+enum StageOpKind : int32_t {
+    SK_DENSE1 = 0, SK_DENSE2 = 1, SK_DIAG1 = 2, SK_DIAG2 = 3, SK_REAL1 = 4, SK_PERM1 = 5, SK_SWAP1 = 6, SK_RXL1 = 7
+};
+// Register codes: the structure of a stage op as the tile kernels resolve it at compile time.
+// P / Q: register positions of matrix bits 0 / 1; C: position of the only register control;
+// K: matrix bit of the diagonal target that sits on a register.  The backward kernels use
+// code * 4 + gradient selector (0 no gradient, 1 angle 0, 2 angles 0..2, 3 runtime mask).
+enum RegCode : int32_t {
+    RC_DENSE1 = 0,      // + P        dense 2x2, no register control
+    RC_REAL1 = 5,       // + P        real 2x2 (RY, H)
+    RC_RXL1 = 10,       // + P        [[a, ib], [ib, a]], a and b real (RX)
+    RC_X1 = 15,         // + P        X (register swap)
+    RC_DIAG1 = 20,      // + P        diagonal on a register
+    RC_SCALE = 25,      //            diagonal whose targets are off the registers (one factor per thread)
+    RC_DENSE1C = 26,    // + 5P + C   dense 2x2, one register control
+    RC_X1C = 51,        // + 5P + C   CNOT inside the registers
+    RC_DIAG1C = 76,     // + 5P + C   controlled diagonal (CZ, CRZ, CPS)
+    RC_SCALEC = 101,    // + C        SCALE with one register control
+    RC_DIAG2 = 106,     // + 5P + Q   two-target diagonal on registers (RZZ)
+    RC_DIAG2S = 131,    // + 5K + P   two-target diagonal, one target on register P, the other off
+    RC_DENSE2 = 141,    // + 5P + Q   dense 4x4, no register control
+    RC_GDENSE1 = 166,   // + P        dense 2x2, register control mask tested at run time
+    RC_GDIAG = 171,     //            any diagonal, register control mask tested at run time
+    RC_GDENSE2 = 172,   // + 5P + Q   dense 4x4, register control mask tested at run time
+    RC_COUNT = 197
+};
 struct StageOp {
     int32_t op;          // program op index
     int32_t kind;        // StageOpKind
@@ -88,7 +114,10 @@ struct StageOp {
     int32_t mcount;      // entries copied into the table (M, then dM_0..)
     int64_t msrc;        // source offset: per-sample block (msrc_ps) or constant pool
     int32_t msrc_ps;     // 1: per-sample matrices, 0: constant pool
-    int32_t rc1;         // the register position of the only control when rctrl has one bit, else -1
+    int32_t code;        // RegCode of the forward kernels
+    int32_t bcode;       // code * 4 + gradient selector, for the backward kernels
+    int32_t cflags;      // bit 0: octrl != 0, bit 1: tctrl != 0 (controls checked per thread)
+    int32_t pad;
 };
 
 // A pass: one sweep over the state(s).

@@ -200,6 +200,91 @@ Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool
 
 // Greedy register-stage grouping of one fused pass (same blocking rule as the pass scan, over
 // tile-local bits), then padding of the register set and a bank-conflict-aware thread-bit order.
+// Register code (forward) and code * 4 + gradient selector (backward) of a stage op; ops whose
+// shape or gradient angles have no specialised kernel take the generic codes.
+void assign_codes(StageOp &so) {
+    const int nrc = popc(so.rctrl);
+    const int C = nrc == 1 ? __builtin_ctz(so.rctrl) : -1;
+    const int gm = so.n_angles ? so.grad_mask : 0;
+    int code = -1, gsel = 0;
+    switch (so.kind) {
+        case SK_DENSE1:
+        case SK_REAL1:
+        case SK_RXL1:
+        case SK_PERM1:
+        case SK_SWAP1: {
+            const int P = so.p0;
+            if (nrc == 0) {
+                if (so.kind == SK_SWAP1) code = RC_X1 + P;
+                else if (so.kind == SK_REAL1) code = RC_REAL1 + P;
+                else if (so.kind == SK_RXL1) code = RC_RXL1 + P;
+                else code = RC_DENSE1 + P;
+            } else if (nrc == 1) {
+                code = so.kind == SK_SWAP1 ? RC_X1C + 5 * P + C : RC_DENSE1C + 5 * P + C;
+            } else {
+                code = RC_GDENSE1 + P;
+            }
+            // gradient selector; what the specialised kernels lack goes generic
+            const bool x = code >= RC_X1 && code < RC_X1 + 5;
+            const bool xc = code >= RC_X1C && code < RC_X1C + 25;
+            if (gm == 0) {
+                gsel = code >= RC_GDENSE1 ? 3 : 0;
+            } else if ((x || xc) && gm) {
+                code = RC_GDENSE1 + P;   // X matrices carry no derivative; never reached by lowered gates
+                gsel = 3;
+            } else if (code >= RC_GDENSE1) {
+                gsel = 3;
+            } else if (gm == 1) {
+                gsel = 1;
+            } else if (code < RC_DENSE1 + 5 && gm == 7) {
+                gsel = 2;
+            } else if (code < RC_DENSE1 + 5) {
+                gsel = 3;
+            } else {
+                code = RC_GDENSE1 + P;
+                gsel = 3;
+            }
+        } break;
+        case SK_DENSE2: {
+            const int P = so.p0, Q = so.p1;
+            if (nrc == 0) {
+                code = RC_DENSE2 + 5 * P + Q;
+                gsel = gm == 0 ? 0 : gm == 1 ? 1 : 3;
+            } else {
+                code = RC_GDENSE2 + 5 * P + Q;
+                gsel = 3;
+            }
+        } break;
+        case SK_DIAG1:
+        case SK_DIAG2: {
+            const bool two = so.kind == SK_DIAG2;
+            const bool in0 = so.dsrc[0] == 0, in1 = two && so.dsrc[1] == 0;
+            if (gm != 0 && gm != 1) {
+                code = RC_GDIAG;
+            } else if (!two) {
+                if (in0) code = nrc == 0 ? RC_DIAG1 + so.dval[0] : nrc == 1 ? RC_DIAG1C + 5 * so.dval[0] + C : RC_GDIAG;
+                else code = nrc == 0 ? RC_SCALE : nrc == 1 ? RC_SCALEC + C : RC_GDIAG;
+            } else if (nrc != 0) {
+                code = RC_GDIAG;
+            } else if (in0 && in1) {
+                code = RC_DIAG2 + 5 * so.dval[0] + so.dval[1];
+            } else if (in0) {
+                code = RC_DIAG2S + so.dval[0];
+            } else if (in1) {
+                code = RC_DIAG2S + 5 + so.dval[1];
+            } else {
+                code = RC_SCALE;
+            }
+            gsel = code == RC_GDIAG ? 3 : gm;
+        } break;
+        default:
+            throw std::runtime_error("stage op of unknown kind");
+    }
+    so.code = code;
+    so.bcode = code * 4 + gsel;
+    so.cflags = (so.octrl ? 1 : 0) | (so.tctrl ? 2 : 0);
+}
+
 void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int precision, bool forward) {
     std::vector<StageDesc> &stages = forward ? s.f_stages : s.stages;
     std::vector<StageOp> &stage_ops = forward ? s.f_stage_ops : s.stage_ops;
@@ -298,7 +383,6 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
                 so.msrc = dop.mat_off;
                 so.msrc_ps = dop.per_sample;
                 mtab += so.mcount;
-                so.rc1 = -1;
                 so.octrl = po.octrl;
                 so.rctrl = 0;
                 so.tctrl = 0;
@@ -309,16 +393,18 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
                     else
                         so.tctrl |= 1u << b;
                 }
-                if (popc(so.rctrl) == 1) so.rc1 = __builtin_ctz(so.rctrl);
                 if (po.kind == KIND_DENSE) {
                     so.kind = po.m == 1 ? SK_DENSE1 : SK_DENSE2;
                     if (po.m == 1 && dop.sub == SUB_REAL) so.kind = SK_REAL1;
                     if (po.m == 1 && dop.sub == SUB_PERM) so.kind = SK_PERM1;
                     if (po.m == 1 && dop.sub == SUB_SWAP) so.kind = SK_SWAP1;
+                    if (po.m == 1 && dop.sub == SUB_RXL) so.kind = SK_RXL1;
                     so.p0 = pos_of[po.lt[0]];
                     so.p1 = po.m == 2 ? pos_of[po.lt[1]] : 0;
                 } else {
                     so.kind = po.m == 1 ? SK_DIAG1 : SK_DIAG2;
+                    so.dsrc[1] = 3;   // absent second target
+                    so.dval[1] = 0;
                     for (int k = 0; k < po.m; ++k) {
                         if (po.lt[k] >= 0 && pos_of[po.lt[k]] >= 0) {
                             so.dsrc[k] = 0;
@@ -332,6 +418,7 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
                         }
                     }
                 }
+                assign_codes(so);
                 stage_ops.push_back(so);
                 done[i] = 1;
                 ++n_done;

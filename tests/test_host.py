@@ -39,7 +39,8 @@ def test_gate_ids_match_header():
 
 
 def _random_circuit(rng, n, n_gates, kinds=None):
-    kinds = kinds or ['h', 'x', 'cx', 'rx', 'ry', 'rz', 'rzz', 'u3', 'swap', 'cz', 'ccx', 'rxy', 'fsim', 'ps']
+    kinds = kinds or ['h', 'x', 'cx', 'rx', 'ry', 'rz', 'rzz', 'u3', 'swap', 'cz', 'ccx', 'rxy', 'fsim', 'ps',
+                      'ry1', 'crx', 'crz', 'ccz', 'crzz', 'y', 'cu3']
     c = Circuit()
     for i in range(n_gates):
         k = kinds[rng.integers(len(kinds))]
@@ -72,6 +73,20 @@ def _random_circuit(rng, n, n_gates, kinds=None):
             c += G.SWAP.on(qs[:2])
         elif k == 'fsim':
             c += G.FSim(f'a{i}', f'b{i}').on(qs[:2])
+        elif k == 'ry1':
+            c += G.RY(f'p{i}').on(qs[0])
+        elif k == 'crx':
+            c += G.RX(f'p{i}').on(qs[0], qs[1])
+        elif k == 'crz':
+            c += G.RZ(f'p{i}').on(qs[0], qs[1])
+        elif k == 'ccz':
+            c += G.Z.on(qs[0], qs[1:3])
+        elif k == 'crzz':
+            c += G.Rzz(f'p{i}').on(qs[:2], qs[2])
+        elif k == 'y':
+            c += G.Y.on(qs[0])
+        elif k == 'cu3':
+            c += G.U3(f'a{i}', f'b{i}', f'c{i}').on(qs[0], qs[1])
     return c
 
 
