@@ -90,7 +90,9 @@ typedef struct mqb_param_term {
 typedef struct mqb_program_options {
     int32_t fuse;          /* 1: fused tile passes (default), 0: one kernel per gate (plain path) */
     int32_t tile_bits;     /* 0: automatic */
-    int32_t reserved[6];
+    int32_t jit;           /* generated pass kernels: 0 automatic (registers of 18 qubits and more),
+                              1 always, -1 never (the precompiled tile kernels) */
+    int32_t reserved[5];
 } mqb_program_options;
 
 typedef struct mqb_program mqb_program;
@@ -137,6 +139,14 @@ MQB_API int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *
                               int32_t *n_stages);
 /* Passes and tile bits of the schedule mqb_expectation_with_grad uses for n_hams Hamiltonians. */
 MQB_API int mqb_program_grad_passes(mqb_program *prog, int n_hams, int *n_passes, int *tile_bits);
+
+/* Generate the pass kernels of a circuit (the forward kernels, and the backward kernels for
+ * n_hams lambdas when n_hams > 0) and compile them with NVRTC without loading them, so no GPU is
+ * needed; *n_kernels receives the number of distinct kernels.  No counterpart in the reference:
+ * a build check of the generated kernels. */
+MQB_API int mqb_jit_check(int n_qubits, int precision, const mqb_gate_desc *gates, int n_gates,
+                          const double *const_matrices, int64_t n_const_entries, int tile_bits, int n_hams,
+                          int *n_kernels);
 
 /* Workspace (bytes) that mqb_apply needs for `batch` samples. */
 MQB_API int mqb_apply_workspace_size(const mqb_program *prog, int64_t batch, size_t *bytes);

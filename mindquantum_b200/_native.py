@@ -42,7 +42,8 @@ class ParamTerm(ctypes.Structure):
 
 
 class ProgramOptions(ctypes.Structure):
-    _fields_ = [('fuse', ctypes.c_int32), ('tile_bits', ctypes.c_int32), ('reserved', ctypes.c_int32 * 6)]
+    _fields_ = [('fuse', ctypes.c_int32), ('tile_bits', ctypes.c_int32), ('jit', ctypes.c_int32),
+                ('reserved', ctypes.c_int32 * 5)]
 
 
 class ProgramInfo(ctypes.Structure):
@@ -76,6 +77,7 @@ SIGNATURES = {
     'mqb_program_create': [_I, _I, _P, _I, _P, _I, _I, _P, _I64, _P, _P],
     'mqb_program_destroy': [_P],
     'mqb_plan_schedule': [_I, _I, _P, _I, _P, _I64, _I, _I, _P, _P, _P, _P, _P, _P],
+    'mqb_jit_check': [_I, _I, _P, _I, _P, _I64, _I, _I, _P],
     'mqb_program_get_info': [_P, _P],
     'mqb_program_grad_passes': [_P, _I, _P, _P],
     'mqb_apply_workspace_size': [_P, _I64, _P],

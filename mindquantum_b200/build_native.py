@@ -3,7 +3,8 @@
     python -m mindquantum_b200.build_native        # rebuild if any source changed
 
 The library is compiled with nvcc for ``arch=compute_100a,code=sm_100a`` only and links the
-CUDA runtime statically, so the .so has no dependency beyond the NVIDIA driver.
+CUDA runtime statically; beyond the NVIDIA driver it needs the toolkit's NVRTC (libnvrtc.so.12),
+which compiles the generated pass kernels at run time.
 """
 import os
 import subprocess
@@ -15,8 +16,14 @@ CSRC = os.path.join(HERE, 'csrc')
 INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
 LIB = os.path.join(HERE, 'libmqb200.so')
 FUSED = ['fused_fwd_c64.cu', 'fused_fwd_c128.cu', 'fused_bwd_c64.cu', 'fused_bwd_c128.cu']
-SOURCES = ['kernels.cu', *FUSED, 'capi.cpp', 'scheduler.cpp', 'noalloc.cu']
-HEADERS = ['kernels.cuh', 'mqb_internal.h', 'mqb_gate_ids.h', 'fused_impl.cuh', 'regops.cuh']
+SOURCES = ['kernels.cu', *FUSED, 'capi.cpp', 'scheduler.cpp', 'noalloc.cu', 'jit.cpp']
+HEADERS = ['kernels.cuh', 'mqb_internal.h', 'mqb_gate_ids.h', 'fused_impl.cuh', 'regops.cuh', 'regmath.cuh',
+           'tile.cuh', 'jit_abi.h', 'jit.h']
+# headers compiled again at run time by NVRTC for the generated pass kernels (embedded as text)
+JIT_HEADERS = [('kJitRegmath', 'regmath.cuh'), ('kJitTile', 'tile.cuh'), ('kJitAbi', 'jit_abi.h')]
+# NVRTC from the CUDA toolkit the library is built with (found again at run time through the rpath)
+CUDA_LIB = '/usr/local/cuda/lib64'
+NVRTC_LIBS = [f'-L{CUDA_LIB}', '-lnvrtc', '-Xlinker', f'-rpath={CUDA_LIB}']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 
@@ -54,14 +61,30 @@ def build(force=False, verbose=False):
     def obj(name):
         return os.path.join(bdir, os.path.splitext(name)[0] + '.o')
 
+    # the NVRTC headers as C++ string literals
+    embed = os.path.join(bdir, 'jit_embed.cpp')
+    text = ['// generated by build_native.py from the headers below', 'namespace mqb {']
+    for sym, name in JIT_HEADERS:
+        body = open(os.path.join(CSRC, name), encoding='utf8').read()
+        if ')MQBJIT"' in body:
+            raise RuntimeError(f'{name} contains the raw-string delimiter')
+        text.append(f'extern const char *const {sym} = R"MQBJIT({body})MQBJIT";')
+    text.append('}  // namespace mqb')
+    text = '\n'.join(text) + '\n'
+    if not os.path.exists(embed) or open(embed, encoding='utf8').read() != text:
+        with open(embed, 'w', encoding='utf8') as f:
+            f.write(text)
+
     compiles = [[_nvcc(), *ARCH, '-lineinfo', *common, '-c', os.path.join(CSRC, f), '-o', obj(f)]
                 for f in ('kernels.cu', *FUSED, 'noalloc.cu')]
     compiles.append([_nvcc(), *ARCH, '-lineinfo', *common, '-x', 'cu', '-c', os.path.join(CSRC, 'capi.cpp'),
                      '-o', obj('capi.cpp')])
     compiles.append([_nvcc(), *common, '-x', 'c++', '-c', os.path.join(CSRC, 'scheduler.cpp'),
                      '-o', obj('scheduler.cpp')])
+    compiles.append([_nvcc(), *common, '-x', 'c++', '-c', os.path.join(CSRC, 'jit.cpp'), '-o', obj('jit.cpp')])
+    compiles.append([_nvcc(), *common, '-x', 'c++', '-c', embed, '-o', obj('jit_embed.cpp')])
     link = [_nvcc(), *ARCH, '-shared', '-cudart', 'static', '-ccbin', 'g++',
-            *[obj(f) for f in SOURCES], '-o', LIB + '.tmp']
+            *[obj(f) for f in SOURCES], obj('jit_embed.cpp'), *NVRTC_LIBS, '-lpthread', '-ldl', '-o', LIB + '.tmp']
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, 'mqb200.h')]
     newest_header = max(os.path.getmtime(h) for h in headers)
 

@@ -10,10 +10,12 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
+#include "jit.h"
 #include "kernels.cuh"
 
 namespace {
@@ -125,7 +127,13 @@ struct mqb_hamiltonian {
 
 struct SchedDev {
     Schedule s;
+    JitMtab *d_jmt = nullptr, *d_f_jmt = nullptr;    // matrix-table sources of the generated kernels
+    std::mutex jit_mu;
+    std::vector<const void *> jit_fwd;                // generated forward kernel of every pass
+    std::map<int, std::vector<const void *>> jit_bwd; // generated backward kernels, by lambdas
     ~SchedDev() {
+        cudaFree(d_jmt);
+        cudaFree(d_f_jmt);
         cudaFree(s.d_pass_ops);
         cudaFree(s.d_slot_map);
         cudaFree(s.d_stages);
@@ -136,7 +144,7 @@ struct SchedDev {
 };
 
 struct mqb_program {
-    int n = 0, precision = 0, n_params = 0, fuse = 1, tile_bits = 0;
+    int n = 0, precision = 0, n_params = 0, fuse = 1, tile_bits = 0, jit = 0;
     std::vector<DevOp> ops;
     std::vector<mqb_gate_desc> descs;
     DevOp *d_ops = nullptr;
@@ -160,7 +168,37 @@ struct mqb_program {
         cudaFree(d_csr_coeff);
     }
     size_t elem() const { return precision == MQB_PREC_C64 ? 8 : 16; }
+    // generated pass kernels pay their compile time back from 2^18 amplitudes on
+    bool use_jit() const { return jit > 0 || (jit == 0 && n >= 18); }
 };
+
+// Calls that promise to allocate nothing (mqb_apply_static) run the precompiled kernels only.
+static thread_local bool t_jit_blocked = false;
+namespace mqb {
+JitBlock::JitBlock() : prev_(t_jit_blocked) { t_jit_blocked = true; }
+JitBlock::~JitBlock() { t_jit_blocked = prev_; }
+}  // namespace mqb
+
+static std::vector<JitMtab> jit_mtab(const std::vector<StageOp> &v) {
+    std::vector<JitMtab> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = JitMtab{v[i].moff, v[i].mcount, (long long)v[i].msrc, v[i].msrc_ps, 0};
+    return o;
+}
+
+static const std::vector<const void *> *jit_forward(const mqb_program &p, SchedDev &sd) {
+    if (!p.use_jit() || t_jit_blocked || sd.s.passes.empty()) return nullptr;
+    std::lock_guard<std::mutex> lk(sd.jit_mu);
+    if (sd.jit_fwd.empty()) sd.jit_fwd = jit_forward_kernels(sd.s, p.precision);
+    return &sd.jit_fwd;
+}
+
+static const std::vector<const void *> *jit_backward(const mqb_program &p, SchedDev &sd, int n_hams) {
+    if (!p.use_jit() || t_jit_blocked || sd.s.passes.empty()) return nullptr;
+    std::lock_guard<std::mutex> lk(sd.jit_mu);
+    auto &v = sd.jit_bwd[n_hams];
+    if (v.empty()) v = jit_backward_kernels(sd.s, p.precision, n_hams);
+    return &v;
+}
 
 static std::unique_ptr<SchedDev> make_sched(const mqb_program &p, int K, bool fuse, int reg_bits) {
     auto sd = std::make_unique<SchedDev>();
@@ -176,6 +214,8 @@ static std::unique_ptr<SchedDev> make_sched(const mqb_program &p, int K, bool fu
     sd->s.d_stage_ops = upload(sd->s.stage_ops);
     sd->s.d_f_stages = upload(sd->s.f_stages);
     sd->s.d_f_stage_ops = upload(sd->s.f_stage_ops);
+    sd->d_jmt = upload(jit_mtab(sd->s.stage_ops));
+    sd->d_f_jmt = upload(jit_mtab(sd->s.f_stage_ops));
     return sd;
 }
 
@@ -205,10 +245,32 @@ static TileGeom pass_geom(int n, const Pass &ps) {
 
 // ---------------------------------------------------------------------------------------------- execution
 template <typename R>
-static void run_forward_pass(const mqb_program &p, const Schedule &s, const Pass &ps, const cplx<R> *mats,
-                             const cplx<R> *src, int64_t src_stride, cplx<R> *dst, int64_t batch, cudaStream_t st) {
+static void run_forward_pass(const mqb_program &p, const SchedDev &sd, size_t pi, const void *jk,
+                             const cplx<R> *mats, const cplx<R> *src, int64_t src_stride, cplx<R> *dst, int64_t batch,
+                             cudaStream_t st) {
+    const Schedule &s = sd.s;
+    const Pass &ps = s.passes[pi];
     const int sm = sm_count_cached();
     const cplx<R> *cpool = static_cast<const cplx<R> *>(p.d_cpool);
+    if (ps.fused && jk) {
+        JitFwdArgs<cplx<R>> a{};
+        a.g = make_geom(p.n, ps.qbits);
+        a.mt = sd.d_f_jmt + ps.f_sop_begin;
+        a.n_mt = ps.f_n_sops;
+        a.mtab_entries = ps.f_mtab_entries;
+        a.mats = mats;
+        a.mats_stride = p.per_sample;
+        a.cpool = cpool;
+        a.src = src;
+        a.dst = dst;
+        a.batch = batch;
+        a.src_batch_stride = src_stride;
+        TimeScope ts(TK_FWD, st);
+        ck(jit_launch(jk, &a, 1 << (ps.K - ps.f_reg_bits), jit_forward_smem(ps, p.precision), sm,
+                      (long long)batch << a.g.n_out, st),
+           "generated forward pass");
+        return;
+    }
     if (ps.fused) {
         Fwd2Args<R> a{};
         a.g = make_geom(p.n, ps.qbits);
@@ -266,8 +328,10 @@ static void apply_impl(mqb_program &p, void *states, int64_t batch, const double
     cplx<R> *mats = static_cast<cplx<R> *>(ws);
     run_matgen<R>(p, params, param_stride, custom, batch, mats, st);
     cplx<R> *s = static_cast<cplx<R> *>(states);
-    const Schedule &sc = p.apply_sched->s;
-    for (const Pass &ps : sc.passes) run_forward_pass<R>(p, sc, ps, mats, s, int64_t(1) << p.n, s, batch, st);
+    SchedDev &sd = *p.apply_sched;
+    const auto *jk = jit_forward(p, sd);
+    for (size_t i = 0; i < sd.s.passes.size(); ++i)
+        run_forward_pass<R>(p, sd, i, jk ? (*jk)[i] : nullptr, mats, s, int64_t(1) << p.n, s, batch, st);
 }
 
 // Hamiltonian passes: out = H ket (if out), f += <bra|H ket> (if fout)
@@ -360,10 +424,12 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
     // forward: psi_{q+1} = pass_q(psi_q), psi_0 = init (or |0...0>)
     const V *init_v = static_cast<const V *>(init);
     const int64_t init_stride = init_batched ? dim : 0;
+    const auto *jf = jit_forward(p, sd);
+    const auto *jb = jit_backward(p, sd, n_hams);
     for (int q = 0; q < P; ++q) {
         const V *src = (q == 0) ? init_v : loc(q);
         const int64_t sstr = (q == 0) ? init_stride : dim;
-        run_forward_pass<R>(p, s, s.passes[q], mats, src, sstr, loc(q + 1), batch, st);
+        run_forward_pass<R>(p, sd, q, jf ? (*jf)[q] : nullptr, mats, src, sstr, loc(q + 1), batch, st);
     }
     V *psiP = W;
     if (P > 0) {
@@ -378,7 +444,29 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
     for (int q = P - 1; q >= 0; --q) {
         const Pass &ps = s.passes[q];
         const bool stored_q = L.ckpt_index[q] >= 0;
-        if (ps.fused) {
+        if (ps.fused && jb && (*jb)[q]) {
+            JitBwdArgs<V> a{};
+            a.g = make_geom(p.n, ps.qbits);
+            a.mt = sd.d_jmt + ps.sop_begin;
+            a.n_mt = ps.n_sops;
+            a.mtab_entries = ps.mtab_entries;
+            a.mats = mats;
+            a.mats_stride = p.per_sample;
+            a.cpool = cpool;
+            a.psi_src = loc(q + 1);
+            a.psi_dst = (q > 0 && !stored_q) ? W : nullptr;
+            a.lam = lam;
+            a.gslots = gslots;
+            a.slot_map = s.d_slot_map + ps.slot_begin;
+            a.n_slots = std::max(1, p.n_slots);
+            a.n_hams = n_hams;
+            a.n_local_slots = ps.n_slots;
+            a.batch = batch;
+            TimeScope ts(TK_BWD, st);
+            ck(jit_launch((*jb)[q], &a, 1 << (ps.K - ps.reg_bits), jit_backward_smem(ps, p.precision, n_hams), sm,
+                          (long long)batch << a.g.n_out, st),
+               "generated backward pass");
+        } else if (ps.fused) {
             Bwd2Args<R> a{};
             a.g = make_geom(p.n, ps.qbits);
             a.stages = s.d_stages + ps.stage_begin;
@@ -595,6 +683,7 @@ int mqb_program_create(int n_qubits, int precision, const mqb_gate_desc *gates, 
         p->n_params = n_params;
         p->fuse = options ? options->fuse : 1;
         p->tile_bits = options ? options->tile_bits : 0;
+        p->jit = options ? options->jit : 0;
         p->descs.assign(gates, gates + n_gates);
         std::vector<std::complex<double>> pool;
         std::vector<std::vector<std::pair<int32_t, double>>> csr(std::max(0, n_params));
@@ -704,6 +793,32 @@ int mqb_plan_schedule(int n_qubits, int precision, const mqb_gate_desc *gates, i
             }
         }
         *n_passes = int(s.passes.size());
+    });
+}
+
+int mqb_jit_check(int n_qubits, int precision, const mqb_gate_desc *gates, int n_gates, const double *const_matrices,
+                  int64_t n_const_entries, int tile_bits, int n_hams, int *n_kernels) {
+    return guarded([&] {
+        if (n_qubits < 1 || n_qubits > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
+        if (precision != MQB_PREC_C64 && precision != MQB_PREC_C128) fail(MQB_ERR_INVALID, "unknown precision");
+        if (n_hams < 0 || n_hams > 4 || !n_kernels) fail(MQB_ERR_INVALID, "invalid argument");
+        std::vector<DevOp> ops;
+        int slots = 0;
+        for (int k = 0; k < n_gates; ++k) {
+            DevOp op = basic_op(gates[k], k, n_qubits, nullptr, 0, 0, const_matrices, n_const_entries);
+            if (op.grad_mask) {
+                op.slot0 = slots;
+                for (int a = 0; a < op.n_angles; ++a) slots += (op.grad_mask >> a) & 1;
+            }
+            ops.push_back(op);
+        }
+        const int rb = n_hams ? bwd_reg_bits(precision, n_hams) : fwd_reg_bits(precision);
+        int K = std::min(n_qubits, rb + 8);
+        if (tile_bits > 0) K = std::min(n_qubits, std::max(rb + 5, tile_bits));
+        Schedule s = build_schedule(n_qubits, K, contiguity_bits(precision), ops, K >= rb + 5);
+        build_stages(s, ops, rb, precision, false);
+        build_stages(s, ops, fwd_reg_bits(precision), precision, true);
+        *n_kernels = jit_compile_check(s, precision, n_hams);
     });
 }
 

@@ -23,6 +23,7 @@
 
 #include "kernels.cuh"
 #include "regops.cuh"
+#include "tile.cuh"
 
 namespace mqb {
 
@@ -30,90 +31,13 @@ namespace {
 
 using reg::warp_sum;
 
-template <typename V>
-__device__ __forceinline__ uint32_t swz(uint32_t L) {
-    if (sizeof(V) == 8) return L ^ ((L >> 4) & 15u) ^ ((L >> 8) & 15u) ^ ((L >> 12) & 15u);
-    return L ^ ((L >> 3) & 7u) ^ ((L >> 6) & 7u) ^ ((L >> 9) & 7u) ^ ((L >> 12) & 7u);
-}
-
-__device__ __forceinline__ uint64_t tile_base(const TileGeom &g, uint64_t t) {
-    uint64_t base = 0;
-    for (int i = 0; i < g.n_out; ++i)
-        if (t >> i & 1) base |= uint64_t(1) << g.outside[i];
-    return base;
-}
-
-__device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-
-__device__ __forceinline__ void build_table(uint64_t *tab, const TileGeom &g) {
-    const int nh = 1 << (g.K - g.c);
-    for (int h = threadIdx.x; h < nh; h += blockDim.x) {
-        uint64_t off = 0;
-        for (int i = 0; i < g.K - g.c; ++i)
-            if (h >> i & 1) off |= uint64_t(1) << g.qbits[g.c + i];
-        tab[h] = off;
-    }
-}
-
-// global (coalesced 16-byte vectors) -> swizzled shared tile.  Every thread moves NV vectors;
-// all of its global loads are issued before the first shared store so their latencies overlap.
-template <typename V, int NV>
-__device__ __forceinline__ void stage_in(V *tile, const V *src, uint64_t base, const uint64_t *tab, int c) {
-    constexpr int APV = 16 / sizeof(V);
-    constexpr int CH = NV < 8 ? NV : 8;   // vectors in flight per thread (bounded register use)
-    const uint32_t lowmask = (1u << c) - 1u;
-#pragma unroll
-    for (int i0 = 0; i0 < NV; i0 += CH) {
-        uint4 buf[CH];
-#pragma unroll
-        for (int i = 0; i < CH; ++i) {
-            const uint32_t L = (threadIdx.x + uint32_t(i0 + i) * blockDim.x) * APV;
-            const uint64_t gi = base + tab[L >> c] + (L & lowmask);
-            buf[i] = __ldcs(reinterpret_cast<const uint4 *>(src + gi));
-        }
-#pragma unroll
-        for (int i = 0; i < CH; ++i) {
-            const uint32_t L = (threadIdx.x + uint32_t(i0 + i) * blockDim.x) * APV;
-            if (APV == 2) {
-                const V *pv = reinterpret_cast<const V *>(&buf[i]);
-                tile[swz<V>(L)] = pv[0];
-                tile[swz<V>(L + 1)] = pv[1];
-            } else {
-                *reinterpret_cast<uint4 *>(&tile[swz<V>(L)]) = buf[i];
-            }
-        }
-    }
-}
-
-template <typename V>
-__device__ __forceinline__ void stage_zero(V *tile, uint64_t base, int K) {
-    for (int L = threadIdx.x; L < (1 << K); L += blockDim.x) {
-        V v;
-        v.x = (base == 0 && L == 0) ? 1 : 0;
-        v.y = 0;
-        tile[swz<V>(L)] = v;
-    }
-}
-
-template <typename V, int NV>
-__device__ __forceinline__ void stage_out(const V *tile, V *dst, uint64_t base, const uint64_t *tab, int c) {
-    constexpr int APV = 16 / sizeof(V);
-    const uint32_t lowmask = (1u << c) - 1u;
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-        const uint32_t L = (threadIdx.x + uint32_t(i) * blockDim.x) * APV;
-        const uint64_t gi = base + tab[L >> c] + (L & lowmask);
-        uint4 raw;
-        if (APV == 2) {
-            V *pv = reinterpret_cast<V *>(&raw);
-            pv[0] = tile[swz<V>(L)];
-            pv[1] = tile[swz<V>(L + 1)];
-        } else {
-            raw = *reinterpret_cast<const uint4 *>(&tile[swz<V>(L)]);
-        }
-        __stcs(reinterpret_cast<uint4 *>(dst + gi), raw);
-    }
-}
+using mqb::tile::swz;
+using mqb::tile::tile_base;
+using mqb::tile::align16;
+using mqb::tile::build_table;
+using mqb::tile::stage_in;
+using mqb::tile::stage_zero;
+using mqb::tile::stage_out;
 
 // Copy the matrices (and derivative matrices) of every gate of the pass into shared memory.
 template <typename V>
@@ -151,7 +75,7 @@ __global__ void __launch_bounds__(256, 2) fused_fwd2_kernel(const Fwd2Args<R> a)
     size_t o = align16((size_t(1) << K) * sizeof(V));
     V *mtab = reinterpret_cast<V *>(smem + o);
     o = align16(o + size_t(a.mtab_entries) * sizeof(V));
-    uint64_t *tab = reinterpret_cast<uint64_t *>(smem + o);
+    mqb::tile::u64 *tab = reinterpret_cast<mqb::tile::u64 *>(smem + o);
     o = align16(o + (size_t(1) << (K - c)) * sizeof(uint64_t));
     StageDesc *sst = reinterpret_cast<StageDesc *>(smem + o);
     o = align16(o + size_t(a.n_stages) * sizeof(StageDesc));
@@ -218,7 +142,7 @@ __global__ void __launch_bounds__(256, 2) fused_bwd2_kernel(const Bwd2Args<R> a)
     size_t o = align16(size_t(TS) * sizeof(V) * (1 + NH));
     V *mtab = reinterpret_cast<V *>(smem + o);
     o = align16(o + size_t(a.mtab_entries) * sizeof(V));
-    uint64_t *tab = reinterpret_cast<uint64_t *>(smem + o);
+    mqb::tile::u64 *tab = reinterpret_cast<mqb::tile::u64 *>(smem + o);
     o = align16(o + (size_t(1) << (K - c)) * sizeof(uint64_t));
     StageDesc *sst = reinterpret_cast<StageDesc *>(smem + o);
     o = align16(o + size_t(a.n_stages) * sizeof(StageDesc));

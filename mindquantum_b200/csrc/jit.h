@@ -1,0 +1,39 @@
+// Pass kernels generated at run time: each fused pass of a schedule gets its own kernel, in
+// which the stage layouts and every gate (kind, register positions, control masks, matrix-table
+// offsets, gradient slots) are compile-time constants.  The kernels are compiled with NVRTC for
+// sm_100a, cached by source text, and launched with the same arguments the precompiled tile
+// kernels take.
+#ifndef MQB_JIT_H_
+#define MQB_JIT_H_
+
+#include <string>
+#include <vector>
+
+#include "mqb_internal.h"
+
+namespace mqb {
+
+// Per pass of `s`: the forward kernel (nullptr for unfused passes).  Compiles what the cache
+// lacks, in parallel; throws std::runtime_error with the compiler log on failure.
+std::vector<const void *> jit_forward_kernels(const Schedule &s, int precision);
+// Per pass of `s`: the backward kernel for n_hams lambdas.
+std::vector<const void *> jit_backward_kernels(const Schedule &s, int precision, int n_hams);
+
+size_t jit_forward_smem(const Pass &p, int precision);
+size_t jit_backward_smem(const Pass &p, int precision, int n_hams);
+
+// Launch a generated kernel over `work` tiles with 2^(K - RB) threads.
+cudaError_t jit_launch(const void *kernel, void *args, int threads, size_t smem, int sm_count, long long work,
+                       cudaStream_t st);
+
+// Generate and compile (without loading: no GPU needed) the kernels of every fused pass, the
+// backward ones too when n_hams > 0; returns the number of distinct kernels.
+int jit_compile_check(const Schedule &s, int precision, int n_hams);
+
+// Sources of the kernels of one pass (for tests and inspection).
+std::string jit_forward_source(const Schedule &s, const Pass &p, int precision);
+std::string jit_backward_source(const Schedule &s, const Pass &p, int precision, int n_hams);
+
+}  // namespace mqb
+
+#endif

@@ -1,0 +1,65 @@
+// Plain structures shared by the host and the tile kernels generated at run time (compiled by
+// NVRTC, so only built-in types are used here).
+#ifndef MQB_JIT_ABI_H_
+#define MQB_JIT_ABI_H_
+
+namespace mqb {
+
+// Tile geometry of a fused pass: K tile qubits qbits[0..K) (the c low ones contiguous in memory)
+// and the n - K outside qubits that number the tiles.
+struct TileGeom {
+    int n;                  // qubits
+    int K;                  // tile bits
+    int c;                  // contiguity bits
+    int n_out;              // outside bits
+    signed char qbits[13];
+    signed char outside[64];
+};
+
+// Where one op's matrices come from and where they go in the pass's shared-memory table.
+struct JitMtab {
+    int moff;               // offset in the table (complex entries)
+    int mcount;             // entries (M, then dM_0, dM_1, ...)
+    long long msrc;         // offset in the per-sample block or the constant pool
+    int msrc_ps;            // 1: per-sample matrices, 0: constant pool
+    int pad;
+};
+
+template <typename V>
+struct JitFwdArgs {
+    TileGeom g;
+    const JitMtab *mt;
+    int n_mt;
+    int mtab_entries;
+    const V *mats;
+    long long mats_stride;
+    const V *cpool;
+    const V *src;           // nullptr: start from |0...0>
+    V *dst;
+    long long batch;
+    long long src_batch_stride;
+};
+
+template <typename V>
+struct JitBwdArgs {
+    TileGeom g;
+    const JitMtab *mt;
+    int n_mt;
+    int mtab_entries;
+    const V *mats;
+    long long mats_stride;
+    const V *cpool;
+    const V *psi_src;       // state after the pass
+    V *psi_dst;             // state before the pass (nullptr: not stored)
+    V *lam;                 // [n_hams][batch][dim]
+    double *gslots;         // [batch][n_slots][n_hams]
+    const int *slot_map;    // pass-local slot -> global slot
+    int n_slots;
+    int n_hams;
+    int n_local_slots;
+    long long batch;
+};
+
+}  // namespace mqb
+
+#endif

@@ -10,12 +10,13 @@
 #include <vector>
 
 #include "../../include/mqb200.h"
+#include "jit_abi.h"
 #include "mqb_gate_ids.h"
 
 namespace mqb {
 
 constexpr int kMaxFusedM = 2;        // gates with <= 2 targets run inside fused tiles
-constexpr int kMaxTileBits = 13;     // upper bound of the tile size 2^K
+constexpr int kMaxTileBits = 13;     // upper bound of the tile size 2^K (TileGeom::qbits)
 constexpr int kMaxPassOps = 256;     // ops of one fused pass (staged in shared memory)
 constexpr int kMaxPassSlots = 96;    // gradient slots of one fused pass (accumulated in shared memory)
 constexpr int kMaxGroupClasses = 64; // flip classes of one Hamiltonian pass
@@ -155,16 +156,6 @@ struct Schedule {
     StageOp *d_stage_ops = nullptr;
 };
 
-// Kernel-facing description of a fused pass (passed by value).
-struct TileGeom {
-    int32_t n;          // qubits
-    int32_t K;          // tile bits
-    int32_t c;          // contiguity bits
-    int32_t n_out;      // outside bits
-    int8_t qbits[kMaxTileBits];
-    int8_t outside[64];
-};
-
 // Hamiltonian: terms grouped into passes; every group's flip masks fit in one tile.
 struct HamTerm {
     double coeff;
@@ -181,6 +172,19 @@ struct HamClass {       // terms sharing one flip mask
 struct HamGroup {
     TileGeom geom;
     int class_begin, class_count;
+};
+
+// While alive, calls on this thread run the precompiled tile kernels only: no pass kernel is
+// generated or loaded (callers that promise to allocate nothing).
+class JitBlock {
+  public:
+    JitBlock();
+    ~JitBlock();
+    JitBlock(const JitBlock &) = delete;
+    JitBlock &operator=(const JitBlock &) = delete;
+
+  private:
+    bool prev_;
 };
 
 // Builders (scheduler.cpp)

@@ -22,6 +22,7 @@
 #include <mutex>
 
 #include "../../include/mqb200.h"
+#include "mqb_internal.h"
 
 namespace mqb {
 void set_last_error(const char *msg);   // capi.cpp: the message mqb_last_error() returns on this thread
@@ -78,6 +79,7 @@ MQB_API int mqb_apply_static(mqb_program *prog, void *states, int64_t batch, con
         }
         scratch = g_static_ptr[dev];
     }
+    mqb::JitBlock no_generated_kernels;   // loading a generated kernel would allocate device memory
     return mqb_apply(prog, states, batch, params, param_stride, custom, scratch, kStaticScratchBytes, stream);
 }
 

@@ -1,4 +1,4 @@
-// Register kernels of the fused tile passes (sm_100a).
+// Register-op dispatch of the precompiled fused tile kernels (sm_100a).
 //
 // Inside a register stage every thread holds the 2^RB amplitudes of the tile whose tile-local
 // indices differ in the stage's RB register bits.  A gate of the stage is resolved on the host
@@ -19,62 +19,10 @@
 
 #include "kernels.cuh"
 
+#include "regmath.cuh"
+
 namespace mqb {
 namespace reg {
-
-template <typename V>
-__device__ __forceinline__ V cmul(V a, V b) {
-    V r;
-    r.x = a.x * b.x - a.y * b.y;
-    r.y = a.x * b.y + a.y * b.x;
-    return r;
-}
-template <typename V>
-__device__ __forceinline__ V cmadd(V a, V b, V c) {  // a * b + c
-    V r;
-    r.x = fma(a.x, b.x, fma(-a.y, b.y, c.x));
-    r.y = fma(a.x, b.y, fma(a.y, b.x, c.y));
-    return r;
-}
-template <typename V>
-__device__ __forceinline__ V cconj(V a) {
-    a.y = -a.y;
-    return a;
-}
-template <typename V, typename R>
-__device__ __forceinline__ V rlin(R a, V x, R b, V y) {  // a x + b y, a and b real
-    V r;
-    r.x = fma(a, x.x, b * y.x);
-    r.y = fma(a, x.y, b * y.y);
-    return r;
-}
-template <typename V, typename R>
-__device__ __forceinline__ V rxl(R a, V x, R b, V y) {  // a x + i b y, a and b real
-    V r;
-    r.x = fma(a, x.x, -b * y.y);
-    r.y = fma(a, x.y, b * y.x);
-    return r;
-}
-template <typename V>
-__device__ __forceinline__ decltype(V::x) redot(V l, V y) {  // Re(conj(l) y)
-    return fma(l.x, y.x, l.y * y.y);
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Register index j takes part in a gate on position P with single control position C (C < 0: none).
-template <int P, int C>
-__device__ __forceinline__ constexpr bool active(int j) {
-    return !((j >> P) & 1) && (C < 0 || ((j >> (C < 0 ? 0 : C)) & 1));
-}
-template <int C>
-__device__ __forceinline__ constexpr bool ctl_on(int j) {
-    return C < 0 || ((j >> (C < 0 ? 0 : C)) & 1);
-}
 
 // Bit of an off-register diagonal target: src 1 thread (tile-local bit of Lt), 2 outside (global
 // qubit of base), 3 absent (0).  src 0 (register position) only occurs in generic ops.
@@ -92,102 +40,61 @@ __device__ __forceinline__ int scale_index(const StageOp &so, uint32_t Lt, uint6
     return off_bit(so.dsrc[0], so.dval[0], Lt, base) | (off_bit(so.dsrc[1], so.dval[1], Lt, base) << 1);
 }
 
-// ============================================================================ forward (U psi)
+// ================================================================= forward (U psi)
+// Interpreter forms: matrices read from the pass's matrix table M; C = single register control
+// position (-1: none).
+__host__ __device__ constexpr unsigned cmask(int c) { return c < 0 ? 0u : (1u << c); }
 
 template <typename V, int RB, int P, int C>
 __device__ __forceinline__ void f_dense1(V (&v)[1 << RB], const V *M) {
-    const V m00 = M[0], m01 = M[1], m10 = M[2], m11 = M[3];
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!active<P, C>(j)) continue;
-        const V a = v[j], b = v[j | (1 << P)];
-        v[j] = cmadd(m00, a, cmul(m01, b));
-        v[j | (1 << P)] = cmadd(m10, a, cmul(m11, b));
-    }
+    j_dense1<V, RB, P, cmask(C)>(v, M[0], M[1], M[2], M[3]);
 }
-
 template <typename V, int RB, int P, int C>
 __device__ __forceinline__ void f_real1(V (&v)[1 << RB], const V *M) {
-    const auto m00 = M[0].x, m01 = M[1].x, m10 = M[2].x, m11 = M[3].x;
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!active<P, C>(j)) continue;
-        const V a = v[j], b = v[j | (1 << P)];
-        v[j] = rlin(m00, a, m01, b);
-        v[j | (1 << P)] = rlin(m10, a, m11, b);
-    }
+    j_real1<V, RB, P, cmask(C)>(v, M[0].x, M[1].x, M[2].x, M[3].x);
 }
-
-// [[a, i b], [i b, a]] with a, b real (RX)
 template <typename V, int RB, int P, int C>
 __device__ __forceinline__ void f_rxl1(V (&v)[1 << RB], const V *M) {
-    const auto a = M[0].x, b = M[1].y;
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!active<P, C>(j)) continue;
-        const V x0 = v[j], x1 = v[j | (1 << P)];
-        v[j] = rxl(a, x0, b, x1);
-        v[j | (1 << P)] = rxl(a, x1, b, x0);
-    }
+    j_rxl1<V, RB, P, cmask(C)>(v, M[0].x, M[1].y);
 }
-
 template <typename V, int RB, int P, int C>
 __device__ __forceinline__ void f_x1(V (&v)[1 << RB]) {
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!active<P, C>(j)) continue;
-        const V a = v[j];
-        v[j] = v[j | (1 << P)];
-        v[j | (1 << P)] = a;
-    }
+    j_x1<V, RB, P, cmask(C)>(v);
 }
-
 template <typename V, int RB, int P, int C>
 __device__ __forceinline__ void f_diag1(V (&v)[1 << RB], V d0, V d1) {
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!ctl_on<C>(j)) continue;
-        v[j] = cmul(v[j], ((j >> P) & 1) ? d1 : d0);
-    }
+    j_diag1<V, RB, P, cmask(C)>(v, d0, d1);
 }
-
 template <typename V, int RB, int C>
 __device__ __forceinline__ void f_scale(V (&v)[1 << RB], V d) {
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!ctl_on<C>(j)) continue;
-        v[j] = cmul(v[j], d);
-    }
+    j_scale<V, RB, cmask(C)>(v, d);
 }
-
-// diagonal on two register positions: P carries matrix bit 0, Q matrix bit 1
 template <typename V, int RB, int P, int Q>
 __device__ __forceinline__ void f_diag2(V (&v)[1 << RB], const V *M) {
-    const V d0 = M[0], d1 = M[1], d2 = M[2], d3 = M[3];
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        const int r = ((j >> P) & 1) | (((j >> Q) & 1) << 1);
-        v[j] = cmul(v[j], r == 0 ? d0 : r == 1 ? d1 : r == 2 ? d2 : d3);
-    }
+    j_diag2<V, RB, P, Q, 0u>(v, M[0], M[1], M[2], M[3]);
 }
 
-// dense 4x4: P carries matrix bit 0, Q matrix bit 1; MASK (runtime) = register controls
+// dense 4x4 with a runtime register control mask (GEN) or none
 template <typename V, int RB, int P, int Q, bool GEN>
-__device__ __forceinline__ void f_dense2(V (&v)[1 << RB], const V *M, uint32_t mask) {
+__device__ __forceinline__ void f_dense2(V (&v)[1 << RB], const V *M, unsigned mask) {
+    if constexpr (!GEN) {
+        j_dense2<V, RB, P, Q, 0u>(v, M);
+    } else {
 #pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (((j >> P) & 1) || ((j >> Q) & 1)) continue;
-        if (GEN && (uint32_t(j) & mask) != mask) continue;
-        const int id[4] = {j, j | (1 << P), j | (1 << Q), j | (1 << P) | (1 << Q)};
-        V x[4];
+        for (int j = 0; j < (1 << RB); ++j) {
+            if (((j >> P) & 1) || ((j >> Q) & 1)) continue;
+            if ((unsigned(j) & mask) != mask) continue;
+            const int id[4] = {j, j | (1 << P), j | (1 << Q), j | (1 << P) | (1 << Q)};
+            V x[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) x[r] = v[id[r]];
+            for (int r = 0; r < 4; ++r) x[r] = v[id[r]];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            V s = cmul(M[r * 4], x[0]);
+            for (int r = 0; r < 4; ++r) {
+                V s = cmul(M[r * 4], x[0]);
 #pragma unroll
-            for (int c = 1; c < 4; ++c) s = cmadd(M[r * 4 + c], x[c], s);
-            v[id[r]] = s;
+                for (int c = 1; c < 4; ++c) s = cmadd(M[r * 4 + c], x[c], s);
+                v[id[r]] = s;
+            }
         }
     }
 }
@@ -327,36 +234,43 @@ __device__ __forceinline__ void fwd_op(int code, V (&v)[1 << RB], const V *M, co
 }
 
 // ============================================== backward (psi <- U^dag psi, gradients, lambda)
-// acc[a][h] += Re<lambda_h | dU/d angle_a | psi'> over the thread's amplitudes, psi' = U^dag psi,
-// lambda_h taken before its own uncompute.  G: gradient-angle mask (compile time), or -1 for the
-// runtime mask gm.  Derivative matrices follow M in the table: dM_a = M + (1 + a) * size(M).
+// Interpreter forms over the register math of regmath.cuh: U and dU_a = M + (1 + a) size(M)
+// read from the matrix table.  C = -2 marks a runtime register control mask, G = -1 a runtime
+// gradient mask (the generic codes).
 
 template <typename V, int RB, int NH, int P, int C, int G>
 __device__ __forceinline__ void b_dense1(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M, int gm, uint32_t mask,
                                          decltype(V::x) (&acc)[3][NH]) {
     const V a00 = cconj(M[0]), a01 = cconj(M[2]), a10 = cconj(M[1]), a11 = cconj(M[3]);
-    const int gmask = G >= 0 ? G : gm;
+    if constexpr (C >= -1 && G >= 0) {
+        V d[3][4];
 #pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!active<P, C>(j)) continue;
-        if (C == -2 && (uint32_t(j) & mask) != mask) continue;   // generic: runtime control mask
-        constexpr int bit = 1 << P;
-        const V w0 = cmadd(a00, v[j], cmul(a01, v[j | bit])), w1 = cmadd(a10, v[j], cmul(a11, v[j | bit]));
-        v[j] = w0;
-        v[j | bit] = w1;
+        for (int an = 0; an < 3; ++an)
 #pragma unroll
-        for (int an = 0; an < 3; ++an) {
-            if (!((gmask >> an) & 1)) continue;
-            const V *d = M + 4 + an * 4;
-            const V y0 = cmadd(d[0], w0, cmul(d[1], w1)), y1 = cmadd(d[2], w0, cmul(d[3], w1));
+            for (int e = 0; e < 4; ++e) d[an][e] = ((G >> an) & 1) ? M[4 + an * 4 + e] : cval<V>(0, 0);
+        jb_dense1<V, RB, NH, P, cmask(C), G>(v, l, a00, a01, a10, a11, d, acc);
+    } else {
 #pragma unroll
-            for (int h = 0; h < NH; ++h) acc[an][h] += redot(l[h][j], y0) + redot(l[h][j | bit], y1);
-        }
+        for (int j = 0; j < (1 << RB); ++j) {
+            if (((j >> P) & 1) || (uint32_t(j) & mask) != mask) continue;
+            constexpr int bit = 1 << P;
+            const V w0 = cmadd(a00, v[j], cmul(a01, v[j | bit])), w1 = cmadd(a10, v[j], cmul(a11, v[j | bit]));
+            v[j] = w0;
+            v[j | bit] = w1;
 #pragma unroll
-        for (int h = 0; h < NH; ++h) {
-            const V x0 = l[h][j], x1 = l[h][j | bit];
-            l[h][j] = cmadd(a00, x0, cmul(a01, x1));
-            l[h][j | bit] = cmadd(a10, x0, cmul(a11, x1));
+            for (int an = 0; an < 3; ++an) {
+                if (!((gm >> an) & 1)) continue;
+                const V *d = M + 4 + an * 4;
+                const V y0 = cmadd(d[0], w0, cmul(d[1], w1)), y1 = cmadd(d[2], w0, cmul(d[3], w1));
+#pragma unroll
+                for (int h = 0; h < NH; ++h) acc[an][h] += redot(l[h][j], y0) + redot(l[h][j | bit], y1);
+            }
+#pragma unroll
+            for (int h = 0; h < NH; ++h) {
+                const V x0 = l[h][j], x1 = l[h][j | bit];
+                l[h][j] = cmadd(a00, x0, cmul(a01, x1));
+                l[h][j | bit] = cmadd(a10, x0, cmul(a11, x1));
+            }
         }
     }
 }
@@ -364,131 +278,44 @@ __device__ __forceinline__ void b_dense1(V (&v)[1 << RB], V (&l)[NH][1 << RB], c
 template <typename V, int RB, int NH, int P, int C, int G>
 __device__ __forceinline__ void b_real1(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M,
                                         decltype(V::x) (&acc)[3][NH]) {
-    const auto a00 = M[0].x, a01 = M[2].x, a10 = M[1].x, a11 = M[3].x;   // U^dag = U^T
-    decltype(V::x) d00 = 0, d01 = 0, d10 = 0, d11 = 0;
-    if (G & 1) {
-        d00 = M[4].x;
-        d01 = M[5].x;
-        d10 = M[6].x;
-        d11 = M[7].x;
-    }
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!active<P, C>(j)) continue;
-        constexpr int bit = 1 << P;
-        const V w0 = rlin(a00, v[j], a01, v[j | bit]), w1 = rlin(a10, v[j], a11, v[j | bit]);
-        v[j] = w0;
-        v[j | bit] = w1;
-        if (G & 1) {
-            const V y0 = rlin(d00, w0, d01, w1), y1 = rlin(d10, w0, d11, w1);
-#pragma unroll
-            for (int h = 0; h < NH; ++h) acc[0][h] += redot(l[h][j], y0) + redot(l[h][j | bit], y1);
-        }
-#pragma unroll
-        for (int h = 0; h < NH; ++h) {
-            const V x0 = l[h][j], x1 = l[h][j | bit];
-            l[h][j] = rlin(a00, x0, a01, x1);
-            l[h][j | bit] = rlin(a10, x0, a11, x1);
-        }
-    }
+    using R = decltype(V::x);
+    const R z = 0;
+    jb_real1<V, RB, NH, P, cmask(C), G>(v, l, M[0].x, M[2].x, M[1].x, M[3].x, (G & 1) ? M[4].x : z,
+                                        (G & 1) ? M[5].x : z, (G & 1) ? M[6].x : z, (G & 1) ? M[7].x : z, acc);
 }
 
-// U = [[a, i b], [i b, a]]: U^dag = [[a, -i b], [-i b, a]]; dU has the same form
 template <typename V, int RB, int NH, int P, int C, int G>
 __device__ __forceinline__ void b_rxl1(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M,
                                        decltype(V::x) (&acc)[3][NH]) {
-    const auto a = M[0].x, nb = -M[1].y;
-    decltype(V::x) da = 0, db = 0;
-    if (G & 1) {
-        da = M[4].x;
-        db = M[5].y;
-    }
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!active<P, C>(j)) continue;
-        constexpr int bit = 1 << P;
-        const V x0 = v[j], x1 = v[j | bit];
-        const V w0 = rxl(a, x0, nb, x1), w1 = rxl(a, x1, nb, x0);
-        v[j] = w0;
-        v[j | bit] = w1;
-        if (G & 1) {
-            const V y0 = rxl(da, w0, db, w1), y1 = rxl(da, w1, db, w0);
-#pragma unroll
-            for (int h = 0; h < NH; ++h) acc[0][h] += redot(l[h][j], y0) + redot(l[h][j | bit], y1);
-        }
-#pragma unroll
-        for (int h = 0; h < NH; ++h) {
-            const V z0 = l[h][j], z1 = l[h][j | bit];
-            l[h][j] = rxl(a, z0, nb, z1);
-            l[h][j | bit] = rxl(a, z1, nb, z0);
-        }
-    }
+    using R = decltype(V::x);
+    const R z = 0;
+    jb_rxl1<V, RB, NH, P, cmask(C), G>(v, l, M[0].x, -M[1].y, (G & 1) ? M[4].x : z, (G & 1) ? M[5].y : z, acc);
 }
 
 template <typename V, int RB, int NH, int P, int C>
 __device__ __forceinline__ void b_x1(V (&v)[1 << RB], V (&l)[NH][1 << RB]) {
-    f_x1<V, RB, P, C>(v);
-#pragma unroll
-    for (int h = 0; h < NH; ++h) f_x1<V, RB, P, C>(l[h]);
+    jb_x1<V, RB, NH, P, cmask(C)>(v, l);
 }
 
 // diagonal with target on register P: entries (d0, d1), derivative entries (e0, e1)
 template <typename V, int RB, int NH, int P, int C, int G>
 __device__ __forceinline__ void b_diag1(V (&v)[1 << RB], V (&l)[NH][1 << RB], V d0, V d1, V e0, V e1,
                                         decltype(V::x) (&acc)[3][NH]) {
-    const V c0 = cconj(d0), c1 = cconj(d1);
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!ctl_on<C>(j)) continue;
-        const bool hi = (j >> P) & 1;
-        const V w = cmul(v[j], hi ? c1 : c0);
-        v[j] = w;
-        if (G & 1) {
-            const V y = cmul(hi ? e1 : e0, w);
-#pragma unroll
-            for (int h = 0; h < NH; ++h) acc[0][h] += redot(l[h][j], y);
-        }
-#pragma unroll
-        for (int h = 0; h < NH; ++h) l[h][j] = cmul(l[h][j], hi ? c1 : c0);
-    }
+    jb_diag1<V, RB, NH, P, cmask(C), G>(v, l, cconj(d0), cconj(d1), e0, e1, acc);
 }
 
 template <typename V, int RB, int NH, int C, int G>
 __device__ __forceinline__ void b_scale(V (&v)[1 << RB], V (&l)[NH][1 << RB], V d, V e,
                                         decltype(V::x) (&acc)[3][NH]) {
-    const V c = cconj(d);
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (!ctl_on<C>(j)) continue;
-        const V w = cmul(v[j], c);
-        v[j] = w;
-        if (G & 1) {
-            const V y = cmul(e, w);
-#pragma unroll
-            for (int h = 0; h < NH; ++h) acc[0][h] += redot(l[h][j], y);
-        }
-#pragma unroll
-        for (int h = 0; h < NH; ++h) l[h][j] = cmul(l[h][j], c);
-    }
+    jb_scale<V, RB, NH, cmask(C), G>(v, l, cconj(d), e, acc);
 }
 
 template <typename V, int RB, int NH, int P, int Q, int G>
 __device__ __forceinline__ void b_diag2(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M,
                                         decltype(V::x) (&acc)[3][NH]) {
-#pragma unroll
-    for (int j = 0; j < (1 << RB); ++j) {
-        const int r = ((j >> P) & 1) | (((j >> Q) & 1) << 1);
-        const V c = cconj(M[r]);
-        const V w = cmul(v[j], c);
-        v[j] = w;
-        if (G & 1) {
-            const V y = cmul(M[4 + r], w);
-#pragma unroll
-            for (int h = 0; h < NH; ++h) acc[0][h] += redot(l[h][j], y);
-        }
-#pragma unroll
-        for (int h = 0; h < NH; ++h) l[h][j] = cmul(l[h][j], c);
-    }
+    const V c[4] = {cconj(M[0]), cconj(M[1]), cconj(M[2]), cconj(M[3])};
+    const V e[4] = {(G & 1) ? M[4] : c[0], (G & 1) ? M[5] : c[0], (G & 1) ? M[6] : c[0], (G & 1) ? M[7] : c[0]};
+    jb_diag2<V, RB, NH, P, Q, 0u, G>(v, l, c, e, acc);
 }
 
 template <typename V, int RB, int NH, int P, int Q, int G, bool GEN>

@@ -115,9 +115,11 @@ class Program:
         param_names: order of the parameter vector the program reads.
         grad_names: names whose gradients are wanted (others get no gradient slot).
         fuse: fused tile passes (default) or one kernel per gate (the reference's schedule).
+        tile_bits: tile width of the fused passes (0: automatic).
+        jit: generated pass kernels (None automatic, True always, False never).
     """
 
-    def __init__(self, circuit, n_qubits, precision, param_names, grad_names=None, fuse=True, tile_bits=0):
+    def __init__(self, circuit, n_qubits, precision, param_names, grad_names=None, fuse=True, tile_bits=0, jit=None):
         self.n_qubits = n_qubits
         self.precision = precision
         self.param_names = list(param_names)
@@ -132,6 +134,7 @@ class Program:
         opts = N.ProgramOptions()
         opts.fuse = 1 if fuse else 0
         opts.tile_bits = tile_bits
+        opts.jit = 0 if jit is None else (1 if jit else -1)
         handle = ctypes.c_void_p()
         N.call('mqb_program_create', n_qubits, precision, gate_arr, len(descs), term_arr, len(terms),
                len(self.param_names), self._pool.ctypes.data_as(ctypes.c_void_p), pool_arr.size,
@@ -197,10 +200,27 @@ def plan_schedule(circuit, n_qubits, precision, tile_bits=0, fuse=True):
     return order[:n], pass_of[:n], qmask[:k], fused[:k]
 
 
-def lowered(circuit, n_qubits, precision, param_names, grad_names=None, fuse=True, tile_bits=0):
+def jit_check(circuit, n_qubits, precision, tile_bits=0, n_hams=0):
+    """Generate and compile (NVRTC, no GPU needed) the pass kernels of ``circuit``.
+
+    Forward kernels, plus the backward kernels for ``n_hams`` Hamiltonians when n_hams > 0.
+    Returns the number of distinct kernels; raises with the compiler log on failure.
+    """
+    descs, _, pool, _, _ = lower_circuit(circuit, circuit.params_name)
+    n = len(descs)
+    gate_arr = (N.GateDesc * max(1, n))(*descs)
+    pool_arr = np.concatenate(pool) if pool else np.zeros(1, dtype=np.complex128)
+    pool_f = np.ascontiguousarray(pool_arr.astype(np.complex128)).view(np.float64)
+    count = ctypes.c_int()
+    N.call('mqb_jit_check', n_qubits, precision, gate_arr, n, pool_f.ctypes.data_as(ctypes.c_void_p), pool_arr.size,
+           tile_bits, n_hams, ctypes.byref(count))
+    return count.value
+
+
+def lowered(circuit, n_qubits, precision, param_names, grad_names=None, fuse=True, tile_bits=0, jit=None):
     """Program for ``circuit`` cached on the circuit object (invalidated when the circuit changes)."""
     key = (n_qubits, precision, tuple(param_names), None if grad_names is None else tuple(grad_names), fuse,
-           tile_bits, len(circuit))
+           tile_bits, jit, len(circuit))
     cache = getattr(circuit, '_mqb_cache', None)
     if cache is None:
         cache = {}
@@ -210,7 +230,7 @@ def lowered(circuit, n_qubits, precision, param_names, grad_names=None, fuse=Tru
             pass
     prog = cache.get(key)
     if prog is None:
-        prog = Program(circuit, n_qubits, precision, param_names, grad_names, fuse, tile_bits)
+        prog = Program(circuit, n_qubits, precision, param_names, grad_names, fuse, tile_bits, jit)
         cache[key] = prog
     return prog
 

@@ -49,10 +49,12 @@ class MQVectorB200(BackendBase):
         seed: seed of the measurement random stream (std::mt19937 as in the reference).
         dtype: ``complex128`` (default) or ``complex64``.
         fuse: fused tile passes (default) or one kernel per gate.
+        jit: generated pass kernels: None automatic (registers of 18 qubits and more), True always,
+            False never (the precompiled tile kernels).
         device: CUDA device (default: the current one).
     """
 
-    def __init__(self, name, n_qubits, seed=None, dtype=None, fuse=True, device=None):
+    def __init__(self, name, n_qubits, seed=None, dtype=None, fuse=True, device=None, jit=None):
         _require_cuda()
         super().__init__(name, n_qubits, seed, dtype)
         if not isinstance(n_qubits, int) or n_qubits < 1:
@@ -61,6 +63,7 @@ class MQVectorB200(BackendBase):
             seed = int(np.random.randint(1, 2**23))
         self.seed = int(seed)
         self.fuse = fuse
+        self.jit = jit
         self.device = torch.device('cuda', torch.cuda.current_device()) if device is None else torch.device(device)
         self._state = None          # None means |0...0>, like the reference's null state
         self._rng = Mt19937Uniform(self.seed)
@@ -99,13 +102,14 @@ class MQVectorB200(BackendBase):
         self._state = None
 
     def copy(self):
-        sim = MQVectorB200(self.name, self.n_qubits, self.seed, self.arithmetic_type, self.fuse, self.device)
+        sim = MQVectorB200(self.name, self.n_qubits, self.seed, self.arithmetic_type, self.fuse, self.device, self.jit)
         if self._state is not None:
             sim._state = self._state.clone()
         return sim
 
     def astype(self, dtype, seed=None):
-        sim = MQVectorB200(self.name, self.n_qubits, self.seed if seed is None else seed, dtype, self.fuse, self.device)
+        sim = MQVectorB200(self.name, self.n_qubits, self.seed if seed is None else seed, dtype, self.fuse, self.device,
+                           self.jit)
         if self._state is not None:
             sim._state = self._state.to(sim.torch_dtype)
         return sim
@@ -154,7 +158,7 @@ class MQVectorB200(BackendBase):
     def _apply_segment(self, states, circuit, pr, batch=1):
         """Apply a measurement-free circuit in place to ``states`` ([batch][2^n])."""
         names = circuit.params_name
-        prog = lowered(circuit, self.n_qubits, self.precision, names, None, self.fuse)
+        prog = lowered(circuit, self.n_qubits, self.precision, names, None, self.fuse, jit=self.jit)
         if prog.n_gates == 0:
             return
         params, params_np = self._params_tensor(prog, pr)
@@ -309,7 +313,7 @@ class MQVectorB200(BackendBase):
         Returns:
             f: float64 [batch][n_hams][2] (re, im); grad: float64 [batch][n_hams][n_params].
         """
-        prog = lowered(circuit, self.n_qubits, self.precision, param_names, grad_names, self.fuse)
+        prog = lowered(circuit, self.n_qubits, self.precision, param_names, grad_names, self.fuse, jit=self.jit)
         nh = [native_ham(h, self.n_qubits, self.precision) for h in hams]
         params = params.to(device=self.device, dtype=torch.float64).contiguous()
         batch = params.shape[0]
