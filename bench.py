@@ -307,6 +307,7 @@ def run_b200(args, rank, world, local_rank):
         # accuracy: the same parameter set in complex128 (fused, FP64 throughout)
         s128 = MQVectorB200('mqvector_b200', n, dtype=complex128, device=dev)
         p1 = params[:1]
+        s128.expectation_with_grad_tensor([ham], circ, p1, names, ckpt_stride=0)   # compiles the pass kernels
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         f128, g128 = s128.expectation_with_grad_tensor([ham], circ, p1, names, ckpt_stride=0)

@@ -196,7 +196,7 @@ static const std::vector<const void *> *jit_backward(const mqb_program &p, Sched
     if (!p.use_jit() || t_jit_blocked || sd.s.passes.empty()) return nullptr;
     std::lock_guard<std::mutex> lk(sd.jit_mu);
     auto &v = sd.jit_bwd[n_hams];
-    if (v.empty()) v = jit_backward_kernels(sd.s, p.precision, n_hams);
+    if (v.empty()) v = jit_backward_kernels(sd.s, p.precision, n_hams, p.ops);
     return &v;
 }
 
@@ -818,7 +818,7 @@ int mqb_jit_check(int n_qubits, int precision, const mqb_gate_desc *gates, int n
         Schedule s = build_schedule(n_qubits, K, contiguity_bits(precision), ops, K >= rb + 5);
         build_stages(s, ops, rb, precision, false);
         build_stages(s, ops, fwd_reg_bits(precision), precision, true);
-        *n_kernels = jit_compile_check(s, precision, n_hams);
+        *n_kernels = jit_compile_check(s, precision, n_hams, ops);
     });
 }
 

@@ -163,7 +163,26 @@ void emit_forward_op(std::ostringstream &o, const StageOp &so) {
 }
 
 // ------------------------------------------------------------------------------ backward ops
-void emit_backward_op(std::ostringstream &o, const StageOp &so, int NH) {
+// Generator weights of the diagonal phase gates (dU/dt = -i W U, W real diagonal); empty when the
+// gate's gradient goes through its derivative matrix instead.
+std::vector<double> phase_weights(int gid) {
+    switch (gid) {
+        case GID_RZ: return {0.5, -0.5};
+        case GID_PS: return {0.0, -1.0};
+        case GID_GP: return {1.0, 1.0};
+        case GID_RZZ: return {0.5, -0.5, -0.5, 0.5};
+        default: return {};
+    }
+}
+
+std::string lit(double x) {
+    std::ostringstream o;
+    o.precision(17);
+    o << "R(" << x << ")";
+    return o.str();
+}
+
+void emit_backward_op(std::ostringstream &o, const StageOp &so, int NH, int gid) {
     const std::string on = on_expr(so);
     const bool cond = !on.empty();
     const int M = so.moff;
@@ -178,6 +197,49 @@ void emit_backward_op(std::ostringstream &o, const StageOp &so, int NH) {
     auto sel = [&](const std::string &val, const std::string &id) { return cond ? "(on ? " + val + " : " + id + ")" : val; };
     const std::string one = "cval<V>(1, 0)", zero = "cval<V>(0, 0)";
     auto dm = [&](int a, int e) { return mt(M + ms * (1 + a) + e); };
+    const std::vector<double> pw = (G == 1) ? phase_weights(gid) : std::vector<double>();
+    const bool gen_ry = G == 1 && gid == GID_RY && so.kind == SK_REAL1;
+    const bool gen_rx = G == 1 && gid == GID_RX && so.kind == SK_RXL1;
+    const bool gen_diag = !pw.empty() && (so.kind == SK_DIAG1 || so.kind == SK_DIAG2);
+    auto wsel = [&](const std::string &w) { return cond ? "(on ? " + w + " : R(0))" : w; };
+    if (gen_ry) {
+        o << "      jbg_ry<V, RB, NH, " << so.p0 << ", " << CM << ">(v, l, " << sel(mt(M) + ".x", "R(1)") << ", "
+          << sel(mt(M + 2) + ".x", "R(0)") << ", " << sel(mt(M + 1) + ".x", "R(0)") << ", "
+          << sel(mt(M + 3) + ".x", "R(1)") << ", " << wsel("R(0.5)") << ", acc);\n";
+    } else if (gen_rx) {
+        o << "      jbg_rx<V, RB, NH, " << so.p0 << ", " << CM << ">(v, l, " << sel(mt(M) + ".x", "R(1)") << ", "
+          << sel("-" + mt(M + 1) + ".y", "R(0)") << ", " << wsel("R(0.5)") << ", acc);\n";
+    } else if (gen_diag) {
+        const bool two = so.kind == SK_DIAG2;
+        const bool in0 = so.dsrc[0] == 0, in1 = two && so.dsrc[1] == 0;
+        auto c = [&](const std::string &idx) { return sel("cconj(mt[" + std::to_string(M) + " + " + idx + "])", one); };
+        if (!two && in0) {
+            o << "      jbg_diag1<V, RB, NH, " << so.dval[0] << ", " << CM << ">(v, l, " << c("0") << ", " << c("1")
+              << ", " << wsel(lit(pw[0])) << ", " << wsel(lit(pw[1])) << ", acc);\n";
+        } else if (two && in0 && in1) {
+            o << "      const V c[4] = {" << c("0") << ", " << c("1") << ", " << c("2") << ", " << c("3") << "};\n";
+            o << "      const R w[4] = {" << wsel(lit(pw[0])) << ", " << wsel(lit(pw[1])) << ", " << wsel(lit(pw[2]))
+              << ", " << wsel(lit(pw[3])) << "};\n";
+            o << "      jbg_diag2<V, RB, NH, " << so.dval[0] << ", " << so.dval[1] << ", " << CM << ">(v, l, c, w, acc);\n";
+        } else if (two && (in0 || in1)) {
+            const int k = in0 ? 0 : 1;
+            o << "      const int b = " << off_bit_expr(so.dsrc[1 - k], so.dval[1 - k]) << ";\n";
+            if (k == 0) o << "      const int i0 = b << 1, i1 = 1 | (b << 1);\n";
+            else o << "      const int i0 = b, i1 = 2 | b;\n";
+            // weights of the register bit's two values, picked by the other target's bit (selects, no indexing)
+            const std::string w_lo = k == 0 ? "(b ? " + lit(pw[2]) + " : " + lit(pw[0]) + ")" : "(b ? " + lit(pw[1]) + " : " + lit(pw[0]) + ")";
+            const std::string w_hi = k == 0 ? "(b ? " + lit(pw[3]) + " : " + lit(pw[1]) + ")" : "(b ? " + lit(pw[3]) + " : " + lit(pw[2]) + ")";
+            o << "      jbg_diag1<V, RB, NH, " << so.dval[k] << ", " << CM << ">(v, l, " << c("i0") << ", " << c("i1")
+              << ", " << wsel(w_lo) << ", " << wsel(w_hi) << ", acc);\n";
+        } else {
+            o << "      const int r = " << off_bit_expr(so.dsrc[0], so.dval[0]) << " | ("
+              << off_bit_expr(two ? so.dsrc[1] : 3, so.dval[1]) << " << 1);\n";
+            const std::string w_r = pw.size() > 2 ? "(r == 0 ? " + lit(pw[0]) + " : r == 1 ? " + lit(pw[1]) + " : r == 2 ? " +
+                                                        lit(pw[2]) + " : " + lit(pw[3]) + ")"
+                                                  : "(r ? " + lit(pw[1]) + " : " + lit(pw[0]) + ")";
+            o << "      jbg_scale<V, RB, NH, " << CM << ">(v, l, " << c("r") << ", " << wsel(w_r) << ", acc);\n";
+        }
+    } else
     switch (so.kind) {
         case SK_DENSE1:
         case SK_PERM1: {
@@ -259,6 +321,9 @@ void emit_backward_op(std::ostringstream &o, const StageOp &so, int NH) {
     o << "    }\n";
 }
 
+// Blocks per SM the register budget is sized for: 512 threads per SM at 128 registers each.
+int min_blocks(int TB) { return std::max(1, 512 >> TB); }
+
 void emit_header(std::ostringstream &o, int precision) {
     o << "#include \"regmath.cuh\"\n#include \"tile.cuh\"\n"
       << "using namespace mqb;\nusing namespace mqb::reg;\n"
@@ -297,7 +362,8 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
     const int RB = p.f_reg_bits, K = p.K, TB = K - RB;
     std::ostringstream o;
     emit_header(o, precision);
-    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) << ", 2) mqb_pass(const JitFwdArgs<V> a) {\n"
+    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) << ", " << min_blocks(TB)
+      << ") mqb_pass(const JitFwdArgs<V> a) {\n"
       << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", C = " << p.c << ";\n"
       << "  constexpr int NV = NR / (16 / int(sizeof(V)));\n"
       << "  extern __shared__ __align__(16) unsigned char smem[];\n"
@@ -327,12 +393,13 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
     return o.str();
 }
 
-std::string backward_source(const Schedule &s, const Pass &p, int precision, int NH) {
+std::string backward_source(const Schedule &s, const Pass &p, int precision, int NH, const std::vector<DevOp> &ops) {
     const int RB = p.reg_bits, K = p.K, TB = K - RB;
     const int NLS = std::max(1, p.n_slots);
     std::ostringstream o;
     emit_header(o, precision);
-    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) << ", 2) mqb_pass(const JitBwdArgs<V> a) {\n"
+    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) << ", " << min_blocks(TB)
+      << ") mqb_pass(const JitBwdArgs<V> a) {\n"
       << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", C = " << p.c << ", NH = " << NH
       << ", NLS = " << NLS << ", TS = 1 << K;\n"
       << "  constexpr int NV = NR / (16 / int(sizeof(V)));\n"
@@ -361,7 +428,10 @@ std::string backward_source(const Schedule &s, const Pass &p, int precision, int
     for (int si = p.n_stages - 1; si >= 0; --si) {
         const StageDesc &sd = s.stages[p.stage_begin + si];
         emit_stage_load(o, sd, RB, TB, precision, NH);
-        for (int k = sd.op_end - 1; k >= sd.op_begin; --k) emit_backward_op(o, s.stage_ops[p.sop_begin + k], NH);
+        for (int k = sd.op_end - 1; k >= sd.op_begin; --k) {
+            const StageOp &so = s.stage_ops[p.sop_begin + k];
+            emit_backward_op(o, so, NH, ops[so.op].gate_id);
+        }
         emit_stage_store(o, sd, RB, precision, NH);
     }
     o << "   for (int h = 0; h < NH; ++h) tile::stage_out<V, NV>(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, C);\n"
@@ -457,8 +527,9 @@ std::vector<const void *> kernels_for(const std::vector<std::string> &srcs) {
 std::string jit_forward_source(const Schedule &s, const Pass &p, int precision) {
     return forward_source(s, p, precision);
 }
-std::string jit_backward_source(const Schedule &s, const Pass &p, int precision, int n_hams) {
-    return backward_source(s, p, precision, n_hams);
+std::string jit_backward_source(const Schedule &s, const Pass &p, int precision, int n_hams,
+                                const std::vector<DevOp> &ops) {
+    return backward_source(s, p, precision, n_hams, ops);
 }
 
 std::vector<const void *> jit_forward_kernels(const Schedule &s, int precision) {
@@ -468,19 +539,20 @@ std::vector<const void *> jit_forward_kernels(const Schedule &s, int precision) 
     return kernels_for(srcs);
 }
 
-std::vector<const void *> jit_backward_kernels(const Schedule &s, int precision, int n_hams) {
+std::vector<const void *> jit_backward_kernels(const Schedule &s, int precision, int n_hams,
+                                               const std::vector<DevOp> &ops) {
     std::vector<std::string> srcs(s.passes.size());
     for (size_t i = 0; i < s.passes.size(); ++i)
-        if (s.passes[i].fused) srcs[i] = backward_source(s, s.passes[i], precision, n_hams);
+        if (s.passes[i].fused) srcs[i] = backward_source(s, s.passes[i], precision, n_hams, ops);
     return kernels_for(srcs);
 }
 
-int jit_compile_check(const Schedule &s, int precision, int n_hams) {
+int jit_compile_check(const Schedule &s, int precision, int n_hams, const std::vector<DevOp> &ops) {
     std::vector<std::string> srcs;
     for (const Pass &p : s.passes) {
         if (!p.fused) continue;
         srcs.push_back(forward_source(s, p, precision));
-        if (n_hams > 0) srcs.push_back(backward_source(s, p, precision, n_hams));
+        if (n_hams > 0) srcs.push_back(backward_source(s, p, precision, n_hams, ops));
     }
     std::sort(srcs.begin(), srcs.end());
     srcs.erase(std::unique(srcs.begin(), srcs.end()), srcs.end());

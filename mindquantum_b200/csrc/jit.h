@@ -16,8 +16,9 @@ namespace mqb {
 // Per pass of `s`: the forward kernel (nullptr for unfused passes).  Compiles what the cache
 // lacks, in parallel; throws std::runtime_error with the compiler log on failure.
 std::vector<const void *> jit_forward_kernels(const Schedule &s, int precision);
-// Per pass of `s`: the backward kernel for n_hams lambdas.
-std::vector<const void *> jit_backward_kernels(const Schedule &s, int precision, int n_hams);
+// Per pass of `s`: the backward kernel for n_hams lambdas (`ops`: the program's lowered gates).
+std::vector<const void *> jit_backward_kernels(const Schedule &s, int precision, int n_hams,
+                                               const std::vector<DevOp> &ops);
 
 size_t jit_forward_smem(const Pass &p, int precision);
 size_t jit_backward_smem(const Pass &p, int precision, int n_hams);
@@ -28,11 +29,12 @@ cudaError_t jit_launch(const void *kernel, void *args, int threads, size_t smem,
 
 // Generate and compile (without loading: no GPU needed) the kernels of every fused pass, the
 // backward ones too when n_hams > 0; returns the number of distinct kernels.
-int jit_compile_check(const Schedule &s, int precision, int n_hams);
+int jit_compile_check(const Schedule &s, int precision, int n_hams, const std::vector<DevOp> &ops);
 
 // Sources of the kernels of one pass (for tests and inspection).
 std::string jit_forward_source(const Schedule &s, const Pass &p, int precision);
-std::string jit_backward_source(const Schedule &s, const Pass &p, int precision, int n_hams);
+std::string jit_backward_source(const Schedule &s, const Pass &p, int precision, int n_hams,
+                                const std::vector<DevOp> &ops);
 
 }  // namespace mqb
 

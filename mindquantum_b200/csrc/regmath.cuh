@@ -339,6 +339,148 @@ __device__ __forceinline__ void jb_diag2(V (&v)[1 << RB], V (&l)[NH][1 << RB], c
     }
 }
 
+// ---- gradients from the generator.  For U(t) = exp(-i t/2 G) with G a Pauli product (and for
+// the phase gates), dU/dt = -i/2 G U, so Re<lambda| dU |psi'> = Re<lambda| -i/2 G |psi> with psi
+// the state before the uncompute: the derivative costs two FMA per amplitude instead of a matrix
+// product and a dot product.  gs scales the accumulated sum (1/2, or 0 for threads whose
+// thread-level controls are off).
+
+template <typename R, typename V>
+__device__ __forceinline__ R re_acc(V l, V x, R acc) {  // acc + Re(conj(l) x)
+    return fma(l.x, x.x, fma(l.y, x.y, acc));
+}
+template <typename R, typename V>
+__device__ __forceinline__ R im_acc(V l, V x, R acc) {  // acc + Im(conj(l) x)
+    return fma(l.x, x.y, fma(-l.y, x.x, acc));
+}
+
+// RY-like: G = Y, Re<l| -i/2 Y |x> = (Re(conj(l1) x0) - Re(conj(l0) x1)) / 2; U^dag = U^T given
+template <typename V, int RB, int NH, int P, unsigned CM, typename R>
+__device__ __forceinline__ void jbg_ry(V (&v)[1 << RB], V (&l)[NH][1 << RB], R a00, R a01, R a10, R a11, R gs,
+                                       R (&acc)[3][NH]) {
+    R g[NH];
+#pragma unroll
+    for (int h = 0; h < NH; ++h) g[h] = 0;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (!pair_on<P, CM>(j)) continue;
+        constexpr int bit = 1 << P;
+        const V x0 = v[j], x1 = v[j | bit];
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+            g[h] = re_acc(l[h][j | bit], x0, g[h]);
+            g[h] = re_acc(l[h][j], cval<V>(-x1.x, -x1.y), g[h]);
+        }
+        v[j] = rlin(a00, x0, a01, x1);
+        v[j | bit] = rlin(a10, x0, a11, x1);
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+            const V z0 = l[h][j], z1 = l[h][j | bit];
+            l[h][j] = rlin(a00, z0, a01, z1);
+            l[h][j | bit] = rlin(a10, z0, a11, z1);
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < NH; ++h) acc[0][h] += gs * g[h];
+}
+
+// RX-like: G = X, Re<l| -i/2 X |x> = (Im(conj(l0) x1) + Im(conj(l1) x0)) / 2; U^dag = [[a, i nb], [i nb, a]]
+template <typename V, int RB, int NH, int P, unsigned CM, typename R>
+__device__ __forceinline__ void jbg_rx(V (&v)[1 << RB], V (&l)[NH][1 << RB], R a, R nb, R gs, R (&acc)[3][NH]) {
+    R g[NH];
+#pragma unroll
+    for (int h = 0; h < NH; ++h) g[h] = 0;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (!pair_on<P, CM>(j)) continue;
+        constexpr int bit = 1 << P;
+        const V x0 = v[j], x1 = v[j | bit];
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+            g[h] = im_acc(l[h][j], x1, g[h]);
+            g[h] = im_acc(l[h][j | bit], x0, g[h]);
+        }
+        v[j] = rxl(a, x0, nb, x1);
+        v[j | bit] = rxl(a, x1, nb, x0);
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+            const V z0 = l[h][j], z1 = l[h][j | bit];
+            l[h][j] = rxl(a, z0, nb, z1);
+            l[h][j | bit] = rxl(a, z1, nb, z0);
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < NH; ++h) acc[0][h] += gs * g[h];
+}
+
+// Diagonal phase gates (RZ, RZZ, PS, GP): dU/dt = -i W U with W diagonal and real, so the
+// gradient is sum_j w_j Im(conj(l_j) x_j).  One target on register P: weights (w0, w1) by bit P;
+// c0, c1 = conj of the entries for the uncompute.
+template <typename V, int RB, int NH, int P, unsigned CM, typename R>
+__device__ __forceinline__ void jbg_diag1(V (&v)[1 << RB], V (&l)[NH][1 << RB], V c0, V c1, R w0, R w1,
+                                          R (&acc)[3][NH]) {
+    R g0[NH], g1[NH];
+#pragma unroll
+    for (int h = 0; h < NH; ++h) g0[h] = g1[h] = 0;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (!ctl_on<CM>(j)) continue;
+        const bool hi = (j >> P) & 1;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+            if (hi) g1[h] = im_acc(l[h][j], v[j], g1[h]);
+            else g0[h] = im_acc(l[h][j], v[j], g0[h]);
+        }
+        v[j] = cmul(v[j], hi ? c1 : c0);
+#pragma unroll
+        for (int h = 0; h < NH; ++h) l[h][j] = cmul(l[h][j], hi ? c1 : c0);
+    }
+#pragma unroll
+    for (int h = 0; h < NH; ++h) acc[0][h] += w0 * g0[h] + w1 * g1[h];
+}
+
+// two targets on registers P (matrix bit 0) and Q (matrix bit 1): weights w[r], r = b0 | b1 << 1
+template <typename V, int RB, int NH, int P, int Q, unsigned CM, typename R>
+__device__ __forceinline__ void jbg_diag2(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V (&c)[4], const R (&w)[4],
+                                          R (&acc)[3][NH]) {
+    R g[4][NH];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int h = 0; h < NH; ++h) g[r][h] = 0;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (!ctl_on<CM>(j)) continue;
+        const int r = ((j >> P) & 1) | (((j >> Q) & 1) << 1);
+#pragma unroll
+        for (int h = 0; h < NH; ++h) g[r][h] = im_acc(l[h][j], v[j], g[r][h]);
+        v[j] = cmul(v[j], c[r]);
+#pragma unroll
+        for (int h = 0; h < NH; ++h) l[h][j] = cmul(l[h][j], c[r]);
+    }
+#pragma unroll
+    for (int h = 0; h < NH; ++h) acc[0][h] += w[0] * g[0][h] + w[1] * g[1][h] + w[2] * g[2][h] + w[3] * g[3][h];
+}
+
+// targets off the registers: one entry c and one weight w per thread
+template <typename V, int RB, int NH, unsigned CM, typename R>
+__device__ __forceinline__ void jbg_scale(V (&v)[1 << RB], V (&l)[NH][1 << RB], V c, R w, R (&acc)[3][NH]) {
+    R g[NH];
+#pragma unroll
+    for (int h = 0; h < NH; ++h) g[h] = 0;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (!ctl_on<CM>(j)) continue;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) g[h] = im_acc(l[h][j], v[j], g[h]);
+        v[j] = cmul(v[j], c);
+#pragma unroll
+        for (int h = 0; h < NH; ++h) l[h][j] = cmul(l[h][j], c);
+    }
+#pragma unroll
+    for (int h = 0; h < NH; ++h) acc[0][h] += w * g[h];
+}
+
 // dense 4x4 from the matrix table: M = U (row-major), dM_a = M + 16 (1 + a)
 template <typename V, int RB, int NH, int P, int Q, unsigned CM, int G>
 __device__ __forceinline__ void jb_dense2(V (&v)[1 << RB], V (&l)[NH][1 << RB], const V *M,
