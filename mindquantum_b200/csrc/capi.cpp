@@ -117,6 +117,7 @@ void set_last_error(const char *msg) { g_last_error = msg; }
 struct mqb_hamiltonian {
     int n = 0, precision = 0;
     std::vector<HamGroup> groups;
+    std::vector<HamClass> classes;
     HamClass *d_classes = nullptr;
     HamTerm *d_terms = nullptr;
     ~mqb_hamiltonian() {
@@ -351,6 +352,9 @@ static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R>
         a.g = g.geom;
         a.classes = h.d_classes + g.class_begin;
         a.n_classes = g.class_count;
+        a.term_begin = h.classes[g.class_begin].term_begin;
+        a.n_terms = h.classes[g.class_begin + g.class_count - 1].term_begin +
+                    h.classes[g.class_begin + g.class_count - 1].term_count - a.term_begin;
         a.terms = h.d_terms;
         a.ket = ket;
         a.bra = bra;
@@ -897,6 +901,7 @@ int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const ui
         std::vector<HamTerm> hterms;
         build_ham_groups(n_qubits, default_tile_bits(precision, 1), contiguity_bits(precision), mx, my, mz, ny, cf,
                          h->groups, classes, hterms);
+        h->classes = classes;
         h->d_classes = upload(classes);
         h->d_terms = upload(hterms);
         *out = h.release();

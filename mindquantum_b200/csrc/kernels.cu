@@ -445,9 +445,188 @@ __global__ void __launch_bounds__(kThreads) ham_kernel(const HamArgs<R> a) {
     }
 }
 
+// Register-binned Hamiltonian pass.  Every thread owns the NR = 2^NRB amplitudes L = tid + T r of
+// a tile (T = 2^(K - NRB) threads), so the sign (-1)^popc(L & m) of a Pauli term splits into a
+// per-thread part popc(tid & m) and a per-register part popc(r & m_hi).  A class's weight
+// W(L) = sum_t c_t (-1)^popc(L & m_t) is then, for the thread's amplitudes, the Walsh-Hadamard
+// transform over r of bins B[m_hi] = sum_t c_t (-1)^popc(tid & m_t): one signed add per term and
+// NRB * NR butterflies per thread instead of one popcount per term and amplitude.  The outside
+// qubits' signs are folded into the terms' coefficients once per tile.
+template <typename R, int NRB>
+__global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const HamArgs<R> a) {
+    using V = cplx<R>;
+    constexpr int NR = 1 << NRB;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const TileGeom &g = a.g;
+    const int K = g.K, c = g.c;
+    const int TS = 1 << K;
+    const int T = blockDim.x, tid = threadIdx.x;
+    const int nt = a.n_terms;
+    V *ket = reinterpret_cast<V *>(smem);
+    size_t o = align16(size_t(TS) * sizeof(V));
+    uint64_t *tab = reinterpret_cast<uint64_t *>(smem + o);
+    o = align16(o + (size_t(1) << (K - c)) * sizeof(uint64_t));
+    double *wf = reinterpret_cast<double *>(smem + o);
+    o = align16(o + size_t(T / 32) * 2 * sizeof(double));
+    HamClass *cls = reinterpret_cast<HamClass *>(smem + o);
+    o = align16(o + size_t(a.n_classes) * sizeof(HamClass));
+    V *tcoef = reinterpret_cast<V *>(smem + o);
+    o = align16(o + size_t(nt) * sizeof(V));
+    uint32_t *tmask = reinterpret_cast<uint32_t *>(smem + o);
+    const int nw = T / 32, warp = tid / 32, lane = tid % 32;
+    build_table(tab, g);
+    for (int i = tid; i < nw * 2; i += T) wf[i] = 0;
+    for (int i = tid; i < a.n_classes; i += T) cls[i] = a.classes[i];
+    for (int i = tid; i < nt; i += T) tmask[i] = a.terms[a.term_begin + i].lmask;
+    __syncthreads();
+    const int64_t n_tiles = int64_t(1) << g.n_out;
+    const int64_t dim = int64_t(1) << g.n;
+    const int64_t total = a.batch * n_tiles;
+    const uint32_t lowmask = (1u << c) - 1u;
+    const int hi_shift = K - NRB;
+    for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
+        const int64_t b = w >> g.n_out;
+        const uint64_t t = uint64_t(w) & uint64_t(n_tiles - 1);
+        const uint64_t base = tile_base(g, t);
+        load_tile(ket, a.ket + b * dim, base, tab, K, c);
+        for (int q = tid; q < nt; q += T) {
+            const HamTerm &ht = a.terms[a.term_begin + q];
+            const bool neg = __popcll(base & ht.omask) & 1;
+            V cq;
+            cq.x = R(neg ? -ht.cb_re : ht.cb_re);
+            cq.y = R(neg ? -ht.cb_im : ht.cb_im);
+            tcoef[q] = cq;
+        }
+        __syncthreads();
+        R ar[NR], ai[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) ar[r] = ai[r] = 0;
+        for (int k = 0; k < a.n_classes; ++k) {
+            const HamClass &hc = cls[k];
+            const int tb = hc.term_begin - a.term_begin;
+            R wr[NR], wi[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) wr[r] = wi[r] = 0;
+            if (hc.term_count <= 2) {
+                for (int q = tb; q < tb + hc.term_count; ++q) {
+                    const uint32_t m = tmask[q];
+                    const V cq = tcoef[q];
+                    const uint32_t pt = __popc(uint32_t(tid) & m);
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) {
+                        const bool neg = (pt + __popc((uint32_t(r) << hi_shift) & m)) & 1;
+                        wr[r] += neg ? -cq.x : cq.x;
+                        wi[r] += neg ? -cq.y : cq.y;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int bn = 0; bn < NR; ++bn) {
+                    for (int q = tb + hc.bins[bn]; q < tb + hc.bins[bn + 1]; ++q) {
+                        const V cq = tcoef[q];
+                        const bool neg = __popc(uint32_t(tid) & tmask[q]) & 1;
+                        wr[bn] += neg ? -cq.x : cq.x;
+                        wi[bn] += neg ? -cq.y : cq.y;
+                    }
+                }
+#pragma unroll
+                for (int sb = 0; sb < NRB; ++sb)
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) {
+                        if (r >> sb & 1) continue;
+                        const int r2 = r | (1 << sb);
+                        const R xr = wr[r], xi = wi[r];
+                        wr[r] = xr + wr[r2];
+                        wi[r] = xi + wi[r2];
+                        wr[r2] = xr - wr[r2];
+                        wi[r2] = xi - wi[r2];
+                    }
+            }
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const V kv = ket[uint32_t(tid + T * r) ^ hc.lflip];
+                ar[r] = fma(wr[r], kv.x, fma(-wi[r], kv.y, ar[r]));
+                ai[r] = fma(wr[r], kv.y, fma(wi[r], kv.x, ai[r]));
+            }
+        }
+        double fr = 0, fi = 0;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const uint32_t L = uint32_t(tid + T * r);
+            const uint64_t gL = base + tab[L >> c] + (L & lowmask);
+            if (a.fout) {
+                const V bv = a.bra[b * dim + gL];
+                fr += double(bv.x) * double(ar[r]) + double(bv.y) * double(ai[r]);
+                fi += double(bv.x) * double(ai[r]) - double(bv.y) * double(ar[r]);
+            }
+            if (a.out) {
+                V *op = a.out + b * a.out_batch_stride + gL;
+                V v;
+                v.x = ar[r];
+                v.y = ai[r];
+                if (a.accumulate) {
+                    const V old = *op;
+                    v.x += old.x;
+                    v.y += old.y;
+                }
+                *op = v;
+            }
+        }
+        if (a.fout) {
+            fr = warp_sum(fr);
+            fi = warp_sum(fi);
+            if (lane == 0) {
+                wf[warp * 2] += fr;
+                wf[warp * 2 + 1] += fi;
+            }
+        }
+        const int64_t nxt = w + gridDim.x;
+        const bool flush = (nxt >= total) || ((nxt >> g.n_out) != b);
+        __syncthreads();
+        if (flush && a.fout) {
+            if (tid < 2) {
+                double s2 = 0;
+                for (int ww = 0; ww < nw; ++ww) {
+                    s2 += wf[ww * 2 + tid];
+                    wf[ww * 2 + tid] = 0;
+                }
+                atomicAdd(&a.fout[b * a.f_stride + tid], s2);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+static size_t align_up16(size_t x) { return (x + 15) & ~size_t(15); }
+
+static size_t ham2_smem(const TileGeom &g, int elem_bytes, int threads, int n_classes, int n_terms) {
+    size_t s = align_up16((size_t(1) << g.K) * elem_bytes);
+    s = align_up16(s + (size_t(1) << (g.K - g.c)) * sizeof(uint64_t));
+    s = align_up16(s + size_t(threads / 32) * 2 * sizeof(double));
+    s = align_up16(s + size_t(n_classes) * sizeof(HamClass));
+    s = align_up16(s + size_t(n_terms) * elem_bytes);
+    return s + size_t(n_terms) * sizeof(uint32_t);
+}
+
 template <typename R>
 cudaError_t launch_ham(const HamArgs<R> &a, int sm_count, cudaStream_t s) {
     if (a.g.c < 1 || a.g.K > kMaxTileBits || a.g.K < 1) return cudaErrorInvalidValue;  // 16-byte tile accesses need a contiguous low qubit
+    if (a.g.K >= 5 + kHamRegBits && (a.g.K - kHamRegBits) <= (sizeof(R) == 4 ? 9 : 8)) {
+        const int threads = 1 << (a.g.K - kHamRegBits);
+        const size_t smem2 = ham2_smem(a.g, int(sizeof(cplx<R>)), threads, a.n_classes, a.n_terms);
+        if (smem2 <= 160 * 1024) {
+            auto kern = ham2_kernel<R, kHamRegBits>;
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem2));
+            if (e != cudaSuccess) return e;
+            int per_sm = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem2) != cudaSuccess || per_sm < 1)
+                per_sm = 1;
+            const int64_t work = a.batch << a.g.n_out;
+            const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(sm_count) * per_sm, work)));
+            kern<<<blocks, threads, smem2, s>>>(a);
+            return cudaGetLastError();
+        }
+    }
     const size_t smem = ham_smem(a.g, sizeof(cplx<R>));
     auto kern = ham_kernel<R>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));

@@ -80,6 +80,7 @@ struct HamArgs {
     const HamClass *classes;
     int n_classes;
     const HamTerm *terms;
+    int term_begin, n_terms;   // the group's terms: terms[term_begin .. term_begin + n_terms)
     const cplx<R> *ket;
     const cplx<R> *bra;        // used for the expectation accumulation
     cplx<R> *out;              // nullptr: expectation only

@@ -157,17 +157,22 @@ struct Schedule {
 };
 
 // Hamiltonian: terms grouped into passes; every group's flip masks fit in one tile.
+constexpr int kHamRegBits = 4;      // amplitudes per thread of the Hamiltonian kernel: 2^4
 struct HamTerm {
     double coeff;
     uint64_t my_mz;     // mask_y | mask_z (global), phase sign bits
     int32_t ny;
-    int32_t pad;
+    uint32_t lmask;     // my_mz on the group's tile-local bits
+    uint64_t omask;     // my_mz on the qubits outside the tile
+    double cb_re, cb_im;   // coeff * i^ny * (-1)^popc(flip & my_mz): the phase without the index bits
 };
 struct HamClass {       // terms sharing one flip mask
     uint64_t flip;      // global flip mask (mask_x | mask_y)
     uint32_t lflip;     // the same mask on the group's tile-local bits
     int32_t term_begin, term_count;
-    int32_t pad;
+    // terms sorted by the bits of lmask on the thread's register bits (the top kHamRegBits local
+    // bits): bins[b] .. bins[b + 1] is bin b, relative to term_begin
+    int32_t bins[(1 << kHamRegBits) + 1];
 };
 struct HamGroup {
     TileGeom geom;

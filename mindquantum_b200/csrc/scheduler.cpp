@@ -506,13 +506,33 @@ void build_ham_groups(int n, int K, int c, const std::vector<uint64_t> &mx, cons
                 if (hc.flip >> g.geom.qbits[i] & 1) hc.lflip |= 1u << i;
             hc.term_begin = int(terms.size());
             hc.term_count = int(cmem[ci].size());
+            const int K = g.geom.K;
+            const int shift = std::max(0, K - kHamRegBits);
+            std::vector<HamTerm> ts;
             for (int t : cmem[ci]) {
                 HamTerm ht{};
                 ht.coeff = coeff[t];
                 ht.my_mz = my[t] | mz[t];
                 ht.ny = ny[t];
-                terms.push_back(ht);
+                ht.lmask = 0;
+                for (int i = 0; i < K; ++i)
+                    if (ht.my_mz >> g.geom.qbits[i] & 1) ht.lmask |= 1u << i;
+                uint64_t tile_q = 0;
+                for (int i = 0; i < K; ++i) tile_q |= uint64_t(1) << g.geom.qbits[i];
+                ht.omask = ht.my_mz & ~tile_q;
+                // i^ny (ny counts the Y factors, each Y contributing i) and the flip's sign
+                const int ph = (ny[t] + 2 * popc(hc.flip & ht.my_mz)) & 3;
+                ht.cb_re = ph == 0 ? coeff[t] : ph == 2 ? -coeff[t] : 0.0;
+                ht.cb_im = ph == 1 ? coeff[t] : ph == 3 ? -coeff[t] : 0.0;
+                ts.push_back(ht);
             }
+            auto bin_of = [&](const HamTerm &ht) { return int((ht.lmask >> shift) & ((1u << kHamRegBits) - 1)); };
+            std::stable_sort(ts.begin(), ts.end(), [&](const HamTerm &x, const HamTerm &y) { return bin_of(x) < bin_of(y); });
+            for (int b = 0, q = 0; b <= (1 << kHamRegBits); ++b) {
+                while (q < int(ts.size()) && bin_of(ts[q]) < b) ++q;
+                hc.bins[b] = q;
+            }
+            terms.insert(terms.end(), ts.begin(), ts.end());
             classes.push_back(hc);
         }
         groups.push_back(g);

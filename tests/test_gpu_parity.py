@@ -218,6 +218,33 @@ def test_expectation_hamiltonian_and_vdot(dtype):
     assert abs(v - np.vdot(psi, lam_ref)) < tol
 
 
+@pytest.mark.parametrize("dtype", [complex128, complex64])
+@pytest.mark.parametrize("n", [10, 14, 17])
+def test_random_pauli_hamiltonians(dtype, n):
+    """Many terms per flip class, Y factors, masks across tile and outside qubits."""
+    rng = np.random.default_rng(40 + n)
+    op = QubitOperator('', 0.25)
+    for _ in range(120):
+        w = int(rng.integers(1, 7))
+        qs = rng.permutation(n)[:w]
+        op += QubitOperator(' '.join(f"{'XYZ'[int(p)]}{int(q)}" for p, q in zip(rng.integers(0, 3, w), qs)),
+                            float(rng.normal()))
+    for _ in range(60):   # diagonal terms: one large class
+        w = int(rng.integers(1, 5))
+        op += QubitOperator(' '.join(f'Z{int(q)}' for q in rng.permutation(n)[:w]), float(rng.normal()))
+    ham = Hamiltonian(op)
+    psi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi /= np.linalg.norm(psi)
+    sim = Simulator('mqvector_b200', n, dtype=dtype)
+    sim.set_qs(psi)
+    e = sim.get_expectation(ham)
+    lam_ref = O.apply_terms(psi, n, ham)
+    tol = 1e-10 if dtype == complex128 else 2e-5
+    assert abs(e - np.vdot(psi, lam_ref)) < tol
+    sim.apply_hamiltonian(ham)
+    assert np.allclose(sim.get_qs(), lam_ref, atol=1e-11 if dtype == complex128 else 2e-5, rtol=0)
+
+
 def test_sampling_matches_reference_algorithm():
     """Measure-ending circuits: same shots as the reference's sampler for the same seed."""
     n = 6
