@@ -358,6 +358,118 @@ def run_b200(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_workload(args, rank, local_rank):
+    """The other workload families on one GPU: the same JSON line, device-timed.
+
+    qnn: 20-qubit RX-encoder QNN, 512 samples, Z_0..Z_3 (grad evals/s = samples/s with all four
+    expectations and gradients); qaoa: MaxCut QAOA, 30 qubits, p = 10 on a 3-regular graph
+    (complex64, error against complex128); uneven: 64 circuits of 12..24 qubits (U3 layers and
+    brick CNOTs, own 10-term Hamiltonians) through one graph-captured CircuitBatch.
+    """
+    import torch
+
+    from mindquantum_b200 import _native as N
+    from mindquantum_b200 import complex64, complex128, workloads as W
+    from mindquantum_b200.simulator.mqvector_b200 import MQVectorB200
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device('cuda', local_rank)
+    extras = {}
+    if args.workload == 'qnn':
+        n, layers, B = 20, 6, 512
+        circ, hams, enc, ans = W.qnn(n, layers, B, seed=rank)
+        names = circ.params_name
+        params_np = np.concatenate([enc, np.broadcast_to(ans, (B, len(ans)))], axis=1)
+        params = torch.as_tensor(params_np, device=dev)
+        sim = MQVectorB200('mqvector_b200', n, dtype=complex64, device=dev)
+        units = B
+
+        def step():
+            return sim.expectation_with_grad_tensor(hams, circ, params, names)
+
+        def e2e_step():
+            return sim.get_expectation_with_grad(hams, circ)(enc, ans)
+
+        io = (params_np.nbytes, B * len(hams) * (1 + len(names)) * 16)
+        cfg = {"workload": f"QNN {n}q, RX encoder + {layers} x (RY, RZ, CZ ring), {len(names) - n} ansatz params, "
+                           f"Z_0..Z_3, {B} samples", "n_qubits": n, "batch": B}
+    elif args.workload == 'qaoa':
+        n, p = 30, 10
+        circ, ham, pr, edges = W.qaoa_maxcut(n, p, seed=rank)
+        names = circ.params_name
+        params = torch.as_tensor(pr[None, :], device=dev)
+        sim = MQVectorB200('mqvector_b200', n, dtype=complex64, device=dev)
+        units = 1
+
+        def step():
+            return sim.expectation_with_grad_tensor([ham], circ, params, names)
+
+        def e2e_step():
+            return sim.get_expectation_with_grad(ham, circ)(pr)
+
+        io = (pr.nbytes, (1 + len(names)) * 16)
+        cfg = {"workload": f"QAOA MaxCut {n}q, p={p}, 3-regular graph with {len(edges)} edges, H = sum Z_i Z_j",
+               "n_qubits": n, "batch": 1}
+    else:
+        from mindquantum_b200.simulator.batch import CircuitBatch
+
+        members = W.uneven_u3(64, 12, 24, 20, seed=rank)
+        batch = CircuitBatch([(m, c, h) for m, c, h, _ in members], dtype=complex64)
+        plist = [torch.as_tensor(x, device=dev) for _, _, _, x in members]
+        units = len(members)
+
+        def step():
+            return batch(plist)
+
+        def e2e_step():
+            fs, gs = batch([x for _, _, _, x in members])
+            return [f.cpu() for f in fs], [g.cpu() for g in gs]
+
+        io = (sum(x.nbytes for _, _, _, x in members), sum(16 * (1 + len(c.params_name)) for _, c, _, _ in members))
+        cfg = {"workload": "64 circuits of 12..24 qubits, 20 x (U3 on every qubit + brick CNOTs), own 10-term "
+                           "random Pauli Hamiltonians, one CUDA graph per call, autotuned tile widths",
+               "n_circuits": len(members), "qubits": [m for m, _, _, _ in members], "graph_launches_per_call": 1,
+               "kernel_launches_per_call": batch.launches_per_call()}
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    value = units * args.steps / (ms / 1e3)
+    with N.KernelTimer() as kt:
+        for _ in range(args.steps):
+            step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if args.workload == 'qaoa' and not args.skip_extras:
+        f64, g64 = step()
+        s128 = MQVectorB200('mqvector_b200', 30, dtype=complex128, device=dev)
+        f128, g128 = s128.expectation_with_grad_tensor([ham], circ, params, names)
+        extras["grad_err_vs_c128"] = float((g64 - g128).abs().max().item())
+        extras["f_err_vs_c128"] = float((f64[..., 0] - f128[..., 0]).abs().max().item())
+        del s128
+    line = {
+        "metric": f"grad evals/s, {args.workload} workload", "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic", "config": cfg,
+        "e2e": {"value": units * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(io[0]),
+                "d2h_bytes_per_step": int(io[1])},
+        "kernel_ms_per_step": {k: v / args.steps for k, v in kt.ms.items() if v},
+        "clocks": clocks.summary(), "gpu_launches": sum(kt.launches.values()), **extras,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -370,12 +482,18 @@ def main():
     ap.add_argument('--skip-extras', action='store_true')
     ap.add_argument('--skip-plain', action='store_true')
     ap.add_argument('--skip-cpu', action='store_true')
+    ap.add_argument('--workload', default='hea', choices=['hea', 'qnn', 'qaoa', 'uneven'],
+                    help='hea: the headline 26-qubit HEA gradient; the others are the remaining workload families')
     args = ap.parse_args()
     rank = int(os.environ.get('RANK', 0))
     world = int(os.environ.get('WORLD_SIZE', 1))
     local_rank = int(os.environ.get('LOCAL_RANK', 0))
     if args.impl == 'reference':
         run_reference(args, rank)
+        return
+    if args.workload != 'hea':
+        if rank == 0:
+            run_workload(args, rank, local_rank)
         return
     run_b200(args, rank, world, local_rank)
 

@@ -321,6 +321,237 @@ void emit_backward_op(std::ostringstream &o, const StageOp &so, int NH, int gid)
     o << "    }\n";
 }
 
+// ------------------------------------------------------------------ runs of diagonal gates
+// Consecutive diagonal gates of a stage commute; their product is applied as one per-amplitude
+// factor.  Factors of targets off the registers are one scalar per thread, single-target factors
+// on register P are a pair (d0, d1) per thread, so a per-thread table over the register bits
+// carrying such factors costs about two complex products per amplitude for the whole run,
+// after which the run is one complex product per amplitude.  Two-target and register-controlled
+// factors are multiplied in per amplitude.  In the adjoint, Im(conj(lambda) psi) is the same at
+// every point of the run (a common unit-modulus diagonal cancels), so all gradients of the run
+// come from sums of it over the thread's amplitudes, split by the bits their weights depend on.
+
+bool diag_op(const StageOp &so) { return so.kind == SK_DIAG1 || so.kind == SK_DIAG2; }
+
+// Gates a run may hold in the adjoint: no gradient, or a generator-form gradient.
+bool run_ok_backward(const StageOp &so, int gid) {
+    if (!diag_op(so)) return false;
+    const int G = so.n_angles ? so.grad_mask : 0;
+    return G == 0 || (G == 1 && !phase_weights(gid).empty());
+}
+
+struct RunPlan {
+    std::vector<int> bits;   // register positions carrying per-thread factor pairs
+};
+
+enum DiagShape { DS_OFF, DS_REG1, DS_REGOFF, DS_OTHER };
+DiagShape diag_shape(const StageOp &so) {
+    const bool two = so.kind == SK_DIAG2;
+    const bool in0 = so.dsrc[0] == 0, in1 = two && so.dsrc[1] == 0;
+    if (so.rctrl) return DS_OTHER;
+    if (!in0 && !in1) return DS_OFF;
+    if (!two) return DS_REG1;
+    if (in0 != in1) return DS_REGOFF;
+    return DS_OTHER;
+}
+int diag_reg_bit(const StageOp &so) { return so.dsrc[0] == 0 ? so.dval[0] : so.dval[1]; }
+
+// Per-thread factors of a run: sc (scalar) and f0_P / f1_P (pairs); `conj` for U^dag.
+RunPlan emit_run_factors(std::ostringstream &o, const std::vector<const StageOp *> &run, bool conj) {
+    RunPlan plan;
+    const std::string one = "cval<V>(1, 0)";
+    auto ent = [&](int M, const std::string &idx) {
+        const std::string e = "mt[" + std::to_string(M) + " + " + idx + "]";
+        return conj ? "cconj(" + e + ")" : e;
+    };
+    o << "      V sc = cval<V>(1, 0);\n";
+    for (int P = 0; P < kMaxRegBits; ++P) {
+        bool used = false;
+        for (const StageOp *so : run)
+            if ((diag_shape(*so) == DS_REG1 || diag_shape(*so) == DS_REGOFF) && diag_reg_bit(*so) == P) used = true;
+        if (used) {
+            plan.bits.push_back(P);
+            o << "      V f0_" << P << " = cval<V>(1, 0), f1_" << P << " = cval<V>(1, 0);\n";
+        }
+    }
+    for (const StageOp *sp : run) {
+        const StageOp &so = *sp;
+        const std::string on = on_expr(so);
+        auto sel = [&](const std::string &v) { return on.empty() ? v : "((" + on + ") ? " + v + " : " + one + ")"; };
+        const DiagShape sh = diag_shape(so);
+        const int M = so.moff;
+        if (sh == DS_OFF) {
+            const bool two = so.kind == SK_DIAG2;
+            o << "      { const int r = " << off_bit_expr(so.dsrc[0], so.dval[0]) << " | ("
+              << off_bit_expr(two ? so.dsrc[1] : 3, so.dval[1]) << " << 1); sc = cmul(sc, " << sel(ent(M, "r")) << "); }\n";
+        } else if (sh == DS_REG1) {
+            const int P = so.dval[0];
+            o << "      f0_" << P << " = cmul(f0_" << P << ", " << sel(ent(M, "0")) << "); f1_" << P << " = cmul(f1_" << P
+              << ", " << sel(ent(M, "1")) << ");\n";
+        } else if (sh == DS_REGOFF) {
+            const int k = so.dsrc[0] == 0 ? 0 : 1;
+            const int P = so.dval[k];
+            o << "      { const int b = " << off_bit_expr(so.dsrc[1 - k], so.dval[1 - k]) << ";\n";
+            if (k == 0) o << "        const int i0 = b << 1, i1 = 1 | (b << 1);\n";
+            else o << "        const int i0 = b, i1 = 2 | b;\n";
+            o << "        f0_" << P << " = cmul(f0_" << P << ", " << sel(ent(M, "i0")) << "); f1_" << P << " = cmul(f1_" << P
+              << ", " << sel(ent(M, "i1")) << "); }\n";
+        }
+    }
+    // table over the factor bits
+    const int nb = int(plan.bits.size());
+    o << "      V T[" << (1 << nb) << "];\n      T[0] = sc;\n";
+    for (int k = 0; k < nb; ++k) {
+        const int P = plan.bits[k];
+        for (int idx = 0; idx < (1 << k); ++idx) {
+            o << "      T[" << (idx | (1 << k)) << "] = cmul(T[" << idx << "], f1_" << P << "); T[" << idx << "] = cmul(T["
+              << idx << "], f0_" << P << ");\n";
+        }
+    }
+    return plan;
+}
+
+// The factor of amplitude j: table entry times the per-amplitude factors of the run's other gates.
+std::string run_factor_expr(std::ostringstream &o, const RunPlan &plan, const std::vector<const StageOp *> &run, int j,
+                            bool conj) {
+    int idx = 0;
+    for (size_t k = 0; k < plan.bits.size(); ++k)
+        if (j >> plan.bits[k] & 1) idx |= 1 << k;
+    std::string d = "T[" + std::to_string(idx) + "]";
+    const std::string one = "cval<V>(1, 0)";
+    for (const StageOp *sp : run) {
+        const StageOp &so = *sp;
+        const DiagShape sh = diag_shape(so);
+        if (sh != DS_OTHER) continue;
+        if ((uint32_t(j) & so.rctrl) != so.rctrl) continue;   // register controls not satisfied: identity
+        const std::string on = on_expr(so);
+        // entry index from the targets' bits (register bits are literals here)
+        std::string r;
+        auto bit = [&](int k) -> std::string {
+            if (so.dsrc[k] == 0) return std::to_string((j >> so.dval[k]) & 1);
+            return "(" + off_bit_expr(so.dsrc[k], so.dval[k]) + ")";
+        };
+        if (so.kind == SK_DIAG1) r = bit(0);
+        else r = bit(0) + " | (" + bit(1) + " << 1)";
+        std::string e = "mt[" + std::to_string(so.moff) + " + (" + r + ")]";
+        if (conj) e = "cconj(" + e + ")";
+        if (!on.empty()) e = "((" + on + ") ? " + e + " : " + one + ")";
+        d = "cmul(" + d + ", " + e + ")";
+    }
+    (void)o;
+    return d;
+}
+
+void emit_forward_run(std::ostringstream &o, const std::vector<const StageOp *> &run, int RB) {
+    o << "    {   // run of " << run.size() << " diagonal gates\n";
+    const RunPlan plan = emit_run_factors(o, run, false);
+    for (int j = 0; j < (1 << RB); ++j)
+        o << "      v[" << j << "] = cmul(v[" << j << "], " << run_factor_expr(o, plan, run, j, false) << ");\n";
+    o << "    }\n";
+}
+
+void emit_backward_run(std::ostringstream &o, const std::vector<const StageOp *> &run, const std::vector<int> &gids,
+                       int RB, int NH) {
+    o << "    {   // run of " << run.size() << " diagonal gates\n";
+    // gradient sums of p_j = Im(conj(lambda_j) psi_j): all, per register bit, per special gate
+    bool any_grad = false;
+    std::vector<int> need_bits;
+    for (size_t k = 0; k < run.size(); ++k) {
+        const StageOp &so = *run[k];
+        const int G = so.n_angles ? so.grad_mask : 0;
+        if (!G) continue;
+        any_grad = true;
+        const DiagShape sh = diag_shape(so);
+        if (sh == DS_REG1 || sh == DS_REGOFF) {
+            const int P = diag_reg_bit(so);
+            if (std::find(need_bits.begin(), need_bits.end(), P) == need_bits.end()) need_bits.push_back(P);
+        }
+    }
+    if (any_grad) {
+        o << "      R S[NH] = {};\n";
+        for (int P : need_bits) o << "      R SB" << P << "[NH] = {};\n";
+        for (size_t k = 0; k < run.size(); ++k) {
+            const StageOp &so = *run[k];
+            if ((so.n_angles ? so.grad_mask : 0) && diag_shape(so) == DS_OTHER)
+                o << "      R SX" << k << "[4][NH] = {};\n";
+        }
+        for (int j = 0; j < (1 << RB); ++j) {
+            o << "      for (int h = 0; h < NH; ++h) {\n        const R pj = fma(l[h][" << j << "].x, v[" << j << "].y, -l[h]["
+              << j << "].y * v[" << j << "].x);\n        S[h] += pj;";
+            for (int P : need_bits)
+                if (j >> P & 1) o << " SB" << P << "[h] += pj;";
+            for (size_t k = 0; k < run.size(); ++k) {
+                const StageOp &so = *run[k];
+                if (!((so.n_angles ? so.grad_mask : 0) && diag_shape(so) == DS_OTHER)) continue;
+                if ((uint32_t(j) & so.rctrl) != so.rctrl) continue;
+                // class of j by the gate's register targets (off-register target bits enter the weight)
+                int cls = 0;
+                if (so.dsrc[0] == 0) cls |= (j >> so.dval[0]) & 1;
+                if (so.kind == SK_DIAG2 && so.dsrc[1] == 0) cls |= ((j >> so.dval[1]) & 1) << 1;
+                o << " SX" << k << "[" << cls << "][h] += pj;";
+            }
+            o << "\n      }\n";
+        }
+        for (size_t k = 0; k < run.size(); ++k) {
+            const StageOp &so = *run[k];
+            const int G = so.n_angles ? so.grad_mask : 0;
+            if (!G) continue;
+            const std::vector<double> pw = phase_weights(gids[k]);
+            const std::string on = on_expr(so);
+            auto onw = [&](const std::string &w) { return on.empty() ? w : "((" + on + ") ? " + w + " : R(0))"; };
+            auto wsel4 = [&](const std::string &r) {
+                return pw.size() > 2 ? "(" + r + " == 0 ? " + lit(pw[0]) + " : " + r + " == 1 ? " + lit(pw[1]) + " : " + r +
+                                           " == 2 ? " + lit(pw[2]) + " : " + lit(pw[3]) + ")"
+                                     : "(" + r + " ? " + lit(pw[1]) + " : " + lit(pw[0]) + ")";
+            };
+            o << "      {\n        R acc[3][NH];\n";
+            const DiagShape sh = diag_shape(so);
+            if (sh == DS_OFF) {
+                const bool two = so.kind == SK_DIAG2;
+                o << "        const int r = " << off_bit_expr(so.dsrc[0], so.dval[0]) << " | ("
+                  << off_bit_expr(two ? so.dsrc[1] : 3, so.dval[1]) << " << 1);\n";
+                o << "        for (int h = 0; h < NH; ++h) acc[0][h] = " << onw(wsel4("r")) << " * S[h];\n";
+            } else if (sh == DS_REG1) {
+                const int P = so.dval[0];
+                o << "        for (int h = 0; h < NH; ++h) acc[0][h] = " << onw(lit(pw[0])) << " * (S[h] - SB" << P << "[h]) + "
+                  << onw(lit(pw[1])) << " * SB" << P << "[h];\n";
+            } else if (sh == DS_REGOFF) {
+                const int kk = so.dsrc[0] == 0 ? 0 : 1;
+                const int P = so.dval[kk];
+                o << "        const int b = " << off_bit_expr(so.dsrc[1 - kk], so.dval[1 - kk]) << ";\n";
+                const std::string w_lo = kk == 0 ? "(b ? " + lit(pw[2]) + " : " + lit(pw[0]) + ")" : "(b ? " + lit(pw[1]) + " : " + lit(pw[0]) + ")";
+                const std::string w_hi = kk == 0 ? "(b ? " + lit(pw[3]) + " : " + lit(pw[1]) + ")" : "(b ? " + lit(pw[3]) + " : " + lit(pw[2]) + ")";
+                o << "        for (int h = 0; h < NH; ++h) acc[0][h] = " << onw(w_lo) << " * (S[h] - SB" << P << "[h]) + "
+                  << onw(w_hi) << " * SB" << P << "[h];\n";
+            } else {
+                // class c of SX: register target bits; off-register target bits pick the weight per thread
+                o << "        for (int h = 0; h < NH; ++h) acc[0][h] = R(0);\n";
+                for (int cls = 0; cls < 4; ++cls) {
+                    std::string r0 = so.dsrc[0] == 0 ? std::to_string(cls & 1) : "(" + off_bit_expr(so.dsrc[0], so.dval[0]) + ")";
+                    std::string r1 = "0";
+                    if (so.kind == SK_DIAG2)
+                        r1 = so.dsrc[1] == 0 ? std::to_string((cls >> 1) & 1) : "(" + off_bit_expr(so.dsrc[1], so.dval[1]) + ")";
+                    if (so.dsrc[0] != 0 && (cls & 1)) continue;
+                    if ((so.kind != SK_DIAG2 || so.dsrc[1] != 0) && (cls & 2)) continue;
+                    o << "        { const int r = " << r0 << " | (" << r1 << " << 1);\n"
+                      << "          for (int h = 0; h < NH; ++h) acc[0][h] += " << onw(wsel4("r")) << " * SX" << k << "[" << cls
+                      << "][h]; }\n";
+                }
+            }
+            if (so.lslot >= 0)
+                o << "        for (int h = 0; h < NH; ++h) {\n          const double x = warp_sum(double(acc[0][h]));\n"
+                  << "          if (lane == 0) wacc[(warp * NLS + " << so.lslot << ") * NH + h] += x;\n        }\n";
+            o << "      }\n";
+        }
+    }
+    const RunPlan plan = emit_run_factors(o, run, true);
+    for (int j = 0; j < (1 << RB); ++j) {
+        o << "      { const V d = " << run_factor_expr(o, plan, run, j, true) << "; v[" << j << "] = cmul(v[" << j
+          << "], d); for (int h = 0; h < NH; ++h) l[h][" << j << "] = cmul(l[h][" << j << "], d); }\n";
+    }
+    o << "    }\n";
+}
+
 // Blocks per SM the register budget is sized for: 512 threads per SM at 128 registers each.
 int min_blocks(int TB) { return std::max(1, 512 >> TB); }
 
@@ -386,7 +617,18 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
     for (int si = 0; si < p.f_n_stages; ++si) {
         const StageDesc &sd = s.f_stages[p.f_stage_begin + si];
         emit_stage_load(o, sd, RB, TB, precision, 0);
-        for (int k = sd.op_begin; k < sd.op_end; ++k) emit_forward_op(o, s.f_stage_ops[p.f_sop_begin + k]);
+        for (int k = sd.op_begin; k < sd.op_end;) {
+            std::vector<const StageOp *> run;
+            int e = k;
+            while (e < sd.op_end && diag_op(s.f_stage_ops[p.f_sop_begin + e])) run.push_back(&s.f_stage_ops[p.f_sop_begin + e++]);
+            if (run.size() >= 2) {
+                emit_forward_run(o, run, RB);
+                k = e;
+            } else {
+                emit_forward_op(o, s.f_stage_ops[p.f_sop_begin + k]);
+                ++k;
+            }
+        }
         emit_stage_store(o, sd, RB, precision, 0);
     }
     o << "   tile::stage_out<V, NV>(tl, a.dst + b * dim, base, tab, C);\n   __syncthreads();\n  }\n}\n";
@@ -428,9 +670,25 @@ std::string backward_source(const Schedule &s, const Pass &p, int precision, int
     for (int si = p.n_stages - 1; si >= 0; --si) {
         const StageDesc &sd = s.stages[p.stage_begin + si];
         emit_stage_load(o, sd, RB, TB, precision, NH);
-        for (int k = sd.op_end - 1; k >= sd.op_begin; --k) {
-            const StageOp &so = s.stage_ops[p.sop_begin + k];
-            emit_backward_op(o, so, NH, ops[so.op].gate_id);
+        for (int k = sd.op_end - 1; k >= sd.op_begin;) {
+            std::vector<const StageOp *> run;
+            std::vector<int> gids;
+            int e = k;
+            while (e >= sd.op_begin) {
+                const StageOp &so = s.stage_ops[p.sop_begin + e];
+                if (!run_ok_backward(so, ops[so.op].gate_id)) break;
+                run.push_back(&so);
+                gids.push_back(ops[so.op].gate_id);
+                --e;
+            }
+            if (run.size() >= 2) {
+                emit_backward_run(o, run, gids, RB, NH);
+                k = e;
+            } else {
+                const StageOp &so = s.stage_ops[p.sop_begin + k];
+                emit_backward_op(o, so, NH, ops[so.op].gate_id);
+                --k;
+            }
         }
         emit_stage_store(o, sd, RB, precision, NH);
     }

@@ -115,9 +115,13 @@ class CircuitBatch:
                 self._tune(m)
 
     def _tune(self, m):
-        """Time the member's gradient at candidate tile widths; keep the fastest (ties: default)."""
+        """Time the member's gradient at candidate tile widths; keep the fastest (ties: default).
+
+        Members of 18 qubits and more run generated pass kernels, whose compile time per candidate
+        would dominate; they keep the default width.
+        """
         k0 = m.prog.info.tile_bits
-        cands = sorted({0, *[k for k in (k0 - 2, k0 - 1, k0 + 1) if 6 <= k <= 13 and k <= m.n]})
+        cands = [0] if m.n >= 18 else sorted({0, *[k for k in (k0 - 2, k0 - 1, k0 + 1) if 6 <= k <= 13 and k <= m.n]})
         best = None
         stream = self.streams[0]
         for k in cands:

@@ -16,7 +16,8 @@ from test_host import _random_circuit
 
 
 @pytest.mark.parametrize("n,prec,tile,n_hams", [(10, N.MQB_PREC_C64, 0, 0), (11, N.MQB_PREC_C128, 8, 1),
-                                               (12, N.MQB_PREC_C64, 9, 2), (10, N.MQB_PREC_C64, 0, 4)])
+                                               (12, N.MQB_PREC_C64, 9, 2), (10, N.MQB_PREC_C64, 0, 4),
+                                               (12, N.MQB_PREC_C64, 0, 1), (11, N.MQB_PREC_C64, 9, 1)])
 def test_generated_kernels_compile(n, prec, tile, n_hams):
     rng = np.random.default_rng(n + 10 * n_hams)
     c = _random_circuit(rng, n, 60)
