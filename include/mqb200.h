@@ -198,6 +198,19 @@ MQB_API int mqb_expectation_with_grad(mqb_program *prog, const mqb_hamiltonian *
                               int64_t param_stride, const double *custom, double *f, double *grad,
                               int ckpt_stride, void *workspace, size_t workspace_bytes, void *stream);
 
+/* Adjoint sweep with a caller-given lambda: grad[b][k] = sum over the gates of
+ * Re <lambda_g| dU_g/d param_k |psi_{g-1}>, where psi runs forward from init through the program and
+ * lambda starts from `lam` at the end of the circuit ([batch][2^n] when lam_batched, else one state)
+ * and is uncomputed with psi.  No factor 2 and no Hamiltonian: the building block of the
+ * non-Hermitian gradient <phi| U_l^dag H U_r |psi> (imaginary parts from lambda -> i lambda).
+ * Replaces the sweeps of GradientHelper::RightSizeGrad / LeftSizeGrad
+ * (ccsrc/include/simulator/vector/gradient.h:160-236).  Workspace: mqb_grad_workspace_size with
+ * n_hams = 1. */
+MQB_API int mqb_adjoint_with_lambda(mqb_program *prog, const void *lam, int lam_batched, const void *init,
+                                    int init_batched, int64_t batch, const double *params, int64_t param_stride,
+                                    const double *custom, double *grad, int ckpt_stride, void *ws,
+                                    size_t ws_bytes, void *stream);
+
 /* ------------------------------------------------------------------ sampling / measurement */
 /* Sorted uniforms u[s] (device float64, ascending) -> amplitude indices out[s] (device int64):
  * out[s] = smallest i with cdf(i) > u[s], cdf(i) = sum_{j<=i} |psi_j|^2 and cdf(dim-1) = 1.

@@ -78,6 +78,7 @@ SIGNATURES = {
     'mqb_program_destroy': [_P],
     'mqb_plan_schedule': [_I, _I, _P, _I, _P, _I64, _I, _I, _P, _P, _P, _P, _P, _P],
     'mqb_jit_check': [_I, _I, _P, _I, _P, _I64, _I, _I, _P],
+    'mqb_adjoint_with_lambda': [_P, _P, _I, _P, _I, _I64, _P, _I64, _P, _P, _I, _P, _SZ, _P],
     'mqb_program_get_info': [_P, _P],
     'mqb_program_grad_passes': [_P, _I, _P, _P],
     'mqb_apply_workspace_size': [_P, _I64, _P],

@@ -8,6 +8,7 @@ which compiles the generated pass kernels at run time.
 """
 import os
 import subprocess
+import time
 import sys
 from concurrent.futures import ThreadPoolExecutor
 
@@ -50,6 +51,9 @@ def build(force=False, verbose=False):
     """Compile the library unless it is newer than every source."""
     if not force and up_to_date():
         return LIB
+    # outputs are stamped with the build's start time, so a source edited while the build runs
+    # leaves them stale for the next build
+    t_start = time.time()
     bdir = os.path.join(os.path.dirname(HERE), '_build', 'mqb200')
     os.makedirs(bdir, exist_ok=True)
     env = dict(os.environ)
@@ -99,6 +103,9 @@ def build(force=False, verbose=False):
         res = subprocess.run(cmd, capture_output=True, text=True, env=env)
         if res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
+        else:
+            out = cmd[cmd.index('-o') + 1]
+            os.utime(out, (t_start, t_start))
         return res.returncode
 
     todo = [c for c in compiles if stale(c)]
@@ -108,6 +115,7 @@ def build(force=False, verbose=False):
     if any(codes) or run(link) != 0:
         raise RuntimeError('building libmqb200.so failed')
     os.replace(LIB + '.tmp', LIB)
+    os.utime(LIB, (t_start, t_start))
     return LIB
 
 

@@ -398,10 +398,14 @@ static GradLayout grad_layout(const mqb_program &p, const Schedule &s, int64_t b
     return L;
 }
 
+// Adjoint gradient.  With Hamiltonians: lambda_h = H_h psi, f_h = <psi|H_h|psi> and
+// grad = 2 Re sum <lambda|dU|psi> (GradRealDouble).  With lam_in instead (n_hams = 1, hams and f
+// unused): lambda starts from the caller's state and grad = Re sum <lambda|dU|psi> (scale 1).
 template <typename R>
 static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_hams, const void *init,
                       int init_batched, int64_t batch, const double *params, int64_t param_stride, const double *custom,
-                      double *f, double *grad, int stride, void *ws, size_t ws_bytes, cudaStream_t st) {
+                      double *f, double *grad, int stride, void *ws, size_t ws_bytes, cudaStream_t st,
+                      const void *lam_in = nullptr, int lam_batched = 0) {
     using V = cplx<R>;
     SchedDev &sd = grad_schedule(p, n_hams);
     const Schedule &s = sd.s;
@@ -422,7 +426,7 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
     const V *cpool = static_cast<const V *>(p.d_cpool);
 
     ck(cudaMemsetAsync(gslots, 0, L.gslots, st), "memset");
-    ck(cudaMemsetAsync(f, 0, sizeof(double) * 2 * n_hams * batch, st), "memset");
+    if (f) ck(cudaMemsetAsync(f, 0, sizeof(double) * 2 * n_hams * batch, st), "memset");
     run_matgen<R>(p, params, param_stride, custom, batch, mats, st);
 
     // forward: psi_{q+1} = pass_q(psi_q), psi_0 = init (or |0...0>)
@@ -441,9 +445,15 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
     } else {
         ck(launch_copy_or_zero<R>(W, init_v, p.n, batch, init_stride, st), "state copy");
     }
-    // lambda_h = H_h psi_P ; f_h = <psi_P|lambda_h>
-    for (int h = 0; h < n_hams; ++h)
-        ham_impl<R>(*hams[h], psiP, psiP, lam + h * batch * dim, f + 2 * h, 2 * n_hams, batch, st);
+    // lambda_h = H_h psi_P ; f_h = <psi_P|lambda_h>   (or lambda from the caller)
+    if (lam_in) {
+        TimeScope ts(TK_OTHER, st);
+        ck(launch_copy_or_zero<R>(lam, static_cast<const V *>(lam_in), p.n, batch, lam_batched ? dim : 0, st),
+           "lambda copy");
+    } else {
+        for (int h = 0; h < n_hams; ++h)
+            ham_impl<R>(*hams[h], psiP, psiP, lam + h * batch * dim, f + 2 * h, 2 * n_hams, batch, st);
+    }
     // backward
     for (int q = P - 1; q >= 0; --q) {
         const Pass &ps = s.passes[q];
@@ -523,7 +533,7 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
     }
     TimeScope ts(TK_SCATTER, st);
     ck(launch_grad_scatter(gslots, batch, std::max(1, p.n_slots), n_hams, p.d_csr_ptr, p.d_csr_slot, p.d_csr_coeff,
-                           p.n_params, grad, st),
+                           p.n_params, lam_in ? 1.0 : 2.0, grad, st),
        "gradient scatter");
 }
 
@@ -981,6 +991,24 @@ int mqb_expectation_with_grad(mqb_program *p, const mqb_hamiltonian *const *hams
         else
             grad_impl<double>(*p, hams, n_hams, init, init_batched, batch, params, param_stride, custom, f, grad, stride, ws,
                               ws_bytes, st);
+    });
+}
+
+int mqb_adjoint_with_lambda(mqb_program *p, const void *lam, int lam_batched, const void *init, int init_batched,
+                            int64_t batch, const double *params, int64_t param_stride, const double *custom,
+                            double *grad, int stride, void *ws, size_t ws_bytes, void *stream) {
+    return guarded([&] {
+        if (!p || !lam || !grad) fail(MQB_ERR_INVALID, "null argument");
+        if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
+        if (p->custom_entries && !custom) fail(MQB_ERR_INVALID, "custom gate matrices required");
+        if (batch > 65535 / 12) fail(MQB_ERR_INVALID, "batch too large for one call");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (p->precision == MQB_PREC_C64)
+            grad_impl<float>(*p, nullptr, 1, init, init_batched, batch, params, param_stride, custom, nullptr, grad,
+                             stride, ws, ws_bytes, st, lam, lam_batched);
+        else
+            grad_impl<double>(*p, nullptr, 1, init, init_batched, batch, params, param_stride, custom, nullptr, grad,
+                              stride, ws, ws_bytes, st, lam, lam_batched);
     });
 }
 

@@ -938,7 +938,7 @@ cudaError_t launch_copy_or_zero(cplx<R> *dst, const cplx<R> *src, int n, int64_t
 
 __global__ void grad_scatter_kernel(const double *gslots, int64_t batch, int n_slots, int n_hams,
                                     const int32_t *csr_ptr, const int32_t *csr_slot, const double *csr_coeff,
-                                    int n_params, double *grad) {
+                                    int n_params, double scale, double *grad) {
     const int64_t total = batch * n_hams * int64_t(n_params);
     for (int64_t w = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; w < total; w += int64_t(gridDim.x) * blockDim.x) {
         const int p = int(w % n_params);
@@ -947,18 +947,18 @@ __global__ void grad_scatter_kernel(const double *gslots, int64_t batch, int n_s
         double s = 0;
         for (int e = csr_ptr[p]; e < csr_ptr[p + 1]; ++e)
             s += csr_coeff[e] * gslots[(b * n_slots + csr_slot[e]) * n_hams + h];
-        grad[w] = 2.0 * s;   // GradRealDouble: g + conj(g) = 2 Re g
+        grad[w] = scale * s;   // scale 2: GradRealDouble, g + conj(g) = 2 Re g
     }
 }
 
 cudaError_t launch_grad_scatter(const double *gslots, int64_t batch, int n_slots, int n_hams, const int32_t *csr_ptr,
-                                const int32_t *csr_slot, const double *csr_coeff, int n_params, double *grad,
+                                const int32_t *csr_slot, const double *csr_coeff, int n_params, double scale, double *grad,
                                 cudaStream_t s) {
     const int64_t total = batch * n_hams * int64_t(n_params);
     if (total == 0) return cudaSuccess;
     const int blocks = int(std::min<int64_t>((total + 255) / 256, 4096));
     grad_scatter_kernel<<<blocks, 256, 0, s>>>(gslots, batch, n_slots, n_hams, csr_ptr, csr_slot, csr_coeff, n_params,
-                                                grad);
+                                                scale, grad);
     return cudaGetLastError();
 }
 

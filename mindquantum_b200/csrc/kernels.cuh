@@ -114,7 +114,7 @@ template <typename R>
 cudaError_t launch_copy_or_zero(cplx<R> *dst, const cplx<R> *src, int n, int64_t batch, int64_t src_stride,
                                 cudaStream_t s);
 cudaError_t launch_grad_scatter(const double *gslots, int64_t batch, int n_slots, int n_hams, const int32_t *csr_ptr,
-                                const int32_t *csr_slot, const double *csr_coeff, int n_params, double *grad,
+                                const int32_t *csr_slot, const double *csr_coeff, int n_params, double scale, double *grad,
                                 cudaStream_t s);
 template <typename R>
 cudaError_t launch_chunk_probs(const cplx<R> *st, int n, int chunk_bits, double *sums, cudaStream_t s);

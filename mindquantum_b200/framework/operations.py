@@ -86,3 +86,51 @@ class MQEncoderOnlyOps(torch.nn.Module):
 
     def forward(self, enc_data):
         return mq_expectation(enc_data, None, self.expectation_with_grad)
+
+
+class _QRamFunction(torch.autograd.Function):
+    """f[s][m] = Re <psi_s| U^dag H_m U |psi_s> for given initial states psi_s (QRamVecOps)."""
+
+    @staticmethod
+    def forward(ctx, qs_r, qs_i, ans, hams, circ, sim):  # pylint: disable=arguments-differ,too-many-arguments
+        names = circ.params_name
+        init = torch.complex(qs_r.detach().to(torch.float64), qs_i.detach().to(torch.float64)).to(
+            device=sim.device, dtype=sim.torch_dtype).contiguous()
+        batch = init.shape[0]
+        params = ans.detach().to(torch.float64).reshape(1, -1).expand(batch, -1).to(sim.device).contiguous()
+        f, g = sim.expectation_with_grad_tensor(hams, circ, params, names, init_state=init)
+        ctx.save_for_backward(g)
+        ctx.meta = (qs_r.shape, qs_r.dtype, qs_r.device, ans.dtype, ans.device)
+        return f[..., 0].to(device=qs_r.device, dtype=qs_r.dtype)
+
+    @staticmethod
+    def backward(ctx, dout):  # pylint: disable=arguments-differ
+        (g,) = ctx.saved_tensors
+        shape, dt, dev, adt, adev = ctx.meta
+        ans_grad = torch.einsum('smp,sm->p', g, dout.to(g.dtype).to(g.device)).to(device=adev, dtype=adt)
+        zero = torch.zeros(shape, dtype=dt, device=dev)   # no gradient with respect to the amplitudes
+        return zero, zero.clone(), ans_grad, None, None, None
+
+
+class QRamVecOps(torch.nn.Module):
+    """Initial states as input (mindquantum/framework/operations.py:539-664): forward(qs_r, qs_i,
+    ans_data) -> [n_states][n_hams] for states [n_states][2^n] given as real and imaginary parts;
+    the gradient flows to the ansatz parameters only, as in the reference."""
+
+    def __init__(self, hams, circ, sim, n_thread=None):  # pylint: disable=unused-argument
+        super().__init__()
+        from ..core.operators import Hamiltonian  # pylint: disable=import-outside-toplevel
+
+        self.hams = [hams] if isinstance(hams, Hamiltonian) else list(hams)
+        if circ.encoder_params_name:
+            raise ValueError("circ can not have encoder parameters.")
+        self.circ = circ
+        self.sim = getattr(sim, 'backend', sim)
+
+    def forward(self, qs_r, qs_i, ans_data):
+        dim = 1 << self.sim.n_qubits
+        if qs_r.shape != qs_i.shape or qs_r.dim() != 2 or qs_r.shape[1] != dim:
+            raise ValueError(f"quantum states need shape (N, {dim}), got {tuple(qs_r.shape)} and {tuple(qs_i.shape)}")
+        if ans_data.numel() != len(self.circ.params_name):
+            raise ValueError(f"ansatz data requires {len(self.circ.params_name)} values, got {ans_data.numel()}")
+        return _QRamFunction.apply(qs_r, qs_i, ans_data, self.hams, self.circ, self.sim)

@@ -361,8 +361,9 @@ class MQVectorB200(BackendBase):
         if not isinstance(circ_right, Circuit):
             raise TypeError(f"circ_right requires a Circuit, but get {type(circ_right)}")
         if circ_left is not None or simulator_left is not None:
-            raise NotImplementedError("the non-Hermitian adjoint (circ_left / simulator_left) is not part of the "
-                                      "mqvector_b200 backend")
+            if pr_shift:
+                raise NotImplementedError("parameter-shift gradients are not part of the mqvector_b200 backend")
+            return self._non_hermitian_grad_ops(hams, circ_right, circ_left, simulator_left, parallel_worker)
         if pr_shift:
             raise NotImplementedError("parameter-shift gradients are not part of the mqvector_b200 backend")
         if circ_right.has_measure_gate:
@@ -410,6 +411,124 @@ class MQVectorB200(BackendBase):
             if version == 'both':
                 return fc, gc[:, :, :len(enc_names)], gc[:, :, len(enc_names):]
             return fc, gc
+
+        wrapper = GradOpsWrapper(grad_ops, hams, circ_right, circ_left, enc_names, ans_names, parallel_worker, self)
+        wrapper.set_str(f"{self.n_qubits} qubit{'' if self.n_qubits == 1 else 's'} {self.name} VQA Operator")
+        return wrapper
+
+    # ------------------------------------------------------------------ non-Hermitian gradient
+    def _batched_states(self, circuit, names, init, params):
+        """[batch][2^n]: ``circuit`` applied to ``init`` for every parameter row."""
+        B = params.shape[0]
+        st = init.reshape(1, -1).expand(B, -1).contiguous()
+        prog = lowered(circuit, self.n_qubits, self.precision, names, None, self.fuse, jit=self.jit)
+        if prog.n_gates == 0:
+            return st
+        custom = self._custom_tensor(prog, params.cpu().numpy()) if prog.customs else None
+        ws_bytes = ctypes.c_size_t()
+        N.call('mqb_apply_workspace_size', prog.handle, B, ctypes.byref(ws_bytes))
+        ws = torch.empty(max(256, ws_bytes.value), dtype=torch.uint8, device=self.device)
+        N.call('mqb_apply', prog.handle, _ptr(st), B, _ptr(params), params.shape[1], _ptr(custom), _ptr(ws),
+               ws_bytes.value, _stream())
+        return st
+
+    def _adjoint_with_lambda(self, circuit, names, init, lam, params):
+        """[batch][len(names)] complex: sum over gates of <lam_g| dU_g |psi_{g-1}>, psi from ``init``."""
+        B = params.shape[0]
+        prog = lowered(circuit, self.n_qubits, self.precision, names, None, self.fuse, jit=self.jit)
+        custom = self._custom_tensor(prog, params.cpu().numpy()) if prog.customs else None
+        stride = self._choose_stride(prog, B, 1)
+        ws_bytes = ctypes.c_size_t()
+        N.call('mqb_grad_workspace_size', prog.handle, B, 1, stride, ctypes.byref(ws_bytes))
+        ws = torch.empty(max(256, ws_bytes.value), dtype=torch.uint8, device=self.device)
+        out = []
+        for lam_k in (lam, lam * 1j):   # Re <lam|..> and Re <i lam|..> = Im <lam|..>
+            lam_k = lam_k.contiguous()
+            g = torch.zeros((B, max(1, len(names))), dtype=torch.float64, device=self.device)
+            N.call('mqb_adjoint_with_lambda', prog.handle, _ptr(lam_k), 1, _ptr(init), 0, B, _ptr(params),
+                   params.shape[1], _ptr(custom), _ptr(g), stride, _ptr(ws), ws_bytes.value, _stream())
+            out.append(g[:, :len(names)])
+        return torch.complex(out[0], out[1])
+
+    def _non_hermitian_grad_ops(self, hams, circ_right, circ_left, simulator_left, parallel_worker):
+        """f = <phi| U_l^dag H U_r |psi> and its gradient over both circuits' parameters
+        (GradientHelper::NonHermitianAdjointGradient, ccsrc/include/simulator/vector/gradient.h:83-98,
+        199-268; mindquantum/simulator/mqsim.py:282-392).
+
+        The right circuit's gradient is sum <lambda_g| dU_g |psi_{g-1}> with lambda = H U_l phi carried
+        back through U_r; the left circuit's is the conjugate of the same sweep over U_l with
+        lambda = H U_r psi.  Each sweep runs with lambda and with i lambda (real and imaginary parts).
+        """
+        if simulator_left is not None:
+            simulator_left = getattr(simulator_left, 'backend', simulator_left)
+            if not isinstance(simulator_left, MQVectorB200):
+                raise TypeError("simulator_left should be a mqvector_b200 simulator")
+            if simulator_left.n_qubits != self.n_qubits:
+                raise ValueError(f"simulator_left should have the same n_qubits as this simulator, which is "
+                                 f"{self.n_qubits}, but get {simulator_left.n_qubits}")
+            if simulator_left.dtype != self.dtype:
+                raise TypeError(f"simulator_left should have the same data type as this simulator (aka "
+                                f"{self.dtype}), but get {simulator_left.dtype}.")
+        sim_left = self if simulator_left is None else simulator_left
+        circ_left = circ_right if circ_left is None else circ_left
+        if not isinstance(circ_left, Circuit):
+            raise TypeError(f"circ_left requires a Circuit, but get {type(circ_left)}")
+        if circ_left.has_measure_gate or circ_right.has_measure_gate:
+            raise ValueError("circuit for variational algorithm cannot have measure gate")
+        ans_names = list(circ_right.ansatz_params_name)
+        enc_names = list(circ_right.encoder_params_name)
+        ans_names += [k for k in circ_left.ansatz_params_name if k not in ans_names]
+        enc_names += [k for k in circ_left.encoder_params_name if k not in enc_names]
+        if set(ans_names) & set(enc_names):
+            raise RuntimeError("Parameter cannot be both encoder and ansatz parameter.")
+        n_circ = max(circ_left.n_qubits, circ_right.n_qubits)
+        if self.n_qubits < n_circ:
+            raise ValueError(f"Simulator has {self.n_qubits} qubits, but circuit has {n_circ} qubits.")
+        version = "both" if (ans_names and enc_names) else ("encoder" if enc_names else "ansatz")
+        names = enc_names + ans_names
+        sim = self
+
+        def grad_ops(*inputs_):
+            inputs = [np.array(x) if isinstance(x, list) else x for x in inputs_]
+            if version == "both" and len(inputs) != 2:
+                raise ValueError("Need two inputs!")
+            if version in ("encoder", "ansatz") and len(inputs) != 1:
+                raise ValueError("Need one input!")
+            if version in ("both", "encoder"):
+                enc = np.asarray(inputs[0], dtype=np.float64)
+                enc = enc[None, :] if enc.ndim == 1 else enc
+                if enc.ndim != 2 or enc.shape[1] != len(enc_names):
+                    raise ValueError(f"encoder data requires a two dimension array with {len(enc_names)} columns, "
+                                     f"but get shape {enc.shape}")
+                ans = np.asarray(inputs[1], dtype=np.float64).reshape(-1) if version == "both" else np.zeros(0)
+            else:
+                enc = np.zeros((1, 0))
+                ans = np.asarray(inputs[0], dtype=np.float64).reshape(-1)
+            if ans.size != len(ans_names):
+                raise ValueError(f"ansatz data requires {len(ans_names)} values, but get {ans.size}")
+            params = torch.as_tensor(np.concatenate([enc, np.broadcast_to(ans, (enc.shape[0], ans.size))], axis=1),
+                                     device=sim.device).contiguous()
+            B = params.shape[0]
+            psi0, phi0 = sim.state, sim_left.state
+            psi_r = sim._batched_states(circ_right, names, psi0, params)
+            psi_l = sim._batched_states(circ_left, names, phi0, params)
+            res = np.zeros((B, len(hams), 1 + len(names)), dtype=np.complex128)
+            for h_i, ham in enumerate(hams):
+                nh = native_ham(ham, sim.n_qubits, sim.precision)
+                out = torch.zeros((B, 2), dtype=torch.float64, device=sim.device)
+                N.call('mqb_expectation', nh.handle, _ptr(psi_l), _ptr(psi_r), B, _ptr(out), _stream())
+                h_l = torch.empty_like(psi_l)
+                N.call('mqb_apply_hamiltonian', nh.handle, _ptr(psi_l), _ptr(h_l), B, _stream())
+                h_r = torch.empty_like(psi_r)
+                N.call('mqb_apply_hamiltonian', nh.handle, _ptr(psi_r), _ptr(h_r), B, _stream())
+                g = sim._adjoint_with_lambda(circ_right, names, psi0, h_l, params)
+                g = g + sim._adjoint_with_lambda(circ_left, names, phi0, h_r, params).conj()
+                o = out.cpu().numpy()
+                res[:, h_i, 0] = o[:, 0] + 1j * o[:, 1]
+                res[:, h_i, 1:] = g.cpu().numpy()
+            if version == 'both':
+                return res[:, :, 0], res[:, :, 1:1 + len(enc_names)], res[:, :, 1 + len(enc_names):]
+            return res[:, :, 0], res[:, :, 1:]
 
         wrapper = GradOpsWrapper(grad_ops, hams, circ_right, circ_left, enc_names, ans_names, parallel_worker, self)
         wrapper.set_str(f"{self.n_qubits} qubit{'' if self.n_qubits == 1 else 's'} {self.name} VQA Operator")

@@ -96,6 +96,9 @@ def num_threads():
 
 
 def _ptr(a):
+    """Data pointer of a C-contiguous array (the C kernels index it densely)."""
+    if not a.flags['C_CONTIGUOUS']:
+        raise ValueError("the oracle's C kernels need C-contiguous arrays")
     return a.ctypes.data_as(ctypes.c_void_p)
 
 

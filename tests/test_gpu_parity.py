@@ -330,3 +330,82 @@ def test_large_register_properties(dtype):
         d[k] = 1e-4
         fd = (ops(p0 + d)[0] - ops(p0 - d)[0]).real / 2e-4
         assert abs(fd[0, 0] - g[0, 0, k].real) < (1e-6 if dtype == complex128 else 2e-2)
+
+
+@pytest.mark.parametrize("dtype", [complex128, complex64])
+def test_non_hermitian_gradient_against_dense_matrices(dtype):
+    """<phi| U_l^dag H U_r |psi> and its gradient over the parameters of both circuits
+    (tests/st/test_simulator/test_method_of_mqvector.py:130-172), against dense matrices built with
+    the oracle and central finite differences."""
+    from test_host import _random_circuit
+
+    n = 3
+    rng = np.random.default_rng(17)
+    psi0 = rng.normal(size=8) + 1j * rng.normal(size=8)
+    psi0 /= np.linalg.norm(psi0)
+    phi0 = rng.normal(size=8) + 1j * rng.normal(size=8)
+    phi0 /= np.linalg.norm(phi0)
+    fixed = ['h', 'x', 'cx', 'cz', 'swap', 'ccx', 'y']
+    circ0 = _random_circuit(rng, n, 40, fixed)
+    circ1 = _random_circuit(rng, n, 40, fixed)
+    circ_r = circ0 + G.RX({'a': 1, 'b': 2}).on(0) + circ1 + G.RZ('c').on(2, 1)
+    circ_l = _random_circuit(rng, n, 30, fixed) + G.RY('c').on(1) + G.Rzz({'d': 0.5}).on([0, 2])
+    ham = Hamiltonian(QubitOperator('X0 Y1', 0.3) + QubitOperator('Z2', -1.1) + QubitOperator('Y0 Z1 X2', 0.7))
+
+    def unitary(circ, pr):
+        cols = []
+        for k in range(8):
+            e = np.zeros(8, dtype=np.complex128)
+            e[k] = 1
+            cols.append(O.OracleSim(n, np.complex128, e).apply_circuit(circ, pr).qs)
+        return np.array(cols).T
+
+    eye = np.eye(8, dtype=np.complex128)
+    hmat = np.array([O.apply_terms(eye[k].copy(), n, ham) for k in range(8)]).T
+
+    def f_of(pr):
+        return phi0.conj() @ unitary(circ_l, pr).conj().T @ hmat @ unitary(circ_r, pr) @ psi0
+
+    sim = Simulator('mqvector_b200', n, dtype=dtype)
+    sim.set_qs(psi0)
+    sim_left = Simulator('mqvector_b200', n, dtype=dtype)
+    sim_left.set_qs(phi0)
+    ops = sim.get_expectation_with_grad(ham, circ_r, circ_l, sim_left)
+    names = ops.ansatz_params_name
+    p = rng.uniform(0, 2 * np.pi, len(names))
+    f, g = ops(p)
+    pr = dict(zip(names, p))
+    tol = 1e-10 if dtype == complex128 else 2e-5
+    assert abs(f[0, 0] - f_of(pr)) < tol
+    eps = 1e-6
+    for k, name in enumerate(names):
+        pp, pm = dict(pr), dict(pr)
+        pp[name] += eps
+        pm[name] -= eps
+        fd = (f_of(pp) - f_of(pm)) / (2 * eps)
+        assert abs(g[0, 0, k] - fd) < (1e-7 if dtype == complex128 else 5e-5), (name, g[0, 0, k], fd)
+
+
+def test_qram_operator_matches_oracle():
+    """QRamVecOps: a batch of initial states through one ansatz (operations.py:539-664)."""
+    from mindquantum_b200.framework import QRamVecOps
+
+    n = 6
+    rng = np.random.default_rng(23)
+    circ = hea_circuit(n, 2, prefix='w')
+    hams = [Hamiltonian(QubitOperator('Z0 Z1')), Hamiltonian(QubitOperator('X3', 0.4) + QubitOperator('Y5'))]
+    qs = rng.normal(size=(5, 1 << n)) + 1j * rng.normal(size=(5, 1 << n))
+    qs /= np.linalg.norm(qs, axis=1, keepdims=True)
+    ans = torch.tensor(rng.uniform(0, 2 * np.pi, len(circ.params_name)), dtype=torch.float64, requires_grad=True)
+    sim = Simulator('mqvector_b200', n, dtype=complex128)
+    op = QRamVecOps(hams, circ, sim)
+    out = op(torch.tensor(qs.real), torch.tensor(qs.imag), ans)
+    w = torch.tensor(rng.normal(size=(5, 2)), dtype=torch.float64)
+    (out * w).sum().backward()
+    g_ref = np.zeros(len(circ.params_name))
+    for s in range(5):
+        ref = O.get_expectation_with_grad(n, hams, circ, np.zeros((1, 0)), ans.detach().numpy(), [],
+                                          circ.params_name, np.complex128, qs[s])
+        assert np.allclose(out[s].detach().numpy(), ref[0, :, 0].real, atol=1e-10)
+        g_ref += np.einsum('mp,m->p', ref[0, :, 1:].real, w[s].numpy())
+    assert np.allclose(ans.grad.numpy(), g_ref, atol=1e-9)
