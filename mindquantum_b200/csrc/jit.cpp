@@ -594,7 +594,7 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
     std::ostringstream o;
     emit_header(o, precision);
     o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) << ", " << min_blocks(TB)
-      << ") mqb_pass(const JitFwdArgs<V> a) {\n"
+      << ") mqb_fwd_pass(const JitFwdArgs<V> a) {\n"
       << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", C = " << p.c << ";\n"
       << "  constexpr int NV = NR / (16 / int(sizeof(V)));\n"
       << "  extern __shared__ __align__(16) unsigned char smem[];\n"
@@ -641,7 +641,7 @@ std::string backward_source(const Schedule &s, const Pass &p, int precision, int
     std::ostringstream o;
     emit_header(o, precision);
     o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) << ", " << min_blocks(TB)
-      << ") mqb_pass(const JitBwdArgs<V> a) {\n"
+      << ") mqb_adj_pass(const JitBwdArgs<V> a) {\n"
       << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", C = " << p.c << ", NH = " << NH
       << ", NLS = " << NLS << ", TS = 1 << K;\n"
       << "  constexpr int NV = NR / (16 / int(sizeof(V)));\n"
@@ -765,7 +765,8 @@ std::vector<const void *> kernels_for(const std::vector<std::string> &srcs) {
                     throw std::runtime_error(msg);
                 }
                 cudaError_t ce = cudaLibraryLoadData(&e->lib, e->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-                if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&e->kernel, e->lib, "mqb_pass");
+                const char *name = e->src.find(") mqb_adj_pass(") != std::string::npos ? "mqb_adj_pass" : "mqb_fwd_pass";
+                if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&e->kernel, e->lib, name);
                 if (ce != cudaSuccess) {
                     g_cache.erase(e->src);
                     throw std::runtime_error(std::string("loading a generated pass kernel: ") + cudaGetErrorString(ce));

@@ -23,6 +23,7 @@ from ..dtype import complex64, complex128, to_mq_type
 from .backend_base import BackendBase
 from .lowering import lowered, native_ham
 from .measure_result import MeasureResult
+from .parameter_shift import ShiftPlan
 from .rng import Mt19937Uniform
 from .utils import GradOpsWrapper
 
@@ -33,6 +34,28 @@ def _stream():
 
 def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _split_inputs(version, enc_names, ans_names, inputs_):
+    """Encoder rows ``[n_prs][n_enc]`` and the ansatz vector of a grad operator call (mqsim.py:341-380)."""
+    inputs = [np.array(x) if isinstance(x, list) else x for x in inputs_]
+    if version == "both" and len(inputs) != 2:
+        raise ValueError("Need two inputs!")
+    if version in ("encoder", "ansatz") and len(inputs) != 1:
+        raise ValueError("Need one input!")
+    if version in ("both", "encoder"):
+        enc = np.asarray(inputs[0], dtype=np.float64)
+        enc = enc[None, :] if enc.ndim == 1 else enc
+        if enc.ndim != 2 or enc.shape[1] != len(enc_names):
+            raise ValueError(f"encoder data requires a two dimension array with {len(enc_names)} columns, "
+                             f"but get shape {enc.shape}")
+        ans = np.asarray(inputs[1], dtype=np.float64).reshape(-1) if version == "both" else np.zeros(0)
+    else:
+        enc = np.zeros((1, 0))
+        ans = np.asarray(inputs[0], dtype=np.float64).reshape(-1)
+    if ans.size != len(ans_names):
+        raise ValueError(f"ansatz data requires {len(ans_names)} values, but get {ans.size}")
+    return enc, ans
 
 
 def _require_cuda():
@@ -361,11 +384,10 @@ class MQVectorB200(BackendBase):
         if not isinstance(circ_right, Circuit):
             raise TypeError(f"circ_right requires a Circuit, but get {type(circ_right)}")
         if circ_left is not None or simulator_left is not None:
-            if pr_shift:
-                raise NotImplementedError("parameter-shift gradients are not part of the mqvector_b200 backend")
+            # the reference takes the non-Hermitian branch before looking at pr_shift (mqsim.py:384-401)
             return self._non_hermitian_grad_ops(hams, circ_right, circ_left, simulator_left, parallel_worker)
         if pr_shift:
-            raise NotImplementedError("parameter-shift gradients are not part of the mqvector_b200 backend")
+            return self._parameter_shift_grad_ops(hams, circ_right, parallel_worker)
         if circ_right.has_measure_gate:
             raise ValueError("circuit for variational algorithm cannot have measure gate")
         if self.n_qubits < circ_right.n_qubits:
@@ -383,24 +405,7 @@ class MQVectorB200(BackendBase):
         sim = self
 
         def grad_ops(*inputs_):
-            inputs = [np.array(x) if isinstance(x, list) else x for x in inputs_]
-            if version == "both" and len(inputs) != 2:
-                raise ValueError("Need two inputs!")
-            if version in ("encoder", "ansatz") and len(inputs) != 1:
-                raise ValueError("Need one input!")
-            if version in ("both", "encoder"):
-                enc = np.asarray(inputs[0], dtype=np.float64)
-                if enc.ndim == 1:
-                    enc = enc[None, :]
-                if enc.ndim != 2 or enc.shape[1] != len(enc_names):
-                    raise ValueError(f"encoder data requires a two dimension array with {len(enc_names)} columns, "
-                                     f"but get shape {enc.shape}")
-                ans = np.asarray(inputs[1], dtype=np.float64).reshape(-1) if version == "both" else np.zeros(0)
-            else:
-                enc = np.zeros((1, 0))
-                ans = np.asarray(inputs[0], dtype=np.float64).reshape(-1)
-            if ans.size != len(ans_names):
-                raise ValueError(f"ansatz data requires {len(ans_names)} values, but get {ans.size}")
+            enc, ans = _split_inputs(version, enc_names, ans_names, inputs_)
             params = np.concatenate([enc, np.broadcast_to(ans, (enc.shape[0], ans.size))], axis=1)
             init = sim._state
             f, g = sim.expectation_with_grad_tensor(hams, circ_right, torch.as_tensor(params), names, init_state=init)
@@ -489,23 +494,7 @@ class MQVectorB200(BackendBase):
         sim = self
 
         def grad_ops(*inputs_):
-            inputs = [np.array(x) if isinstance(x, list) else x for x in inputs_]
-            if version == "both" and len(inputs) != 2:
-                raise ValueError("Need two inputs!")
-            if version in ("encoder", "ansatz") and len(inputs) != 1:
-                raise ValueError("Need one input!")
-            if version in ("both", "encoder"):
-                enc = np.asarray(inputs[0], dtype=np.float64)
-                enc = enc[None, :] if enc.ndim == 1 else enc
-                if enc.ndim != 2 or enc.shape[1] != len(enc_names):
-                    raise ValueError(f"encoder data requires a two dimension array with {len(enc_names)} columns, "
-                                     f"but get shape {enc.shape}")
-                ans = np.asarray(inputs[1], dtype=np.float64).reshape(-1) if version == "both" else np.zeros(0)
-            else:
-                enc = np.zeros((1, 0))
-                ans = np.asarray(inputs[0], dtype=np.float64).reshape(-1)
-            if ans.size != len(ans_names):
-                raise ValueError(f"ansatz data requires {len(ans_names)} values, but get {ans.size}")
+            enc, ans = _split_inputs(version, enc_names, ans_names, inputs_)
             params = torch.as_tensor(np.concatenate([enc, np.broadcast_to(ans, (enc.shape[0], ans.size))], axis=1),
                                      device=sim.device).contiguous()
             B = params.shape[0]
@@ -531,6 +520,59 @@ class MQVectorB200(BackendBase):
             return res[:, :, 0], res[:, :, 1:]
 
         wrapper = GradOpsWrapper(grad_ops, hams, circ_right, circ_left, enc_names, ans_names, parallel_worker, self)
+        wrapper.set_str(f"{self.n_qubits} qubit{'' if self.n_qubits == 1 else 's'} {self.name} VQA Operator")
+        return wrapper
+
+    # ------------------------------------------------------------------ parameter shift
+    def _row_expectations(self, circuit, names, init, rows, hams):
+        """<psi_r|H_h|psi_r> for psi_r = circuit(rows[r]) applied to ``init``: ``[n_rows][n_hams]`` complex.
+
+        Rows run through the batched forward kernels in chunks that take at most 40 % of the free
+        device memory."""
+        n_rows = rows.shape[0]
+        if rows.shape[1] == 0:
+            rows = np.zeros((n_rows, 1))
+        S = (1 << self.n_qubits) * (8 if self.precision == N.MQB_PREC_C64 else 16)
+        free, _ = torch.cuda.mem_get_info(self.device)
+        chunk = int(max(1, min(n_rows, 2048, (0.4 * free) // S)))
+        nhs = [native_ham(h, self.n_qubits, self.precision) for h in hams]
+        out = torch.empty((len(hams), n_rows, 2), dtype=torch.float64, device=self.device)
+        for a in range(0, n_rows, chunk):
+            p = torch.as_tensor(rows[a:a + chunk], dtype=torch.float64, device=self.device).contiguous()
+            st = self._batched_states(circuit, names, init, p)
+            for h, nh in enumerate(nhs):
+                N.call('mqb_expectation', nh.handle, _ptr(st), _ptr(st), p.shape[0], _ptr(out[h, a:a + p.shape[0]]),
+                       _stream())
+            del st
+        o = out.cpu().numpy()
+        return (o[..., 0] + 1j * o[..., 1]).T
+
+    def _parameter_shift_grad_ops(self, hams, circ, parallel_worker):
+        """Gradients by the parameter-shift rule (mqsim.py:401-411;
+        ``GetExpectationWithGradParameterShiftMultiMulti``, vector_state.tpp:1033-1305), every
+        shifted circuit of every sample evaluated as one batch (``parameter_shift.ShiftPlan``)."""
+        if circ.has_measure_gate:
+            raise ValueError("circuit for variational algorithm cannot have measure gate")
+        if self.n_qubits < circ.n_qubits:
+            raise ValueError(f"Simulator has {self.n_qubits} qubits, but circuit has {circ.n_qubits} qubits.")
+        ans_names = list(circ.ansatz_params_name)
+        enc_names = list(circ.encoder_params_name)
+        if set(ans_names) & set(enc_names):
+            raise RuntimeError("Parameter cannot be both encoder and ansatz parameter.")
+        version = "both" if (ans_names and enc_names) else ("encoder" if enc_names else "ansatz")
+        plan = ShiftPlan(circ, enc_names + ans_names)
+        sim = self
+
+        def grad_ops(*inputs_):
+            enc, ans = _split_inputs(version, enc_names, ans_names, inputs_)
+            P = np.concatenate([enc, np.broadcast_to(ans, (enc.shape[0], ans.size))], axis=1)
+            F = sim._row_expectations(plan.circuit, plan.slot_names, sim.state, plan.rows(P), hams)
+            f, g = plan.combine(F)
+            if version == 'both':
+                return f, g[:, :, :len(enc_names)], g[:, :, len(enc_names):]
+            return f, g
+
+        wrapper = GradOpsWrapper(grad_ops, hams, circ, None, enc_names, ans_names, parallel_worker, self)
         wrapper.set_str(f"{self.n_qubits} qubit{'' if self.n_qubits == 1 else 's'} {self.name} VQA Operator")
         return wrapper
 

@@ -15,6 +15,8 @@ What it restates (reference file:line, paths inside mindquantum-ai/mindquantum):
     ``GeneratePMap`` and the Jacobi of ``Parameterizable`` (ccsrc/include/simulator/vector/gradient.h:100-197,
     ccsrc/include/ops/basic_gate.h:208-241, ccsrc/lib/math/pr/parameter_resolver.cpp:560-573);
   * ``GetExpectation`` (vector_state.tpp:712-726), ``ApplyHamiltonian`` (vector_state.tpp:963-974);
+  * ``GetExpectationWithGradParameterShiftOneMulti`` / ``MultiMulti`` (vector_state.tpp:1033-1305)
+    in ``get_expectation_with_grad_parameter_shift``, with the shift table of ``shift_rule``;
   * ``SamplingMeasurementEndingWithoutNoise`` (vector_state.tpp:1326-1373) with the reference's
     random streams (std::mt19937 + std::uniform_real_distribution<double>), restated in
     ``_Mt19937`` / ``_uniform``.
@@ -31,6 +33,7 @@ oracle's own formulas below, never the gate object's matrices.
 """
 from __future__ import annotations
 
+import copy
 import ctypes
 import math
 import os
@@ -524,6 +527,85 @@ def get_expectation_with_grad(n, hams, circ, enc_data, ans_data, enc_names, ans_
     res[:, :, 1:] = res[:, :, 1:] + np.conj(res[:, :, 1:])   # GradRealDouble
     return res
 
+
+
+# ----------------------------------------------------------------------------- parameter shift
+_PS_EXACT = ('RX', 'RY', 'RZ', 'Rxx', 'Ryy', 'Rzz', 'Rxy', 'Rxz', 'Ryz', 'GP', 'PS', 'U3')
+_PS_MULTI = ('U3', 'FSim')
+
+
+def shift_rule(g):
+    """(shift, coefficient, shifts-the-parameter-value) of one gate, vector_state.tpp:1076-1174.
+
+    Rotation-like gates: +-pi/2 and 1/2; SWAPalpha: +-1/2 and pi/2; every other supported gate and
+    every controlled gate: central difference with step 1e-3.  U3 and FSim keep their angles
+    outside the coefficient list the shift edits, so the reference shifts the value of the first
+    (lexicographically smallest) parameter of the angle instead, which moves every gate using it.
+    """
+    custom = hasattr(g, 'matrix_generator')
+    if not (custom or g.name in _PS_EXACT or g.name in _PS_MULTI or g.name in ('G', 'SWAPalpha')):
+        raise RuntimeError(f"gate {g.name} not supported for parameter shift rule.")
+    if custom:
+        shift, coeff = 0.001, 0.5 / 0.001
+    elif g.name in _PS_EXACT:
+        shift, coeff = math.pi / 2, 0.5
+    elif g.name == 'SWAPalpha':
+        shift, coeff = 0.5, math.pi / 2
+    else:
+        shift, coeff = 0.001, 0.5 / 0.001
+    if len(g.ctrl_qubits):
+        shift, coeff = 0.001, 0.5 / 0.001
+    return shift, coeff, (not custom and g.name in _PS_MULTI)
+
+
+def get_expectation_with_grad_parameter_shift(n, hams, circ, enc_data, ans_data, enc_names, ans_names,
+                                              dtype=np.complex128, init_state=None):
+    """GetExpectationWithGradParameterShiftOneMulti / MultiMulti (vector_state.tpp:1033-1305).
+
+    For every gate whose parameters require a gradient and every non-constant angle k of it, the
+    circuit is evaluated with the angle shifted down and up; coeff * Re(f+ - f-) is the derivative
+    with respect to the angle, and the gate's Jacobi row spreads it over the named parameters.
+    Returns ``[n_prs][n_hams][1 + n_enc + n_ans]`` complex.
+    """
+    gates = [g for g in circ]
+    enc_data = np.atleast_2d(np.asarray(enc_data, dtype=np.float64)) if len(enc_names) else np.zeros((1, 0))
+    ans_data = np.asarray(ans_data, dtype=np.float64).reshape(-1)
+    p_map = {k: i for i, k in enumerate(enc_names)}
+    p_map.update({k: i + len(enc_names) for i, k in enumerate(ans_names)})
+    out = np.zeros((enc_data.shape[0], len(hams), 1 + len(p_map)), dtype=np.complex128)
+
+    def values(gate_list, prd):
+        qs = OracleSim(n, dtype, init_state).apply_circuit(gate_list, prd).qs
+        return np.array([expectation_of_terms(qs, qs, n, h) for h in hams])
+
+    for s in range(enc_data.shape[0]):
+        prd = dict(zip(enc_names, enc_data[s].tolist()))
+        prd.update(dict(zip(ans_names, ans_data.tolist())))
+        out[s, :, 0] = values(gates, prd)
+        for gi, g in enumerate(gates):
+            prs = getattr(g, 'prs', None)
+            if not prs or not any(len(p.requires_grad_parameters) for p in prs):
+                continue
+            shift, coeff, multi = shift_rule(g)
+            for k, p in enumerate(prs):
+                if p.is_const():
+                    continue
+                f = []
+                for sign in (-1.0, 1.0):
+                    shifted, pr_s = g, prd
+                    if multi:
+                        key = min(p.keys())
+                        pr_s = dict(prd)
+                        pr_s[key] = prd[key] + sign * shift / float(np.real(p[key]))
+                    else:
+                        shifted = copy.copy(g)
+                        shifted.prs = list(prs)
+                        shifted.prs[k] = p + sign * shift
+                    f.append(values(gates[:gi] + [shifted] + gates[gi + 1:], pr_s))
+                intrin = coeff * np.real(f[1] - f[0])
+                for name in p.requires_grad_parameters:
+                    out[s, :, 1 + p_map[name]] += intrin * float(np.real(p[name]))
+    return out
 
 # ----------------------------------------------------------------------------- sampling
 class _Mt19937:
