@@ -172,6 +172,15 @@ MQB_API int mqb_apply(mqb_program *prog, void *states, int64_t batch, const doub
 MQB_API int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const uint64_t *mask_y,
                    const uint64_t *mask_z, const int32_t *num_y, const double *coeff, int n_terms,
                    mqb_hamiltonian **out);
+/* A Hamiltonian given as a sparse 2^n x 2^n matrix in CSR form: indptr [2^n + 1] int64 from 0 to
+ * nnz, indices [nnz] int64 column indices, data [nnz] complex (complex64 for MQB_PREC_C64, else
+ * complex128), all host arrays, copied to the device.  Every call that takes a Hamiltonian
+ * (apply, expectation, adjoint gradient) then applies the matrix with the CSR kernel.  Replaces
+ * Hamiltonian(csr_matrix) (HowTo FRONTEND, ccsrc/include/ops/hamiltonian.h:47-49) with
+ * Csr_Dot_Vec / ExpectationOfCsr (ccsrc/include/core/sparse/algo.h:160-200,
+ * cpu_vector_core_dot_like.cpp:132-222). */
+MQB_API int mqb_ham_create_csr(int n_qubits, int precision, int64_t nnz, const int64_t *indptr,
+                               const int64_t *indices, const void *data, mqb_hamiltonian **out);
 MQB_API int mqb_ham_destroy(mqb_hamiltonian *ham);
 
 /* out = H in (separate buffers), `batch` states. */

@@ -85,6 +85,7 @@ SIGNATURES = {
     'mqb_apply': [_P, _P, _I64, _P, _I64, _P, _P, _SZ, _P],
     'mqb_apply_static': [_P, _P, _I64, _P, _I64, _P, _P],
     'mqb_ham_create': [_I, _I, _P, _P, _P, _P, _P, _I, _P],
+    'mqb_ham_create_csr': [_I, _I, _I64, _P, _P, _P, _P],
     'mqb_ham_destroy': [_P],
     'mqb_apply_hamiltonian': [_P, _P, _P, _I64, _P],
     'mqb_expectation': [_P, _P, _P, _I64, _P, _P],

@@ -1,11 +1,11 @@
 """Pauli operators and Hamiltonians.
 
 ``QubitOperator`` mirrors the reference qubit operator for Pauli-string sums (term keys are
-tuples of ``(qubit, 'X'|'Y'|'Z')`` sorted by qubit).  ``Hamiltonian`` mirrors the term-list
-mode of mindquantum/core/operators/hamiltonian.py:40-245 (``HowTo.ORIGIN``): real
-coefficients (imaginary parts discarded with a warning, as the reference does), each term
-lowered to the reference ``PauliMask`` (mask_x, mask_y, mask_z, num_y;
-ccsrc/lib/simulator/utils.cpp:28-40).
+tuples of ``(qubit, 'X'|'Y'|'Z')`` sorted by qubit).  ``Hamiltonian`` mirrors
+mindquantum/core/operators/hamiltonian.py:26-245: the term-list mode (real coefficients,
+imaginary parts discarded with a warning, as the reference does; each term lowered to the
+reference ``PauliMask`` (mask_x, mask_y, mask_z, num_y; ccsrc/lib/simulator/utils.cpp:28-40)),
+``.sparse(n)``, and Hamiltonians given as a ``scipy.sparse.csr_matrix``.
 """
 from __future__ import annotations
 
@@ -143,19 +143,49 @@ class QubitOperator:
     __repr__ = __str__
 
 
+class HowTo:
+    """How a Hamiltonian is applied (mindquantum/core/operators/hamiltonian.py:26-32)."""
+
+    ORIGIN = 0     # Pauli term list
+    BACKEND = 1    # Pauli terms, treated as a sparse matrix of a fixed register size
+    FRONTEND = 2   # a user-given sparse matrix
+
+
 class Hamiltonian:
-    """A real-coefficient Pauli-sum Hamiltonian (term-list mode)."""
+    """A Hamiltonian: a real-coefficient Pauli sum or a sparse matrix (hamiltonian.py:35-245).
+
+    ``Hamiltonian(QubitOperator)`` keeps the term list (``HowTo.ORIGIN``; imaginary parts of the
+    coefficients discarded with a warning, as the reference does); ``.sparse(n)`` marks it as a
+    sparse Hamiltonian of exactly ``n`` qubits (``HowTo.BACKEND``: the reference converts the
+    terms to a CSR matrix on the CPU; here the same operator keeps running through the Pauli
+    kernels).  ``Hamiltonian(scipy.sparse.csr_matrix)`` (``HowTo.FRONTEND``) applies the matrix
+    itself with the device CSR kernel.
+    """
 
     def __init__(self, hamiltonian, dtype=None):
+        import scipy.sparse as sp
+
+        if isinstance(hamiltonian, sp.csr_matrix):
+            if len(hamiltonian.shape) != 2 or hamiltonian.shape[0] != hamiltonian.shape[1]:
+                raise ValueError(
+                    f"Hamiltonian requires a two dimension square csr_matrix, but get shape {hamiltonian.shape}")
+            if np.log2(hamiltonian.shape[0]) % 1 != 0:
+                raise ValueError(f"size of hamiltonian sparse matrix should be power of 2, but get {hamiltonian.shape}")
+            self.ham_dtype = to_mq_type(dtype) if dtype is not None else to_mq_type(hamiltonian.dtype)
+            self._hamiltonian = None
+            self._ham_termlist = None
+            self._sparse_matrix = hamiltonian
+            self.how_to = HowTo.FRONTEND
+            self.n_qubits = int(np.log2(hamiltonian.shape[0]))
+            return
         if not isinstance(hamiltonian, QubitOperator):
-            raise TypeError(
-                "Only Pauli-sum Hamiltonians (QubitOperator) are supported on the state-vector path; "
-                f"got {type(hamiltonian)}. Sparse-matrix Hamiltonians are not part of this backend."
-            )
+            raise TypeError(f"Require a QubitOperator or a csr_matrix, but get {type(hamiltonian)}!")
         self.ham_dtype = to_mq_type(dtype) if dtype is not None else complex128
-        self.hamiltonian = hamiltonian
+        self._hamiltonian = hamiltonian
+        self._sparse_matrix = None
+        self.how_to = HowTo.ORIGIN
         self.n_qubits = hamiltonian.n_qubits
-        self.ham_termlist = []
+        self._ham_termlist = []
         warned = False
         for k, v in hamiltonian.terms.items():
             v = complex(v)
@@ -166,24 +196,58 @@ class Hamiltonian:
                     stacklevel=2,
                 )
                 warned = True
-            self.ham_termlist.append((k, v.real))
+            self._ham_termlist.append((k, v.real))
 
     @property
     def dtype(self):
         return self.ham_dtype
 
+    @property
+    def hamiltonian(self):
+        if self.how_to == HowTo.FRONTEND:
+            raise ValueError("Cannot get QubitOperator: this Hamiltonian was constructed from a sparse matrix.")
+        return self._hamiltonian
+
+    @property
+    def ham_termlist(self):
+        if self.how_to == HowTo.FRONTEND:
+            raise ValueError("Cannot get Pauli term list: this Hamiltonian was constructed from a sparse matrix.")
+        return self._ham_termlist
+
+    @property
+    def sparse_matrix(self):
+        """The matrix as ``scipy.sparse.csr_matrix``."""
+        if self.how_to != HowTo.FRONTEND:
+            import scipy.sparse as sp
+
+            return sp.csr_matrix(self._hamiltonian.matrix(self.n_qubits))
+        return self._sparse_matrix
+
+    def sparse(self, n_qubits=1):
+        """Mark the Hamiltonian as sparse on exactly ``n_qubits`` qubits (hamiltonian.py:122-136)."""
+        if self.how_to != HowTo.ORIGIN:
+            raise ValueError('Already a sparse hamiltonian.')
+        if n_qubits < self.n_qubits:
+            raise ValueError(f"Can not sparse a {self.n_qubits} qubits hamiltonian to {n_qubits} hamiltonian.")
+        self.n_qubits = n_qubits
+        self.how_to = HowTo.BACKEND
+        return self
+
     def astype(self, dtype):
-        return Hamiltonian(self.hamiltonian, dtype)
+        if self.how_to == HowTo.FRONTEND:
+            return Hamiltonian(self._sparse_matrix, dtype)
+        return Hamiltonian(self._hamiltonian, dtype)
 
     def pauli_masks(self):
         """(mask_x, mask_y, mask_z, num_y, coeff) arrays; GenPauliMask, ccsrc/lib/simulator/utils.cpp:28-40."""
-        nt = len(self.ham_termlist)
+        terms = self.ham_termlist
+        nt = len(terms)
         mx = np.zeros(nt, dtype=np.uint64)
         my = np.zeros(nt, dtype=np.uint64)
         mz = np.zeros(nt, dtype=np.uint64)
         ny = np.zeros(nt, dtype=np.int32)
         cf = np.zeros(nt, dtype=np.float64)
-        for t, (k, v) in enumerate(self.ham_termlist):
+        for t, (k, v) in enumerate(terms):
             for q, p in k:
                 bit = np.uint64(1) << np.uint64(q)
                 if p == 'X':
@@ -197,9 +261,13 @@ class Hamiltonian:
         return mx, my, mz, ny, cf
 
     def matrix(self, n_qubits=None):
-        return self.hamiltonian.matrix(n_qubits)
+        if self.how_to == HowTo.FRONTEND:
+            return self._sparse_matrix
+        return self._hamiltonian.matrix(n_qubits)
 
     def __str__(self):
-        return str(self.hamiltonian)
+        if self.how_to == HowTo.FRONTEND:
+            return str(self._sparse_matrix)
+        return str(self._hamiltonian)
 
     __repr__ = __str__

@@ -116,13 +116,24 @@ void set_last_error(const char *msg) { g_last_error = msg; }
 
 struct mqb_hamiltonian {
     int n = 0, precision = 0;
+    // Pauli terms, grouped for the register-binned kernel
     std::vector<HamGroup> groups;
     std::vector<HamClass> classes;
     HamClass *d_classes = nullptr;
     HamTerm *d_terms = nullptr;
+    // or a CSR matrix (csr == true)
+    bool csr = false;
+    int csr_lanes = 1;
+    int64_t nnz = 0;
+    int64_t *d_indptr = nullptr;
+    int32_t *d_indices = nullptr;
+    void *d_data = nullptr;
     ~mqb_hamiltonian() {
         cudaFree(d_classes);
         cudaFree(d_terms);
+        cudaFree(d_indptr);
+        cudaFree(d_indices);
+        cudaFree(d_data);
     }
 };
 
@@ -341,6 +352,22 @@ static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R>
                      int64_t f_stride, int64_t batch, cudaStream_t st) {
     const int sm = sm_count_cached();
     const int64_t dim = int64_t(1) << h.n;
+    if (h.csr) {
+        CsrArgs<R> a{};
+        a.indptr = h.d_indptr;
+        a.indices = h.d_indices;
+        a.data = static_cast<const cplx<R> *>(h.d_data);
+        a.dim = dim;
+        a.bra = bra;
+        a.ket = ket;
+        a.out = out;
+        a.fout = fout;
+        a.f_stride = f_stride;
+        a.batch = batch;
+        TimeScope ts(TK_HAM, st);
+        ck(launch_csr<R>(a, h.csr_lanes, sm, st), "sparse hamiltonian");
+        return;
+    }
     if (h.groups.empty()) {
         // zero Hamiltonian
         if (out) ck(cudaMemsetAsync(out, 0, sizeof(cplx<R>) * dim * batch, st), "memset");
@@ -914,6 +941,45 @@ int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const ui
         h->classes = classes;
         h->d_classes = upload(classes);
         h->d_terms = upload(hterms);
+        *out = h.release();
+    });
+}
+
+int mqb_ham_create_csr(int n_qubits, int precision, int64_t nnz, const int64_t *indptr, const int64_t *indices,
+                       const void *data, mqb_hamiltonian **out) {
+    return guarded([&] {
+        if (!out) fail(MQB_ERR_INVALID, "out is null");
+        *out = nullptr;
+        if (n_qubits < 1 || n_qubits > 31) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 31] for a sparse Hamiltonian");
+        if (precision != MQB_PREC_C64 && precision != MQB_PREC_C128) fail(MQB_ERR_INVALID, "unknown precision");
+        if (nnz < 0 || !indptr || (nnz > 0 && (!indices || !data))) fail(MQB_ERR_INVALID, "null CSR array");
+        const int64_t dim = int64_t(1) << n_qubits;
+        if (indptr[0] != 0 || indptr[dim] != nnz) fail(MQB_ERR_INVALID, "indptr must run from 0 to nnz");
+        for (int64_t r = 0; r < dim; ++r)
+            if (indptr[r + 1] < indptr[r]) fail(MQB_ERR_INVALID, "indptr decreases at row %lld", (long long)r);
+        std::vector<int32_t> idx(static_cast<size_t>(nnz));
+        for (int64_t j = 0; j < nnz; ++j) {
+            if (indices[j] < 0 || indices[j] >= dim)
+                fail(MQB_ERR_INVALID, "column index %lld out of range at entry %lld", (long long)indices[j], (long long)j);
+            idx[size_t(j)] = int32_t(indices[j]);
+        }
+        auto h = std::make_unique<mqb_hamiltonian>();
+        h->n = n_qubits;
+        h->precision = precision;
+        h->csr = true;
+        h->nnz = nnz;
+        // lanes per row: about four entries per lane
+        const double mean = double(nnz) / double(dim);
+        int lanes = 1;
+        while (lanes < 32 && lanes * 4 < mean) lanes *= 2;
+        h->csr_lanes = lanes;
+        h->d_indptr = upload(std::vector<int64_t>(indptr, indptr + dim + 1));
+        h->d_indices = upload(idx);
+        const size_t elem = precision == MQB_PREC_C64 ? 8 : 16;
+        if (nnz > 0) {
+            ck(cudaMalloc(&h->d_data, elem * size_t(nnz)), "cudaMalloc");
+            ck(cudaMemcpy(h->d_data, data, elem * size_t(nnz), cudaMemcpyHostToDevice), "cudaMemcpy");
+        }
         *out = h.release();
     });
 }

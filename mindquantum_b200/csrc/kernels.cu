@@ -913,6 +913,115 @@ cudaError_t launch_vdot(const cplx<R> *a, const cplx<R> *b, int n, int64_t batch
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ sparse (CSR) Hamiltonians
+// out[b] = A ket[b] and fout[b] += <bra[b]|A ket[b]> for a CSR matrix A (Csr_Dot_Vec /
+// ExpectationOfCsr, ccsrc/include/core/sparse/algo.h:160-200).  G lanes share a row (G a power
+// of two dividing 32, chosen from the mean row length); one pass over the matrix serves up to
+// kCsrStates states, so the matrix is read ceil(batch / kCsrStates) times.  Rows run in warp-
+// uniform steps so the group reductions are full-warp shuffles.  Row sums are in the state
+// precision like the reference's; the expectation is accumulated in FP64.
+constexpr int kCsrStates = 4;
+
+template <typename R, int G>
+__global__ void __launch_bounds__(256) csr_kernel(CsrArgs<R> a, int64_t b0) {
+    __shared__ double red[2 * kCsrStates][8];
+    const int nb = int(a.batch - b0 < kCsrStates ? a.batch - b0 : kCsrStates);
+    const int lane = threadIdx.x & 31, lg = lane & (G - 1);
+    const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+    const int64_t n_warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    constexpr int kRowsPerWarp = 32 / G;
+    double fre[kCsrStates], fim[kCsrStates];
+#pragma unroll
+    for (int k = 0; k < kCsrStates; ++k) fre[k] = fim[k] = 0;
+    for (int64_t base = warp * kRowsPerWarp; base < a.dim; base += n_warps * kRowsPerWarp) {
+        const int64_t row = base + lane / G;
+        const bool valid = row < a.dim;
+        R ar[kCsrStates], ai[kCsrStates];
+#pragma unroll
+        for (int k = 0; k < kCsrStates; ++k) ar[k] = ai[k] = 0;
+        if (valid) {
+            const int64_t end = a.indptr[row + 1];
+            for (int64_t j = a.indptr[row] + lg; j < end; j += G) {
+                const int64_t col = a.indices[j];
+                const cplx<R> d = a.data[j];
+#pragma unroll
+                for (int k = 0; k < kCsrStates; ++k) {
+                    if (k < nb) {
+                        const cplx<R> x = a.ket[(b0 + k) * a.dim + col];
+                        ar[k] += d.x * x.x - d.y * x.y;
+                        ai[k] += d.x * x.y + d.y * x.x;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kCsrStates; ++k) {
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) {
+                ar[k] += __shfl_xor_sync(0xffffffffu, ar[k], o);
+                ai[k] += __shfl_xor_sync(0xffffffffu, ai[k], o);
+            }
+        }
+        if (valid && lg == 0) {
+#pragma unroll
+            for (int k = 0; k < kCsrStates; ++k) {
+                if (k < nb) {
+                    const int64_t at = (b0 + k) * a.dim + row;
+                    if (a.out) a.out[at] = cplx<R>{ar[k], ai[k]};
+                    if (a.fout) {
+                        const cplx<R> bv = a.bra[at];
+                        fre[k] += double(bv.x) * ar[k] + double(bv.y) * ai[k];
+                        fim[k] += double(bv.x) * ai[k] - double(bv.y) * ar[k];
+                    }
+                }
+            }
+        }
+    }
+    if (!a.fout) return;
+#pragma unroll
+    for (int k = 0; k < kCsrStates; ++k) {
+        const double r = warp_sum(fre[k]), i = warp_sum(fim[k]);
+        if (lane == 0) {
+            red[2 * k][threadIdx.x >> 5] = r;
+            red[2 * k + 1][threadIdx.x >> 5] = i;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const bool ok = threadIdx.x < (blockDim.x >> 5);
+        for (int k = 0; k < nb; ++k) {
+            const double r = warp_sum(ok ? red[2 * k][threadIdx.x] : 0.0);
+            const double i = warp_sum(ok ? red[2 * k + 1][threadIdx.x] : 0.0);
+            if (threadIdx.x == 0) {
+                atomicAdd(&a.fout[(b0 + k) * a.f_stride], r);
+                atomicAdd(&a.fout[(b0 + k) * a.f_stride + 1], i);
+            }
+        }
+    }
+}
+
+template <typename R>
+cudaError_t launch_csr(const CsrArgs<R> &a, int lanes, int sm_count, cudaStream_t s) {
+    const int threads = 256;
+    const int64_t rows_per_block = int64_t(threads / lanes);
+    const int blocks = int(std::max<int64_t>(1, std::min<int64_t>((a.dim + rows_per_block - 1) / rows_per_block,
+                                                                  int64_t(sm_count) * 8)));
+    for (int64_t b0 = 0; b0 < a.batch; b0 += kCsrStates) {
+        switch (lanes) {
+            case 1: csr_kernel<R, 1><<<blocks, threads, 0, s>>>(a, b0); break;
+            case 2: csr_kernel<R, 2><<<blocks, threads, 0, s>>>(a, b0); break;
+            case 4: csr_kernel<R, 4><<<blocks, threads, 0, s>>>(a, b0); break;
+            case 8: csr_kernel<R, 8><<<blocks, threads, 0, s>>>(a, b0); break;
+            case 16: csr_kernel<R, 16><<<blocks, threads, 0, s>>>(a, b0); break;
+            case 32: csr_kernel<R, 32><<<blocks, threads, 0, s>>>(a, b0); break;
+            default: return cudaErrorInvalidValue;
+        }
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 template <typename R>
 __global__ void copy_kernel(cplx<R> *dst, const cplx<R> *src, int n, int64_t batch, int64_t src_stride) {
     const int64_t dim = int64_t(1) << n;
@@ -1144,6 +1253,7 @@ cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale
     template cudaError_t launch_vdot<R>(const cplx<R> *, const cplx<R> *, int, int64_t, double *, int,             \
                                         cudaStream_t);                                                             \
     template cudaError_t launch_copy_or_zero<R>(cplx<R> *, const cplx<R> *, int, int64_t, int64_t, cudaStream_t);  \
+    template cudaError_t launch_csr<R>(const CsrArgs<R> &, int, int, cudaStream_t);                                 \
     template cudaError_t launch_chunk_probs<R>(const cplx<R> *, int, int, double *, cudaStream_t);                 \
     template cudaError_t launch_sample_search<R>(const cplx<R> *, int, int, const double *, const double *,       \
                                                  int64_t, int64_t *, cudaStream_t);                                \

@@ -110,6 +110,23 @@ cudaError_t launch_plain_grad(const cplx<R> *psi, const cplx<R> *lam, int n, int
 template <typename R>
 cudaError_t launch_vdot(const cplx<R> *a, const cplx<R> *b, int n, int64_t batch, double *out, int sm_count,
                         cudaStream_t s);
+// A CSR matrix applied to `batch` states (rows = dim = 2^n): out[b] = A ket[b] (if out) and
+// fout[b * f_stride .. +1] += <bra[b]|A ket[b]> (if fout).
+template <typename R>
+struct CsrArgs {
+    const int64_t *indptr;     // [dim + 1]
+    const int32_t *indices;    // [nnz]
+    const cplx<R> *data;       // [nnz]
+    int64_t dim;
+    const cplx<R> *bra;
+    const cplx<R> *ket;
+    cplx<R> *out;
+    double *fout;
+    int64_t f_stride;
+    int64_t batch;
+};
+template <typename R>
+cudaError_t launch_csr(const CsrArgs<R> &a, int lanes, int sm_count, cudaStream_t s);
 template <typename R>
 cudaError_t launch_copy_or_zero(cplx<R> *dst, const cplx<R> *src, int n, int64_t batch, int64_t src_stride,
                                 cudaStream_t s);

@@ -13,6 +13,7 @@ import numpy as np
 
 from .. import _native as N
 from ..core import gates as G
+from ..core.operators import HowTo
 
 
 def _real(v):
@@ -236,15 +237,29 @@ def lowered(circuit, n_qubits, precision, param_names, grad_names=None, fuse=Tru
 
 
 class NativeHamiltonian:
-    """An ``mqb_hamiltonian`` built from a Hamiltonian's Pauli masks."""
+    """An ``mqb_hamiltonian``: a Hamiltonian's Pauli masks, or its CSR matrix (``HowTo.FRONTEND``;
+    ``hermitian`` takes the conjugate transpose, like ``get_cpp_obj(hermitian=True)``,
+    mindquantum/core/operators/hamiltonian.py:216-245)."""
 
-    def __init__(self, ham, n_qubits, precision):
-        mx, my, mz, ny, cf = ham.pauli_masks()
-        self._arrays = (np.ascontiguousarray(mx), np.ascontiguousarray(my), np.ascontiguousarray(mz),
-                        np.ascontiguousarray(ny), np.ascontiguousarray(cf))
-        ptr = [a.ctypes.data_as(ctypes.c_void_p) for a in self._arrays]
+    def __init__(self, ham, n_qubits, precision, hermitian=False):
         handle = ctypes.c_void_p()
-        N.call('mqb_ham_create', n_qubits, precision, *ptr, len(cf), ctypes.byref(handle))
+        if ham.how_to == HowTo.FRONTEND:
+            m = ham.sparse_matrix
+            if m.shape[0] != (1 << n_qubits):
+                raise RuntimeError("Sparse hamiltonian size not match with quantum state size.")
+            if hermitian:
+                m = m.conjugate().T.tocsr()
+            cdt = np.complex64 if precision == N.MQB_PREC_C64 else np.complex128
+            self._arrays = (np.ascontiguousarray(m.indptr, dtype=np.int64),
+                            np.ascontiguousarray(m.indices, dtype=np.int64), np.ascontiguousarray(m.data, dtype=cdt))
+            ptr = [a.ctypes.data_as(ctypes.c_void_p) for a in self._arrays]
+            N.call('mqb_ham_create_csr', n_qubits, precision, int(m.nnz), *ptr, ctypes.byref(handle))
+        else:
+            mx, my, mz, ny, cf = ham.pauli_masks()
+            self._arrays = (np.ascontiguousarray(mx), np.ascontiguousarray(my), np.ascontiguousarray(mz),
+                            np.ascontiguousarray(ny), np.ascontiguousarray(cf))
+            ptr = [a.ctypes.data_as(ctypes.c_void_p) for a in self._arrays]
+            N.call('mqb_ham_create', n_qubits, precision, *ptr, len(cf), ctypes.byref(handle))
         self.handle = handle
         self.n_qubits = n_qubits
         self.precision = precision
@@ -259,12 +274,15 @@ class NativeHamiltonian:
             self.handle = None
 
 
-def native_ham(ham, n_qubits, precision):
+def native_ham(ham, n_qubits, precision, hermitian=False):
+    """The native Hamiltonian of ``ham`` (cached on it; a sparse matrix's conjugate transpose when
+    ``hermitian``; Pauli Hamiltonians have real coefficients and are their own)."""
+    hermitian = bool(hermitian) and ham.how_to == HowTo.FRONTEND
     cache = getattr(ham, '_mqb_cache', None)
     if cache is None:
         cache = {}
         ham._mqb_cache = cache  # pylint: disable=protected-access
-    key = (n_qubits, precision)
+    key = (n_qubits, precision, hermitian, ham.how_to)
     if key not in cache:
-        cache[key] = NativeHamiltonian(ham, n_qubits, precision)
+        cache[key] = NativeHamiltonian(ham, n_qubits, precision, hermitian)
     return cache[key]

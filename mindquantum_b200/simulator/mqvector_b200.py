@@ -17,7 +17,7 @@ import torch
 from .. import _native as N
 from ..core import gates as G
 from ..core.circuit import Circuit
-from ..core.operators import Hamiltonian
+from ..core.operators import Hamiltonian, HowTo
 from ..core.parameterresolver import ParameterResolver, to_pr
 from ..dtype import complex64, complex128, to_mq_type
 from .backend_base import BackendBase
@@ -291,9 +291,13 @@ class MQVectorB200(BackendBase):
         self._state = out
 
     def _check_ham(self, ham):
-        if ham.n_qubits > self.n_qubits:
-            raise ValueError(f"Hamiltonian qubits is {ham.n_qubits}, not match with simulator qubits number "
-                             f"{self.n_qubits}")
+        """_check_hamiltonian_qubits_number (mindquantum/utils/type_value_check.py:51-63)."""
+        if ham.how_to != HowTo.ORIGIN:
+            if ham.n_qubits != self.n_qubits:
+                raise ValueError(f"Hamiltonian qubits is {ham.n_qubits}, not match with simulator qubits number "
+                                 f"{self.n_qubits}")
+        elif ham.n_qubits > self.n_qubits:
+            raise ValueError(f"Hamiltonian qubits is {ham.n_qubits}, which is bigger than simulator qubits.")
 
     # ------------------------------------------------------------------ expectations
     def get_expectation(self, hamiltonian, circ_right=None, circ_left=None, simulator_left=None, pr=None):
@@ -504,10 +508,11 @@ class MQVectorB200(BackendBase):
             res = np.zeros((B, len(hams), 1 + len(names)), dtype=np.complex128)
             for h_i, ham in enumerate(hams):
                 nh = native_ham(ham, sim.n_qubits, sim.precision)
+                nh_herm = native_ham(ham, sim.n_qubits, sim.precision, hermitian=True)
                 out = torch.zeros((B, 2), dtype=torch.float64, device=sim.device)
                 N.call('mqb_expectation', nh.handle, _ptr(psi_l), _ptr(psi_r), B, _ptr(out), _stream())
-                h_l = torch.empty_like(psi_l)
-                N.call('mqb_apply_hamiltonian', nh.handle, _ptr(psi_l), _ptr(h_l), B, _stream())
+                h_l = torch.empty_like(psi_l)   # H^dag psi_l (RightSizeGrad's herm_hams, gradient.h:199-217)
+                N.call('mqb_apply_hamiltonian', nh_herm.handle, _ptr(psi_l), _ptr(h_l), B, _stream())
                 h_r = torch.empty_like(psi_r)
                 N.call('mqb_apply_hamiltonian', nh.handle, _ptr(psi_r), _ptr(h_r), B, _stream())
                 g = sim._adjoint_with_lambda(circ_right, names, psi0, h_l, params)

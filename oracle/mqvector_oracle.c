@@ -339,6 +339,34 @@ static inline idx_t insert_zero2(idx_t l, int qa, int qb) {
         prob[dim - 1] = 1.0;                                                                                     \
     }                                                                                                            \
                                                                                                                  \
+    /* Csr_Dot_Vec (ccsrc/include/core/sparse/algo.h:160-176): out = A vec, row sums in T. */                 \
+    void orc_csr_dot_vec_##SUF(const int64_t *indptr, const int64_t *indices, const T *data_, idx_t dim,      \
+                               const T *vec_, T *out_) {                                                         \
+        const c##SUF *data = (const c##SUF *)data_, *vec = (const c##SUF *)vec_;                                 \
+        c##SUF *out = (c##SUF *)out_;                                                                            \
+        OMP_FOR for (idx_t i = 0; i < dim; i++) {                                                                \
+            c##SUF sum = mk##SUF(0, 0);                                                                          \
+            for (int64_t j = indptr[i]; j < indptr[i + 1]; j++) sum += data[j] * vec[indices[j]];               \
+            out[i] = sum;                                                                                        \
+        }                                                                                                        \
+    }                                                                                                            \
+                                                                                                                 \
+    /* ExpectationOfCsr (algo.h:178-200): sum_i conj(bra_i) (A ket)_i. */                                      \
+    void orc_expectation_of_csr_##SUF(const int64_t *indptr, const int64_t *indices, const T *data_, idx_t dim, \
+                                      const T *bra_, const T *ket_, double *out) {                              \
+        const c##SUF *data = (const c##SUF *)data_, *bra = (const c##SUF *)bra_, *ket = (const c##SUF *)ket_;   \
+        T acc_re = 0, acc_im = 0;                                                                                \
+        OMP_RED for (idx_t i = 0; i < dim; i++) {                                                                \
+            c##SUF sum = mk##SUF(0, 0);                                                                          \
+            for (int64_t j = indptr[i]; j < indptr[i + 1]; j++) sum += data[j] * ket[indices[j]];               \
+            c##SUF t = conj(bra[i]) * sum;                                                                       \
+            acc_re += creal(t);                                                                                  \
+            acc_im += cimag(t);                                                                                  \
+        }                                                                                                        \
+        out[0] = acc_re;                                                                                         \
+        out[1] = acc_im;                                                                                         \
+    }                                                                                                            \
+                                                                                                                 \
     /* LowerBound: cpu_vector_core_policy.cpp:315-332 (merge of sorted uniforms into the cdf). */              \
     void orc_lower_bound_##SUF(const T *cum, idx_t dim, const T *sampled, idx_t ns, uint32_t *out) {          \
         idx_t s = 0, d = 0;                                                                                      \

@@ -14,7 +14,9 @@ What it restates (reference file:line, paths inside mindquantum-ai/mindquantum):
   * ``GradientHelper::HermitianAdjointGradient`` / ``LeftSizeGrad`` / ``GradRealDouble`` /
     ``GeneratePMap`` and the Jacobi of ``Parameterizable`` (ccsrc/include/simulator/vector/gradient.h:100-197,
     ccsrc/include/ops/basic_gate.h:208-241, ccsrc/lib/math/pr/parameter_resolver.cpp:560-573);
-  * ``GetExpectation`` (vector_state.tpp:712-726), ``ApplyHamiltonian`` (vector_state.tpp:963-974);
+  * ``GetExpectation`` (vector_state.tpp:712-726), ``ApplyHamiltonian`` (vector_state.tpp:963-974),
+    with ``Csr_Dot_Vec`` / ``ExpectationOfCsr`` (ccsrc/include/core/sparse/algo.h:160-200) for
+    Hamiltonians given as sparse matrices;
   * ``GetExpectationWithGradParameterShiftOneMulti`` / ``MultiMulti`` (vector_state.tpp:1033-1305)
     in ``get_expectation_with_grad_parameter_shift``, with the shift table of ``shift_rule``;
   * ``SamplingMeasurementEndingWithoutNoise`` (vector_state.tpp:1326-1373) with the reference's
@@ -86,6 +88,8 @@ def _declare(L):
         getattr(L, f'orc_expect_diff_rps_{suf}').argtypes = [_P, _P, _I, _U64, _U64, _U64, _I, _U64, _D, _P]
         getattr(L, f'orc_cumulative_probs_{suf}').argtypes = [_P, _I, _P]
         getattr(L, f'orc_lower_bound_{suf}').argtypes = [_P, _U64, _P, _U64, _P]
+        getattr(L, f'orc_csr_dot_vec_{suf}').argtypes = [_P, _P, _P, _U64, _P, _P]
+        getattr(L, f'orc_expectation_of_csr_{suf}').argtypes = [_P, _P, _P, _U64, _P, _P, _P]
     L.orc_num_threads.restype = _I
     L.orc_set_num_threads.argtypes = [_I]
 
@@ -181,10 +185,25 @@ def ham_masks(ham):
     return mx, my, mz, ny, cf
 
 
+_FRONTEND = 2   # HowTo.FRONTEND: a user-given sparse matrix (mindquantum/core/operators/hamiltonian.py:26-32)
+
+
+def _csr_arrays(ham, dtype):
+    m = ham.sparse_matrix
+    return (np.ascontiguousarray(m.indptr, dtype=np.int64), np.ascontiguousarray(m.indices, dtype=np.int64),
+            np.ascontiguousarray(m.data, dtype=dtype))
+
+
 def apply_terms(qs, n, ham):
-    """ApplyTerms: returns H|qs> in a fresh buffer (cpu_vector_core_policy.cpp:133-161)."""
+    """ApplyTerms: returns H|qs> in a fresh buffer (cpu_vector_core_policy.cpp:133-161); a sparse
+    matrix Hamiltonian goes through Csr_Dot_Vec instead (VectorState::ApplyHamiltonian,
+    vector_state.tpp:963-974)."""
     L, s = lib(), _suf(qs)
     out = np.zeros_like(qs)
+    if getattr(ham, 'how_to', 0) == _FRONTEND:
+        ip, ix, dt = _csr_arrays(ham, qs.dtype)
+        getattr(L, f'orc_csr_dot_vec_{s}')(_ptr(ip), _ptr(ix), _ptr(dt), 1 << n, _ptr(qs), _ptr(out))
+        return out
     mx, my, mz, ny, cf = ham_masks(ham)
     getattr(L, f'orc_apply_terms_{s}')(_ptr(qs), _ptr(out), n, len(cf), _ptr(mx), _ptr(my), _ptr(mz), _ptr(ny),
                                        _ptr(cf))
@@ -192,8 +211,15 @@ def apply_terms(qs, n, ham):
 
 
 def expectation_of_terms(bra, ket, n, ham):
+    """ExpectationOfTerms (cpu_vector_core_policy.cpp:212-261), or ExpectationOfCsr for a sparse
+    matrix Hamiltonian (vector_state.tpp:712-726)."""
     L, s = lib(), _suf(bra)
     out = np.zeros(2)
+    if getattr(ham, 'how_to', 0) == _FRONTEND:
+        ip, ix, dt = _csr_arrays(ham, bra.dtype)
+        getattr(L, f'orc_expectation_of_csr_{s}')(_ptr(ip), _ptr(ix), _ptr(dt), 1 << n, _ptr(bra), _ptr(ket),
+                                                  _ptr(out))
+        return complex(out[0], out[1])
     mx, my, mz, ny, cf = ham_masks(ham)
     getattr(L, f'orc_expectation_of_terms_{s}')(_ptr(bra), _ptr(ket), n, len(cf), _ptr(mx), _ptr(my), _ptr(mz),
                                                 _ptr(ny), _ptr(cf), _ptr(out))
