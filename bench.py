@@ -15,6 +15,7 @@ reported.  ``--impl reference`` times the reference algorithm's CPU implementati
 port of the mqvector CPU kernels) on the host cores, one bounded sample per step.
 """
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -410,6 +411,77 @@ def run_workload(args, rank, local_rank):
         io = (pr.nbytes, (1 + len(names)) * 16)
         cfg = {"workload": f"QAOA MaxCut {n}q, p={p}, 3-regular graph with {len(edges)} edges, H = sum Z_i Z_j",
                "n_qubits": n, "batch": 1}
+    elif args.workload == 'csr':
+        import scipy.sparse as sp  # noqa: F401
+        from mindquantum_b200.core.operators import Hamiltonian
+        from mindquantum_b200.simulator.lowering import native_ham
+
+        n, layers, B = 22, 6, 8
+        circ, ham_p, params_np = build_workload(n, layers, B, seed=rank)
+        names = circ.params_name
+        ham = Hamiltonian(W.pauli_csr(ham_p, n, np.complex64))
+        params = torch.as_tensor(params_np, device=dev)
+        sim = MQVectorB200('mqvector_b200', n, dtype=complex64, device=dev)
+        units = B
+
+        def step():
+            return sim.expectation_with_grad_tensor([ham], circ, params, names)
+
+        def e2e_step():
+            return sim.get_expectation_with_grad(ham, circ)(params_np)
+
+        io = (params_np.nbytes, B * (1 + len(names)) * 16)
+        nnz = ham.sparse_matrix.nnz
+        cfg = {"workload": f"HEA {n}q x {layers} layers, {len(names)} params, the ZZ+X Hamiltonian as a CSR matrix "
+                           f"({nnz} entries), batched adjoint gradient", "n_qubits": n, "batch": B, "nnz": int(nnz)}
+        # the CSR kernel alone: <psi_b|A|psi_b> of B resident states (matrix and states larger than L2)
+        nh = native_ham(ham, n, sim.precision)
+        states = torch.randn((B, 1 << n), dtype=torch.complex64, device=dev)
+        out = torch.zeros((B, 2), dtype=torch.float64, device=dev)
+        call = lambda: N.call('mqb_expectation', nh.handle, ctypes.c_void_p(states.data_ptr()),  # noqa: E731
+                              ctypes.c_void_p(states.data_ptr()), B, ctypes.c_void_p(out.data_ptr()),
+                              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        for _ in range(3):
+            call()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10
+        c0.record()
+        for _ in range(reps):
+            call()
+        c1.record()
+        torch.cuda.synchronize()
+        csr_ms = c0.elapsed_time(c1) / reps
+        S = (1 << n) * 8
+        passes = (B + 3) // 4
+        alg = passes * (nnz * 12 + 8 * ((1 << n) + 1)) + B * 2 * S
+        peak, peak_kind = _peaks()
+        extras["csr_kernel"] = {"ms_per_call": csr_ms, "alg_bytes_per_call": int(alg),
+                                "achieved_gbs": alg / (csr_ms / 1e3) / 1e9, "peak_gbs": peak, "peak_source": peak_kind,
+                                "frac": alg / (csr_ms / 1e3) / 1e9 / peak, "states": B,
+                                "bytes_model": "passes*(nnz*(4+8) + 8*(dim+1)) + B*2*S, passes = ceil(B/4)"}
+        del states
+    elif args.workload == 'pshift':
+        n, layers = 16, 2
+        circ, ham, params_np = build_workload(n, layers, 1, seed=rank)
+        names = circ.params_name
+        sim_api = None
+        from mindquantum_b200.simulator import Simulator
+
+        sim_api = Simulator('mqvector_b200', n, dtype=complex64)
+        ops = sim_api.get_expectation_with_grad(ham, circ, pr_shift=True)
+        units = 1
+
+        def step():
+            return ops(params_np[0])
+
+        e2e_step = step
+        io = (params_np.nbytes, (1 + len(names)) * 16)
+        cfg = {"workload": f"parameter-shift gradient, HEA {n}q x {layers} layers, {len(names)} params "
+                           f"({2 * len(names) + 1} shifted circuits as one batch)", "n_qubits": n, "batch": 1}
+        adj = sim_api.get_expectation_with_grad(ham, circ)
+        f_a, g_a = adj(params_np[0])
+        f_s, g_s = ops(params_np[0])
+        extras["grad_err_vs_adjoint"] = float(np.abs(g_s - g_a).max())
     else:
         from mindquantum_b200.simulator.batch import CircuitBatch
 
@@ -482,7 +554,7 @@ def main():
     ap.add_argument('--skip-extras', action='store_true')
     ap.add_argument('--skip-plain', action='store_true')
     ap.add_argument('--skip-cpu', action='store_true')
-    ap.add_argument('--workload', default='hea', choices=['hea', 'qnn', 'qaoa', 'uneven'],
+    ap.add_argument('--workload', default='hea', choices=['hea', 'qnn', 'qaoa', 'uneven', 'csr', 'pshift'],
                     help='hea: the headline 26-qubit HEA gradient; the others are the remaining workload families')
     args = ap.parse_args()
     rank = int(os.environ.get('RANK', 0))

@@ -129,3 +129,33 @@ def qaoa_maxcut(n, p, seed=0):
     for (i, j) in edges:
         op += QubitOperator(f'Z{i} Z{j}')
     return circ, Hamiltonian(op), params, edges
+
+
+def pauli_csr(ham, n, dtype=np.complex128):
+    """The 2^n x 2^n matrix of a Pauli Hamiltonian as ``scipy.sparse.csr_matrix``, built per flip
+    mask without a dense matrix: P|i> = i^{n_y} (-1)^{popcount(i & (m_y | m_z))} |i ^ m_flip>, so
+    row r has one entry per distinct flip mask f, at column r ^ f."""
+    import scipy.sparse as sp
+
+    mx, my, mz, ny, cf = ham.pauli_masks()
+    dim = 1 << n
+    cols_of, vals_of = [], []
+    rows = np.arange(dim, dtype=np.int64)
+    flips = sorted({int(a) | int(b) for a, b in zip(mx, my)})
+    for f in flips:
+        col = rows ^ f
+        val = np.zeros(dim, dtype=np.complex128)
+        for t in range(len(cf)):
+            if (int(mx[t]) | int(my[t])) != f:
+                continue
+            sign = 1 - 2 * (np.bitwise_count(col & np.int64(int(my[t]) | int(mz[t]))) & 1).astype(np.int64)
+            val += cf[t] * (1j ** int(ny[t])) * sign
+        cols_of.append(col)
+        vals_of.append(val)
+    cols = np.stack(cols_of)            # [flips][dim]
+    vals = np.stack(vals_of)
+    order = np.argsort(cols, axis=0)
+    cols = np.take_along_axis(cols, order, axis=0).T.reshape(-1)
+    vals = np.take_along_axis(vals, order, axis=0).T.reshape(-1).astype(dtype)
+    indptr = np.arange(0, dim * len(flips) + 1, len(flips), dtype=np.int64)
+    return sp.csr_matrix((vals, cols, indptr), shape=(dim, dim))

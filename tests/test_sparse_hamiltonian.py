@@ -59,6 +59,14 @@ def test_oracle_csr_equals_pauli_kernels():
     assert abs(O.expectation_of_terms(b, a, n, hm) - np.vdot(b, m @ a)) < 1e-12
 
 
+def test_pauli_csr_builder_matches_dense_matrix():
+    for n, seed in ((4, 1), (7, 2)):
+        h = W.random_pauli_hamiltonian(n, 15, np.random.default_rng(seed))
+        m = W.pauli_csr(h, n)
+        assert np.array_equal(m.indptr, np.sort(m.indptr))
+        assert np.allclose(m.toarray(), h.hamiltonian.matrix(n), atol=1e-14)
+
+
 def test_hamiltonian_modes():
     qo = QubitOperator('X0 Y2', 0.5) + QubitOperator('Z1')
     h = Hamiltonian(qo)
