@@ -124,12 +124,16 @@ def _peaks():
 
 
 def _traffic_from_profiles():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, 'profiles', 'fused_backward_26q_c64.json')
+    """DRAM bytes per state byte of one adjoint launch, from the committed ncu summary (a smaller
+    case of the same kernel; traffic grows with the state bytes a launch processes)."""
+    import re
+
+    path = os.path.join(ROOT, 'profiles', 'mqb_adj_pass_hea24_c64.md')
     try:
         with open(path, encoding='utf8') as f:
-            return json.load(f)
-    except (OSError, ValueError):
+            m = re.search(r'^dram_bytes_per_state_byte:\s*([0-9.]+)', f.read(), re.M)
+        return float(m.group(1)) if m else None
+    except OSError:
         return None
 
 
@@ -280,7 +284,8 @@ def run_b200(args, rank, world, local_rank):
     traffic = _traffic_from_profiles()
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
-                "traffic": (traffic or {}).get('dram_bytes_per_launch'),
+                "traffic": (traffic * S if (traffic and dom == 'fused_backward') else None),
+                "traffic_source": "profiles/mqb_adj_pass_hea24_c64.md: dram bytes per state byte x S*B",
                 "alg_bytes_per_launch": alg.get(dom, 0) / max(1, kt.launches[dom] // args.steps),
                 "avg_launch_ms": kt.ms[dom] / max(1, kt.launches[dom]), "peak_source": peak_kind,
                 "step_hbm_gbs": total_alg / (ms / 1e3) / 1e9 if world == 1 else None,

@@ -429,7 +429,7 @@ class MQVectorB200(BackendBase):
     def _batched_states(self, circuit, names, init, params):
         """[batch][2^n]: ``circuit`` applied to ``init`` for every parameter row."""
         B = params.shape[0]
-        st = init.reshape(1, -1).expand(B, -1).contiguous()
+        st = init.reshape(1, -1).repeat(B, 1)   # always a copy: the circuit is applied in place
         prog = lowered(circuit, self.n_qubits, self.precision, names, None, self.fuse, jit=self.jit)
         if prog.n_gates == 0:
             return st

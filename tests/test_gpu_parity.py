@@ -374,6 +374,8 @@ def test_non_hermitian_gradient_against_dense_matrices(dtype):
     names = ops.ansatz_params_name
     p = rng.uniform(0, 2 * np.pi, len(names))
     f, g = ops(p)
+    # the operator leaves both simulators' states as they were
+    assert np.allclose(sim.get_qs(), psi0, atol=1e-6) and np.allclose(sim_left.get_qs(), phi0, atol=1e-6)
     pr = dict(zip(names, p))
     tol = 1e-10 if dtype == complex128 else 2e-5
     assert abs(f[0, 0] - f_of(pr)) < tol

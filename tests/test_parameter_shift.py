@@ -169,6 +169,7 @@ def test_parameter_shift_matches_oracle(dtype, make):
     ans = rng.uniform(0, 2 * np.pi, len(circ.ansatz_params_name))
     sim = Simulator('mqvector_b200', 3, dtype=dtype)
     f, ge, ga = sim.get_expectation_with_grad(HAMS, circ, pr_shift=True)(enc, ans)
+    assert abs(sim.get_qs()[0] - 1) < 1e-6   # the simulator's own state is untouched
     ref = _oracle_shift(circ, HAMS, enc, ans, circ.encoder_params_name, circ.ansatz_params_name)
     ne = len(circ.encoder_params_name)
     ftol, gtol = (1e-9, 1e-9) if dtype == complex128 else (1e-5, 2e-3)
