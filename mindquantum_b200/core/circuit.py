@@ -158,7 +158,7 @@ class Circuit(list):
 
     @property
     def is_noise_circuit(self):
-        return False
+        return any(isinstance(g, G.NoiseGate) for g in self)
 
     @property
     def is_measure_end(self):

@@ -692,6 +692,159 @@ class BarrierGate(BasicGate):
         self.show = show
 
 
+class NoiseGate(BasicGate):
+    """A quantum channel, simulated as a stochastic trajectory (VectorState::ApplyChannel,
+    vector_state.tpp:465-709; classes of mindquantum/core/gates/channel.py)."""
+
+    def hermitian(self):
+        new = copy.deepcopy(self)
+        new.hermitianed = not new.hermitianed
+        return new
+
+
+def _check_real(name, v):
+    if isinstance(v, bool) or not isinstance(v, (int, float)):
+        raise TypeError(f"Unsupported type for {name}, get {type(v)}.")
+
+
+class PauliChannel(NoiseGate):
+    """X, Y, Z with probabilities px, py, pz, identity otherwise (channel.py:125-230)."""
+
+    def __init__(self, px: float, py: float, pz: float, name: str = 'PC'):
+        super().__init__(name, 1)
+        for k, v in (('px', px), ('py', py), ('pz', pz)):
+            _check_real(k, v)
+        if min(px, py, pz) < 0.0:
+            raise ValueError("Probability cannot be negative value.")
+        if not 0 <= px + py + pz <= 1:
+            raise ValueError("Required total probability P = px + py + pz ∈ [0,1].")
+        self.px, self.py, self.pz = float(px), float(py), float(pz)
+
+    def hermitian(self):
+        return copy.deepcopy(self)
+
+    def cumulative_probs(self):
+        """[0, px, px + py, px + py + pz, 1] (PauliChannel, ccsrc/include/ops/basic_gate.h:341-352)."""
+        probs = [self.px, self.py, self.pz, 1 - self.px - self.py - self.pz]
+        out, acc = [0.0], 0.0
+        for p in probs:
+            acc += p
+            out.append(acc)
+        return out
+
+
+class BitFlipChannel(PauliChannel):
+    def __init__(self, p: float):
+        super().__init__(p, 0, 0, 'BFC')
+
+
+class PhaseFlipChannel(PauliChannel):
+    def __init__(self, p: float):
+        super().__init__(0, 0, p, 'PFC')
+
+
+class BitPhaseFlipChannel(PauliChannel):
+    def __init__(self, p: float):
+        super().__init__(0, p, 0, 'BPFC')
+
+
+class GroupedPauliChannel(NoiseGate):
+    """One independent Pauli channel per object qubit, rows of ``probs`` = (px, py, pz) (channel.py:32-123)."""
+
+    def __init__(self, probs):
+        if not isinstance(probs, np.ndarray):
+            raise TypeError(f"probs requires a numpy.ndarray, but get {type(probs)}")
+        if not np.issubdtype(probs.dtype, np.floating):
+            raise TypeError(f"probs requires a real number type, but get {probs.dtype}")
+        if np.any(probs < 0.0):
+            raise ValueError("probs cannot be negative value.")
+        if probs.ndim != 2:
+            raise ValueError(f"probs requires a two dimension array, but get dimension with {probs.shape}")
+        if probs.shape[1] != 3:
+            raise ValueError(f"The second dimension of probs should be two, but get {probs.shape[1]}")
+        wrong = np.where(probs.sum(axis=1) > 1)[0]
+        if wrong.shape[0]:
+            raise ValueError(f"Wrong probs for {wrong[0]}-pauli channel: {probs[wrong[0]]}")
+        super().__init__('GPC', probs.shape[0])
+        self.probs = probs
+
+    def hermitian(self):
+        return copy.deepcopy(self)
+
+
+class DepolarizingChannel(NoiseGate):
+    """Depolarizing channel on n qubits with parameter p (channel.py:425-528)."""
+
+    def __init__(self, p: float, n_qubits: int = 1):
+        super().__init__('DC', n_qubits)
+        _check_real('argument p', p)
+        if not 0 <= p <= 4**n_qubits / (4**n_qubits - 1):
+            raise ValueError(f"Required argument p ∈ [0, {4**n_qubits}/{4**n_qubits - 1}], but get p = {p}.")
+        self.p = p
+
+    def hermitian(self):
+        return copy.deepcopy(self)
+
+
+class AmplitudeDampingChannel(NoiseGate):
+    """Amplitude damping with coefficient gamma (channel.py:530-606)."""
+
+    def __init__(self, gamma: float):
+        super().__init__('ADC', 1)
+        _check_real('gamma', gamma)
+        if not 0 <= gamma <= 1:
+            raise ValueError("Required damping coefficient gamma ∈ [0,1].")
+        self.gamma = gamma
+
+
+class PhaseDampingChannel(NoiseGate):
+    """Phase damping with coefficient gamma (channel.py:608-684)."""
+
+    def __init__(self, gamma: float):
+        super().__init__('PDC', 1)
+        _check_real('gamma', gamma)
+        if not 0 <= gamma <= 1:
+            raise ValueError("Required damping coefficient gamma ∈ [0,1].")
+        self.gamma = gamma
+
+
+class KrausChannel(NoiseGate):
+    """A single-qubit channel given by its Kraus operators (channel.py:686-766)."""
+
+    def __init__(self, name: str, kraus_op):
+        kraus_op = np.asarray(kraus_op)
+        if not np.issubdtype(kraus_op.dtype, np.number):
+            raise TypeError(f"{name} requires a numerical array, but get {kraus_op.dtype}")
+        for mat in kraus_op:
+            if mat.ndim != 2:
+                raise ValueError(f"matrix_value require shape of 2, but get shape of {mat.shape}")
+            if mat.shape[0] != mat.shape[1]:
+                raise ValueError(f"matrix_value need a square matrix, but get shape {mat.shape}")
+            if mat.shape[0] != 2:
+                raise ValueError(f"Dimension of matrix_value need should be 2, but get {mat.shape[0]}")
+        total = sum(np.conj(m).T @ m for m in kraus_op.astype(np.complex128))
+        if not np.allclose(total, np.eye(2), atol=1e-6):
+            raise ValueError(f"kraus_op need to satisfy the completeness condition, but get {total}")
+        super().__init__(name, 1)
+        self.kraus_op = kraus_op
+
+
+class ThermalRelaxationChannel(NoiseGate):
+    """Thermal relaxation with times T1, T2 and the gate time (channel.py:768-871)."""
+
+    def __init__(self, t1: float, t2: float, gate_time: float):
+        super().__init__('TRC', 1)
+        for k, v in (('t1', t1), ('t2', t2), ('gate_time', gate_time)):
+            _check_real(k, v)
+        if t1 <= 0 or t2 <= 0:
+            raise ValueError(f"T1 and T2 must be positive, but get T1={t1}, T2={t2}")
+        if gate_time < 0:
+            raise ValueError(f"gate time cannot be negative, but get {gate_time}")
+        if t2 >= 2 * t1:
+            raise ValueError("(T2 >= 2 * T1) is invalid case for thermal relaxation channel.")
+        self.t1, self.t2, self.gate_time = t1, t2, gate_time
+
+
 # Singletons with the reference's names
 X = XGate()
 Y = YGate()

@@ -25,7 +25,7 @@ from .lowering import lowered, native_ham
 from .measure_result import MeasureResult
 from .parameter_shift import ShiftPlan
 from .rng import Mt19937Uniform
-from .utils import GradOpsWrapper
+from .utils import GradOpsWrapper, _thread_balance
 
 
 def _stream():
@@ -206,24 +206,179 @@ class MQVectorB200(BackendBase):
             self._apply_segment(state, Circuit([G.X.on(q)]), ParameterResolver())
         return int(collapse_to_one)
 
+    @staticmethod
+    def _split(circuit):
+        """The circuit as unitary segments, measurements and channels (cached on the circuit)."""
+        key = len(circuit)
+        cached = getattr(circuit, '_mqb_split', None)
+        if cached is not None and cached[0] == key:
+            return cached[1]
+        parts, segment = [], Circuit()
+        for g in circuit:
+            if isinstance(g, (G.Measure, G.NoiseGate)):
+                if len(segment):
+                    parts.append(segment)
+                    segment = Circuit()
+                parts.append(g)
+            elif not isinstance(g, G.BarrierGate):
+                segment.append(g)
+        if len(segment):
+            parts.append(segment)
+        try:
+            circuit._mqb_split = (key, parts)  # pylint: disable=protected-access
+        except AttributeError:
+            pass
+        return parts
+
     def _run(self, state, circuit, pr, rng):
-        if not circuit.has_measure_gate:
+        """Apply ``circuit`` in place; measurements and channels draw from ``rng``
+        (VectorState::ApplyCircuit, vector_state.tpp:949-960)."""
+        if not circuit.has_measure_gate and not circuit.is_noise_circuit:
             if len(circuit):
                 self._apply_segment(state, circuit, pr)
             return {}
         results = {}
-        segment = Circuit()
-        for g in circuit:
-            if isinstance(g, G.Measure):
-                if len(segment):
-                    self._apply_segment(state, segment, pr)
-                    segment = Circuit()
-                results[g.key] = self._measure(state, g, rng)
-            elif not isinstance(g, G.BarrierGate):
-                segment.append(g)
-        if len(segment):
-            self._apply_segment(state, segment, pr)
+        for part in self._split(circuit):
+            if isinstance(part, G.Measure):
+                results[part.key] = self._measure(state, part, rng)
+            elif isinstance(part, G.NoiseGate):
+                self._channel(state, part, rng)
+            else:
+                self._apply_segment(state, part, pr)
         return results
+
+    # ------------------------------------------------------------------ noise channels
+    def _matrix_on(self, state, m, q, ctrls=()):
+        """A constant 2x2 matrix (unitary or not) on qubit q under ``ctrls``, in place."""
+        self._apply_segment(state, Circuit([G.UnivMathGate('K', np.asarray(m, dtype=complex)).on(q, list(ctrls))]),
+                            ParameterResolver())
+
+    def _pauli_on(self, state, which, q, ctrls=()):
+        gate = (G.X, G.Y, G.Z)[which]
+        self._apply_segment(state, Circuit([gate.on(q, list(ctrls))]), ParameterResolver())
+
+    def _one_probability(self, state, q):
+        out = torch.zeros(1, dtype=torch.float64, device=self.device)
+        N.call('mqb_qubit_one_probability', self.n_qubits, self.precision, _ptr(state), q, _ptr(out), _stream())
+        return float(out.item())
+
+    @staticmethod
+    def _pauli_index(cum, r):
+        """lower_bound over [0, px, px+py, px+py+pz, 1]: 0 = X, 1 = Y, 2 = Z, 3 = identity."""
+        import bisect
+
+        it = bisect.bisect_left(cum, r)
+        return it - 1 if it > 0 else 0
+
+    def _channel(self, state, g, rng):
+        """One trajectory step of a channel (VectorState::ApplyChannel, vector_state.tpp:465-709).
+
+        The draws come from ``rng`` in the reference's order; probabilities that depend on the
+        state (damping, Kraus, thermal relaxation) are reduced on the device in FP64."""
+        objs, ctrls = list(g.obj_qubits), list(g.ctrl_qubits)
+        draw = rng.draw
+        if isinstance(g, G.PauliChannel):
+            k = self._pauli_index(g.cumulative_probs(), draw())
+            if k < 3:
+                self._pauli_on(state, k, objs[0], ctrls)
+        elif isinstance(g, G.GroupedPauliChannel):
+            picks = []
+            for q, row in zip(objs, g.probs):
+                px, py, pz = (float(v) for v in row)
+                k = self._pauli_index([0.0, px, px + py, px + py + pz, px + py + pz + (1 - px - py - pz)], draw())
+                if k < 3:
+                    picks.append((k, q))
+            for k, q in picks:    # ApplyPauliString: no controls
+                self._pauli_on(state, k, q)
+        elif isinstance(g, G.DepolarizingChannel):
+            idx, p = 0, float(g.p)
+            while idx < len(objs):
+                if draw() < p * 3.0 / 4.0:
+                    p_i = draw()
+                    self._pauli_on(state, 0 if p_i < 1.0 / 3.0 else (1 if p_i < 2.0 / 3.0 else 2), objs[idx], ctrls)
+                    for q in objs[idx + 1:]:
+                        p_i = draw()
+                        if p_i < 0.75:
+                            self._pauli_on(state, 0 if p_i < 0.25 else (1 if p_i < 0.5 else 2), q, ctrls)
+                    break
+                if not 4 > 3 * p:
+                    break
+                idx, p = idx + 1, p / (4 - 3 * p)
+        elif isinstance(g, G.KrausChannel):
+            total = 1.0
+            for m in np.asarray(g.kraus_op, dtype=np.complex128):
+                if abs(m[0, 1]) < 1e-6 and abs(m[1, 0]) < 1e-6 and abs(m[0, 0] - m[1, 1]) < 1e-6:
+                    prob = float((m[0, 0] * np.conj(m[0, 0])).real)
+                    rel = prob / total
+                    total -= prob
+                    if draw() < rel:
+                        if m[0, 0].imag >= 1e-6:   # identity with a phase
+                            v = m[0, 0] / math.sqrt(prob)
+                            self._matrix_on(state, [[v, 0], [0, v]], 0)
+                        return
+                else:
+                    tmp = state.clone()
+                    self._matrix_on(tmp, m, objs[0], ctrls)
+                    out = torch.zeros(2, dtype=torch.float64, device=self.device)
+                    N.call('mqb_vdot', self.n_qubits, self.precision, _ptr(tmp), _ptr(tmp), 1, _ptr(out), _stream())
+                    prob = float(out[0].item())
+                    rel = prob / total
+                    total -= prob
+                    if draw() < rel:
+                        v = 1 / math.sqrt(prob)
+                        self._matrix_on(tmp, [[v, 0], [0, v]], 0)
+                        state.copy_(tmp)
+                        return
+        elif isinstance(g, (G.AmplitudeDampingChannel, G.PhaseDampingChannel)):
+            renorm = self._one_probability(state, objs[0])
+            if renorm < 1e-6:
+                return
+            gamma = float(g.gamma)
+            prob = gamma * renorm
+            if draw() <= prob:
+                if isinstance(g, G.AmplitudeDampingChannel):
+                    self._matrix_on(state, [[0, 1 / math.sqrt(renorm)], [0, 0]], objs[0], ctrls)
+                else:
+                    self._matrix_on(state, [[0, 0], [0, 1 / math.sqrt(renorm)]], objs[0], ctrls)
+            else:
+                a, b = 1 / math.sqrt(1 - prob), math.sqrt(1 - gamma) / math.sqrt(1 - prob)
+                self._matrix_on(state, [[a, 0], [0, b]], objs[0], ctrls)
+        elif isinstance(g, G.ThermalRelaxationChannel):
+            t1, t2, tg = float(g.t1), float(g.t2), float(g.gate_time)
+            e1, e2 = math.exp(-tg / t1), math.exp(-tg / t2)
+            p_reset = 1 - e1
+            q = objs[0]
+            if t1 >= t2:
+                pz = e1 * (1 - e2 / e1) / 2
+                r = draw()
+                if r < 1 - pz - p_reset:
+                    return
+                if r < 1 - p_reset:
+                    self._pauli_on(state, 2, q, ctrls)
+                else:
+                    zero = 1.0 - self._one_probability(state, q)
+                    if draw() < zero:
+                        self._matrix_on(state, [[1 / math.sqrt(zero), 0], [0, 0]], q, ctrls)
+                    else:
+                        self._matrix_on(state, [[0, 1 / math.sqrt(1 - zero)], [0, 0]], q, ctrls)
+            elif 2 * t1 > t2:
+                r = draw()
+                root = math.sqrt(p_reset * p_reset + 4 * e2 * e2)
+                ev0, ev1 = (2 - p_reset + root) / 2, (2 - p_reset - root) / 2
+                vec0, vec1 = (ev0 - e1) / e2, (ev1 - e1) / e2
+                zero = 1.0 - self._one_probability(state, q)
+                one = 1 - zero
+                c0 = vec0 * vec0 * zero + one
+                p0 = c0 * ev0 / (vec0 * vec0 + 1)
+                if r < p0:
+                    self._matrix_on(state, [[vec0 / math.sqrt(c0), 0], [0, 1 / math.sqrt(c0)]], q, ctrls)
+                elif r < 1 - p_reset * one:
+                    c1 = vec1 * vec1 * zero + one
+                    self._matrix_on(state, [[vec1 / math.sqrt(c1), 0], [0, 1 / math.sqrt(c1)]], q, ctrls)
+                else:
+                    self._matrix_on(state, [[0, 1 / math.sqrt(one)], [0, 0]], q, ctrls)
+        else:
+            raise ValueError(f"{g.name} is not a noise channel.")
 
     def _check_pr(self, circuit, pr):
         if circuit.params_name:
@@ -300,6 +455,13 @@ class MQVectorB200(BackendBase):
             raise ValueError(f"Hamiltonian qubits is {ham.n_qubits}, which is bigger than simulator qubits.")
 
     # ------------------------------------------------------------------ expectations
+    def _sub_seed(self, sim):
+        """static_cast<unsigned>(static_cast<calc_type>(rng_()) * (1 << 20)) on ``sim``'s stream."""
+        d = sim._rng.draw()  # pylint: disable=protected-access
+        if self.precision == N.MQB_PREC_C64:
+            return int(np.float32(np.float32(d) * np.float32(1 << 20)))
+        return int(d * (1 << 20))
+
     def get_expectation(self, hamiltonian, circ_right=None, circ_left=None, simulator_left=None, pr=None):
         """<psi| circ_left^dag H circ_right |psi> (GetExpectation, vector_state.tpp:712-768)."""
         if not isinstance(hamiltonian, Hamiltonian):
@@ -307,18 +469,24 @@ class MQVectorB200(BackendBase):
         self._check_ham(hamiltonian)
         circ_right = Circuit() if circ_right is None else circ_right
         pr = ParameterResolver() if pr is None else to_pr(pr, circ_right.params_name)
-        ket = self.state.clone()
-        self._run(ket, circ_right, pr, Mt19937Uniform(self.seed + 1))
+        # sub-streams as the reference seeds its copies: int(float(draw) * 2^20), the bra's first
+        # (from simulator_left's stream when there is one), vector_state.tpp:712-768
         if circ_left is None and simulator_left is None:
+            ket = self.state.clone()
+            self._run(ket, circ_right, pr, Mt19937Uniform(self._sub_seed(self)))
             bra = ket
         else:
-            src = self if simulator_left is None else simulator_left
+            src = self if simulator_left is None else getattr(simulator_left, 'backend', simulator_left)
             if isinstance(src, BackendBase) and not isinstance(src, MQVectorB200):
                 raise TypeError("simulator_left should be a mqvector_b200 simulator")
             if src.n_qubits != self.n_qubits or src.dtype != self.dtype:
                 raise ValueError("simulator_left should have the same qubits and dtype")
+            bra_seed = self._sub_seed(src)
+            ket_seed = self._sub_seed(self)
+            ket = self.state.clone()
+            self._run(ket, circ_right, pr, Mt19937Uniform(ket_seed))
             bra = src.state.clone()
-            self._run(bra, circ_right if circ_left is None else circ_left, pr, Mt19937Uniform(self.seed + 2))
+            self._run(bra, circ_right if circ_left is None else circ_left, pr, Mt19937Uniform(bra_seed))
         h = native_ham(hamiltonian, self.n_qubits, self.precision)
         out = torch.zeros(2, dtype=torch.float64, device=self.device)
         N.call('mqb_expectation', h.handle, _ptr(bra), _ptr(ket), 1, _ptr(out), _stream())
@@ -387,7 +555,14 @@ class MQVectorB200(BackendBase):
             self._check_ham(h)
         if not isinstance(circ_right, Circuit):
             raise TypeError(f"circ_right requires a Circuit, but get {type(circ_right)}")
+        if circ_right.is_noise_circuit:
+            if circ_left is not None or simulator_left is not None:
+                raise ValueError("noise circuit use parameter shift rule to get grad, which not support circ_left "
+                                 "and simulator_left.")
+            pr_shift = True    # mqsim.py:281-287
         if circ_left is not None or simulator_left is not None:
+            if circ_left is not None and circ_left.is_noise_circuit:
+                raise ValueError("noise left circuit not support yet.")
             # the reference takes the non-Hermitian branch before looking at pr_shift (mqsim.py:384-401)
             return self._non_hermitian_grad_ops(hams, circ_right, circ_left, simulator_left, parallel_worker)
         if pr_shift:
@@ -552,6 +727,54 @@ class MQVectorB200(BackendBase):
         o = out.cpu().numpy()
         return (o[..., 0] + 1j * o[..., 1]).T
 
+    def _noisy_shift(self, plan, P, hams, n_thread):
+        """Parameter shift over stochastic channels, one trajectory per evaluation, in the
+        reference's order of random draws (vector_state.tpp:1033-1230): every evaluation runs on a
+        copy of the state re-seeded with int(draw * 10000) from this simulator's stream, every
+        Hamiltonian copy consumes one more draw, Hamiltonians go in groups of ``n_thread`` and the
+        Hamiltonian loop sits inside the gate loop."""
+        rows = plan.rows(P)
+        R, E = plan.rows_per_sample, plan.n_shifts
+        nhs = [native_ham(h, self.n_qubits, self.precision) for h in hams]
+        n_prs, n_h = P.shape[0], len(hams)
+        f = np.zeros((n_prs, n_h), dtype=np.complex128)
+        g = np.zeros((n_prs, n_h, plan.J.shape[1]), dtype=np.complex128)
+        out = torch.zeros(2, dtype=torch.float64, device=self.device)
+        by_gate = {}
+        for e, gi in enumerate(plan.gate_of):
+            by_gate.setdefault(gi, []).append(e)
+
+        def trajectory(row):
+            st = self.state.clone()
+            pr = ParameterResolver(dict(zip(plan.slot_names, (float(v) for v in row))))
+            self._run(st, plan.circuit, pr, Mt19937Uniform(int(self._rng.draw() * 10000)))
+            return st
+
+        def expect(st, j):
+            N.call('mqb_expectation', nhs[j].handle, _ptr(st), _ptr(st), 1, _ptr(out), _stream())
+            o = out.cpu().numpy()
+            return complex(o[0], o[1])
+
+        for s in range(n_prs):
+            base = trajectory(rows[s * R])
+            for start in range(0, n_h, n_thread):
+                group = range(start, min(start + n_thread, n_h))
+                self._rng.draw()
+                for j in group:
+                    self._rng.draw()
+                    f[s, j] = expect(base, j)
+                for gi in sorted(by_gate):
+                    for j in group:
+                        for e in by_gate[gi]:
+                            st = trajectory(rows[s * R + 1 + e])
+                            self._rng.draw()
+                            f_minus = expect(st, j)
+                            st = trajectory(rows[s * R + 1 + E + e])
+                            self._rng.draw()
+                            f_plus = expect(st, j)
+                            g[s, j] += plan.coeff[e] * (f_plus - f_minus).real * plan.J[e]
+        return f, g
+
     def _parameter_shift_grad_ops(self, hams, circ, parallel_worker):
         """Gradients by the parameter-shift rule (mqsim.py:401-411;
         ``GetExpectationWithGradParameterShiftMultiMulti``, vector_state.tpp:1033-1305), every
@@ -568,11 +791,20 @@ class MQVectorB200(BackendBase):
         plan = ShiftPlan(circ, enc_names + ans_names)
         sim = self
 
+        noisy = circ.is_noise_circuit
+
         def grad_ops(*inputs_):
             enc, ans = _split_inputs(version, enc_names, ans_names, inputs_)
             P = np.concatenate([enc, np.broadcast_to(ans, (enc.shape[0], ans.size))], axis=1)
-            F = sim._row_expectations(plan.circuit, plan.slot_names, sim.state, plan.rows(P), hams)
-            f, g = plan.combine(F)
+            n_thread = max(1, min(_thread_balance(P.shape[0], len(hams), parallel_worker)[1], 15, len(hams)))
+            if noisy:
+                f, g = sim._noisy_shift(plan, P, hams, n_thread)
+            else:
+                F = sim._row_expectations(plan.circuit, plan.slot_names, sim.state, plan.rows(P), hams)
+                f, g = plan.combine(F)
+                # the reference seeds every evaluation from the simulator's stream: advance it alike
+                n_groups = -(-len(hams) // n_thread)
+                sim._rng.draw(P.shape[0] * (1 + n_groups + len(hams) * (1 + 4 * plan.n_shifts)))
             if version == 'both':
                 return f, g[:, :, :len(enc_names)], g[:, :, len(enc_names):]
             return f, g
@@ -600,7 +832,7 @@ class MQVectorB200(BackendBase):
         key_map = res.keys_map
         rng = Mt19937Uniform(seed)
         samples = np.zeros((shots, len(key_map)), dtype=np.int64)
-        if circuit.is_measure_end:
+        if circuit.is_measure_end and not circuit.is_noise_circuit:
             sub = int(rng.draw(low=1.0, high=float(1 << 20)))
             sim_rng = Mt19937Uniform(sub)
             m_gates = [g for g in circuit if isinstance(g, G.Measure)]

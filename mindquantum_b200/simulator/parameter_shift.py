@@ -58,10 +58,10 @@ class ShiftPlan:
         names = list(names)
         index = {k: i for i, k in enumerate(names)}
         gates, C, c0 = [], [], []
-        shifts = []   # (kind, position, amount, coeff, jacobi row)
-        for g in circuit:
+        shifts = []   # (kind, position, amount, coeff, jacobi row, gate index)
+        for gi, g in enumerate(circuit):
             if not isinstance(g, G.ParameterGate) or not g.parameterized:
-                gates.append(g)
+                gates.append(g)    # constant gates, measurements and channels stay as they are
                 continue
             new = copy.copy(g)
             new.prs = list(g.prs)
@@ -87,9 +87,9 @@ class ShiftPlan:
                     jac[index[name]] = float(np.real(p[name]))
                 if by_value:
                     key = min(p.keys())
-                    shifts.append(('value', index[key], shift / float(np.real(p[key])), coeff, jac))
+                    shifts.append(('value', index[key], shift / float(np.real(p[key])), coeff, jac, gi))
                 else:
-                    shifts.append(('slot', j, shift, coeff, jac))
+                    shifts.append(('slot', j, shift, coeff, jac, gi))
         self.names = names
         self.circuit = Circuit(gates)
         self.slot_names = [f'_slot{j}' for j in range(len(C))]
@@ -97,7 +97,8 @@ class ShiftPlan:
         self.c0 = np.array(c0, dtype=np.float64)
         self.n_shifts = len(shifts)
         self.D = np.zeros((len(shifts), len(C)))
-        for e, (kind, pos, amount, _, _) in enumerate(shifts):
+        self.gate_of = [sh[5] for sh in shifts]   # circuit position of every shifted angle
+        for e, (kind, pos, amount, _, _, _) in enumerate(shifts):
             if kind == 'slot':
                 self.D[e, pos] = amount
             else:

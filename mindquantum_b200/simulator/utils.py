@@ -1,6 +1,21 @@
 """GradOpsWrapper: the callable returned by get_expectation_with_grad (mindquantum/simulator/utils.py)."""
 
 
+def _thread_balance(n_prs, n_meas, parallel_worker):
+    """(batch_threads, mea_threads) the reference derives from ``parallel_worker``
+    (mindquantum/simulator/utils.py:18-32); here it fixes the order of the random draws of a
+    noisy parameter-shift gradient."""
+    if parallel_worker is None:
+        parallel_worker = n_meas * n_prs
+    if n_meas * n_prs <= parallel_worker:
+        return n_prs, n_meas
+    if n_meas < n_prs:
+        batch = min(n_prs, parallel_worker)
+        return batch, min(n_meas, max(1, parallel_worker // batch))
+    mea = min(n_meas, parallel_worker)
+    return min(n_prs, max(1, parallel_worker // mea)), mea
+
+
 class GradOpsWrapper:
     """Wrap a grad operator with the data it was built from.
 

@@ -19,6 +19,8 @@ What it restates (reference file:line, paths inside mindquantum-ai/mindquantum):
     Hamiltonians given as sparse matrices;
   * ``GetExpectationWithGradParameterShiftOneMulti`` / ``MultiMulti`` (vector_state.tpp:1033-1305)
     in ``get_expectation_with_grad_parameter_shift``, with the shift table of ``shift_rule``;
+  * ``ApplyChannel`` and the channel kernels (vector_state.tpp:465-709) in ``apply_channel``, and the
+    parameter-shift loop with stochastic channels in ``get_expectation_with_grad_parameter_shift_noisy``;
   * ``SamplingMeasurementEndingWithoutNoise`` (vector_state.tpp:1326-1373) with the reference's
     random streams (std::mt19937 + std::uniform_real_distribution<double>), restated in
     ``_Mt19937`` / ``_uniform``.
@@ -489,12 +491,18 @@ class OracleSim:
         self.dtype = dtype
         self.qs = zero_state(n, dtype) if state is None else np.array(state, dtype=dtype)
 
-    def apply_circuit(self, circ, prd=None):
+    def apply_circuit(self, circ, prd=None, draw=None):
+        """Apply gates; channels draw from ``draw`` (the simulator's uniform stream)."""
         prd = prd or {}
         for g in circ:
             if g.name == 'M':
                 raise ValueError("oracle apply_circuit does not sample measurements")
-            apply_gate(self.qs, self.n, g, prd)
+            if is_channel(g):
+                if draw is None:
+                    raise ValueError("a noise channel needs a random stream")
+                apply_channel(self.qs, self.n, g, draw)
+            else:
+                apply_gate(self.qs, self.n, g, prd)
         return self
 
     def get_qs(self):
@@ -554,6 +562,241 @@ def get_expectation_with_grad(n, hams, circ, enc_data, ans_data, enc_names, ans_
     return res
 
 
+
+
+# ----------------------------------------------------------------------------- noise channels
+_CHANNELS = ('PC', 'BFC', 'PFC', 'BPFC', 'GPC', 'DC', 'ADC', 'PDC', 'TRC')
+
+
+def is_channel(g):
+    return g.name in _CHANNELS or hasattr(g, 'kraus_op')
+
+
+def _qubit_prob(qs, q, bit):
+    """OneStateVdot / ZeroStateVdot of a state with itself: sum of |amp|^2 where qubit q == bit."""
+    sel = ((np.arange(qs.size) >> q) & 1) == bit
+    return float(np.sum(np.abs(qs[sel].astype(np.complex128)) ** 2))
+
+
+def _x_like(qs, n, q, ctrls, v1, v2):
+    """ApplyXLike (cpu_vector_core_x_like.cpp:29-57): new[i] = old[j] v1, new[j] = old[i] v2."""
+    v1, v2 = complex(v1), complex(v2)
+    getattr(lib(), f'orc_apply_xlike_{_suf(qs)}')(_ptr(qs), n, q, _mask(ctrls), v1.real, v1.imag, v2.real, v2.imag)
+
+
+def _i_like(qs, n, q, ctrls, a, b):
+    """ApplyILike: diag(a, b) on qubit q (under the controls)."""
+    apply_matrix(qs, n, [q], ctrls, np.array([[a, 0], [0, b]], dtype=np.complex128))
+
+
+def _pauli(qs, n, which, q, ctrls):
+    if which == 0:
+        _x_like(qs, n, q, ctrls, 1, 1)
+    elif which == 1:
+        _x_like(qs, n, q, ctrls, -1j, 1j)
+    elif which == 2:
+        getattr(lib(), f'orc_apply_zlike_{_suf(qs)}')(_ptr(qs), n, q, _mask(ctrls), -1, 0)
+
+
+def _pauli_index(cum, r):
+    """lower_bound over [0, px, px+py, px+py+pz, 1]: 0 = X, 1 = Y, 2 = Z, 3 = I (vector_state.tpp:492-503)."""
+    import bisect
+
+    it = bisect.bisect_left(cum, r)
+    return it - 1 if it > 0 else 0
+
+
+def apply_channel(qs, n, g, draw):
+    """VectorState::ApplyChannel and the channel kernels (vector_state.tpp:465-709), in place.
+
+    ``draw()`` is the simulator's uniform(0, 1) stream; every branch draws exactly as the
+    reference does, so a trajectory is reproduced draw for draw.
+    """
+    objs, ctrls = list(g.obj_qubits), list(g.ctrl_qubits)
+    if g.name in ('PC', 'BFC', 'PFC', 'BPFC'):
+        _pauli(qs, n, _pauli_index(g.cumulative_probs(), draw()), objs[0], ctrls)
+    elif g.name == 'GPC':
+        mx = my = mz = 0
+        ny = 0
+        for q, row in zip(objs, g.probs):
+            px, py, pz = (float(v) for v in row)
+            cum = [0.0, px, px + py, px + py + pz, px + py + pz + (1 - px - py - pz)]
+            k = _pauli_index(cum, draw())
+            if k == 0:
+                mx |= 1 << q
+            elif k == 1:
+                my |= 1 << q
+                ny += 1
+            elif k == 2:
+                mz |= 1 << q
+        getattr(lib(), f'orc_apply_pauli_string_{_suf(qs)}')(_ptr(qs), n, mx, my, mz, ny, 0)
+    elif g.name == 'DC':
+        def uniform(idx):
+            while idx < len(objs):
+                p_i = draw()
+                if p_i < 0.25:
+                    _pauli(qs, n, 0, objs[idx], ctrls)
+                elif p_i < 0.5:
+                    _pauli(qs, n, 1, objs[idx], ctrls)
+                elif p_i < 0.75:
+                    _pauli(qs, n, 2, objs[idx], ctrls)
+                idx += 1
+
+        idx, p = 0, float(g.p)
+        while idx < len(objs):
+            if draw() < p * 3.0 / 4.0:
+                p_i = draw()
+                _pauli(qs, n, 0 if p_i < 1.0 / 3.0 else (1 if p_i < 2.0 / 3.0 else 2), objs[idx], ctrls)
+                uniform(idx + 1)
+                break
+            if not 4 > 3 * p:
+                break
+            idx, p = idx + 1, p / (4 - 3 * p)
+    elif hasattr(g, 'kraus_op'):
+        total = 1.0
+        for m in np.asarray(g.kraus_op, dtype=np.complex128):
+            if abs(m[0, 1]) < 1e-6 and abs(m[1, 0]) < 1e-6 and abs(m[0, 0] - m[1, 1]) < 1e-6:
+                prob = float((m[0, 0] * np.conj(m[0, 0])).real)
+                rel = prob / total
+                total -= prob
+                if draw() < rel:
+                    if m[0, 0].imag >= 1e-6:
+                        qs *= m[0, 0] / math.sqrt(prob)
+                    return
+            else:
+                tmp = qs.copy()
+                apply_matrix(tmp, n, objs, ctrls, m)
+                prob = float(np.vdot(tmp, tmp).real)
+                rel = prob / total
+                total -= prob
+                if draw() < rel:
+                    qs[:] = tmp * (1 / math.sqrt(prob))
+                    return
+    elif g.name in ('ADC', 'PDC'):
+        renorm = _qubit_prob(qs, objs[0], 1)
+        if renorm < 1e-6:
+            return
+        gamma = float(g.gamma)
+        prob = gamma * renorm
+        if draw() <= prob:
+            if g.name == 'ADC':
+                _x_like(qs, n, objs[0], ctrls, 1 / math.sqrt(renorm), 0)
+            else:
+                _i_like(qs, n, objs[0], ctrls, 0, 1 / math.sqrt(renorm))
+        else:
+            _i_like(qs, n, objs[0], ctrls, 1 / math.sqrt(1 - prob), math.sqrt(1 - gamma) / math.sqrt(1 - prob))
+    elif g.name == 'TRC':
+        t1, t2, tg = float(g.t1), float(g.t2), float(g.gate_time)
+        e1, e2 = math.exp(-tg / t1), math.exp(-tg / t2)
+        p_reset = 1 - e1
+        q = objs[0]
+        if t1 >= t2:
+            pz = e1 * (1 - e2 / e1) / 2
+            r = draw()
+            if r < 1 - pz - p_reset:
+                return
+            if r < 1 - p_reset:
+                _pauli(qs, n, 2, q, ctrls)
+            else:
+                zero = _qubit_prob(qs, q, 0)
+                if draw() < zero:
+                    _i_like(qs, n, q, ctrls, 1 / math.sqrt(zero), 0)
+                else:
+                    _x_like(qs, n, q, ctrls, 1 / math.sqrt(1 - zero), 0)
+        elif 2 * t1 > t2:
+            r = draw()
+            root = math.sqrt(p_reset * p_reset + 4 * e2 * e2)
+            ev0, ev1 = (2 - p_reset + root) / 2, (2 - p_reset - root) / 2
+            vec0, vec1 = (ev0 - e1) / e2, (ev1 - e1) / e2
+            zero = _qubit_prob(qs, q, 0)
+            one = 1 - zero
+            c0 = vec0 * vec0 * zero + one
+            p0 = c0 * ev0 / (vec0 * vec0 + 1)
+            if r < p0:
+                _i_like(qs, n, q, ctrls, vec0 / math.sqrt(c0), 1 / math.sqrt(c0))
+            elif r < 1 - p_reset * one:
+                c1 = vec1 * vec1 * zero + one
+                _i_like(qs, n, q, ctrls, vec1 / math.sqrt(c1), 1 / math.sqrt(c1))
+            else:
+                _x_like(qs, n, q, ctrls, 1 / math.sqrt(one), 0)
+    else:
+        raise ValueError(f"{g.name} is not a noise channel.")
+
+
+class UniformStream:
+    """std::uniform_real_distribution<double>(lo, hi) over std::mt19937(seed): the reference's rng_."""
+
+    def __init__(self, seed, lo=0.0, hi=1.0):
+        self.eng = _Mt19937(int(seed))
+        self.lo, self.hi = lo, hi
+
+    def __call__(self):
+        return _uniform(self.eng, self.lo, self.hi)
+
+
+def get_expectation_with_grad_parameter_shift_noisy(n, hams, circ, enc_data, ans_data, enc_names, ans_names,
+                                                    draw, dtype=np.complex128, init_state=None, n_thread=None):
+    """The parameter-shift loop of vector_state.tpp:1033-1230 with stochastic channels: every
+    evaluation runs one trajectory of a copy re-seeded with int(draw() * 10000) from the
+    simulator's stream ``draw``, and every Hamiltonian copy consumes one more draw, in the
+    reference's order (Hamiltonians in groups of n_thread, the Hamiltonian loop inside the gate loop).
+    """
+    gates = [g for g in circ]
+    enc_data = np.atleast_2d(np.asarray(enc_data, dtype=np.float64)) if len(enc_names) else np.zeros((1, 0))
+    ans_data = np.asarray(ans_data, dtype=np.float64).reshape(-1)
+    p_map = {k: i for i, k in enumerate(enc_names)}
+    p_map.update({k: i + len(enc_names) for i, k in enumerate(ans_names)})
+    n_h = len(hams)
+    n_thread = min(15, n_h) if n_thread is None else max(1, min(n_thread, 15, n_h))
+    out = np.zeros((enc_data.shape[0], n_h, 1 + len(p_map)), dtype=np.complex128)
+
+    def trajectory(gate_list, prd):
+        sim = OracleSim(n, dtype, init_state)
+        sub = UniformStream(int(draw() * 10000))
+        for g in gate_list:
+            if is_channel(g):
+                apply_channel(sim.qs, n, g, sub)
+            else:
+                apply_gate(sim.qs, n, g, prd)
+        return sim.qs
+
+    for s in range(enc_data.shape[0]):
+        prd = dict(zip(enc_names, enc_data[s].tolist()))
+        prd.update(dict(zip(ans_names, ans_data.tolist())))
+        base = trajectory(gates, prd)
+        for start in range(0, n_h, n_thread):
+            group = range(start, min(start + n_thread, n_h))
+            draw()                                   # the group's copy of the state
+            for j in group:
+                draw()                               # its Hamiltonian copy
+                out[s, j, 0] = expectation_of_terms(base, base, n, hams[j])
+            for gi, g in enumerate(gates):
+                prs = getattr(g, 'prs', None)
+                if is_channel(g) or not prs or not any(len(p.requires_grad_parameters) for p in prs):
+                    continue
+                shift, coeff, multi = shift_rule(g)
+                for j in group:
+                    for k, p in enumerate(prs):
+                        if p.is_const():
+                            continue
+                        f = []
+                        for sign in (-1.0, 1.0):
+                            shifted, pr_s = g, prd
+                            if multi:
+                                key = min(p.keys())
+                                pr_s = dict(prd)
+                                pr_s[key] = prd[key] + sign * shift / float(np.real(p[key]))
+                            else:
+                                shifted = copy.copy(g)
+                                shifted.prs = list(prs)
+                                shifted.prs[k] = p + sign * shift
+                            qs = trajectory(gates[:gi] + [shifted] + gates[gi + 1:], pr_s)
+                            draw()                   # the Hamiltonian copy of this evaluation
+                            f.append(expectation_of_terms(qs, qs, n, hams[j]))
+                        intrin = coeff * float(np.real(f[1] - f[0]))
+                        for name in p.requires_grad_parameters:
+                            out[s, j, 1 + p_map[name]] += intrin * float(np.real(p[name]))
+    return out
 
 # ----------------------------------------------------------------------------- parameter shift
 _PS_EXACT = ('RX', 'RY', 'RZ', 'Rxx', 'Ryy', 'Rzz', 'Rxy', 'Rxz', 'Ryz', 'GP', 'PS', 'U3')
