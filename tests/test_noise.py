@@ -1,0 +1,167 @@
+"""Noise channels as stochastic trajectories (vector_state.tpp:465-709; channel.py).
+
+Host: the oracle's trajectories average to the channel's Kraus map (written here from the
+channel definitions, independent of the oracle), within the statistical error of the sample;
+channel argument validation.  GPU: one trajectory on the device equals the oracle's trajectory
+with the same seed, draw for draw (complex128 1e-10, complex64 1e-5), over many seeds so every
+branch runs; sampling frequencies of noisy circuits against the Kraus map; the noisy
+parameter-shift gradient against the oracle's loop with the same simulator stream.
+Reference tests: tests/st/test_simulator/test_channel_with_simulator.py:40-230.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from mindquantum_b200 import complex64, complex128
+from mindquantum_b200.core import gates as G
+from mindquantum_b200.core.circuit import Circuit
+from mindquantum_b200.core.operators import Hamiltonian, QubitOperator
+from mindquantum_b200.simulator import Simulator
+from oracle import oracle as O
+
+X = np.array([[0, 1], [1, 0]], dtype=complex)
+Y = np.array([[0, -1j], [1j, 0]])
+Z = np.diag([1.0 + 0j, -1.0])
+I2 = np.eye(2, dtype=complex)
+
+
+def kraus_of(g):
+    """Kraus operators of a single-qubit channel, from its definition."""
+    if isinstance(g, G.PauliChannel):
+        return [math.sqrt(1 - g.px - g.py - g.pz) * I2, math.sqrt(g.px) * X, math.sqrt(g.py) * Y,
+                math.sqrt(g.pz) * Z]
+    if isinstance(g, G.DepolarizingChannel):
+        return [math.sqrt(1 - 3 * g.p / 4) * I2] + [math.sqrt(g.p / 4) * P for P in (X, Y, Z)]
+    if isinstance(g, G.AmplitudeDampingChannel):
+        return [np.array([[1, 0], [0, math.sqrt(1 - g.gamma)]]), np.array([[0, math.sqrt(g.gamma)], [0, 0]])]
+    if isinstance(g, G.PhaseDampingChannel):
+        return [np.array([[1, 0], [0, math.sqrt(1 - g.gamma)]]), np.array([[0, 0], [0, math.sqrt(g.gamma)]])]
+    if isinstance(g, G.KrausChannel):
+        return list(np.asarray(g.kraus_op, dtype=complex))
+    raise TypeError(g)
+
+
+def _kraus_ops():
+    a, b = 0.3, 0.5
+    k0 = np.array([[1, 0], [0, math.sqrt(1 - a)]])
+    k1 = np.array([[0, math.sqrt(a) * math.sqrt(b)], [0, 0]])
+    k2 = np.array([[0, math.sqrt(a) * math.sqrt(1 - b)], [0, 0]])
+    return [k0, k1, k2]
+
+
+CHANNELS = [G.BitFlipChannel(0.3), G.PhaseFlipChannel(0.2), G.BitPhaseFlipChannel(0.4),
+            G.PauliChannel(0.1, 0.15, 0.2), G.DepolarizingChannel(0.6), G.AmplitudeDampingChannel(0.35),
+            G.PhaseDampingChannel(0.45), G.KrausChannel('k3', _kraus_ops())]
+
+
+def _rho_avg(g, psi, trajectories, seed0):
+    rho = np.zeros((2, 2), dtype=complex)
+    for t in range(trajectories):
+        qs = O.OracleSim(1, np.complex128, psi).apply_circuit(Circuit([g.on(0)]), {},
+                                                               O.UniformStream(seed0 + t)).qs
+        rho += np.outer(qs, qs.conj())
+    return rho / trajectories
+
+
+@pytest.mark.parametrize("g", CHANNELS, ids=lambda g: g.name)
+def test_oracle_trajectories_average_to_the_kraus_map(g):
+    rng = np.random.default_rng(3)
+    psi = rng.normal(size=2) + 1j * rng.normal(size=2)
+    psi /= np.linalg.norm(psi)
+    T = 4000
+    rho = _rho_avg(g, psi, T, 100)
+    ref = sum(k @ np.outer(psi, psi.conj()) @ k.conj().T for k in kraus_of(g))
+    assert np.allclose(np.trace(ref), 1)
+    assert np.max(np.abs(rho - ref)) < 5 / math.sqrt(T)
+
+
+def test_thermal_relaxation_preserves_trace_and_decays():
+    psi = np.array([0, 1], dtype=complex)
+    g = G.ThermalRelaxationChannel(2.0, 1.5, 0.5)
+    rho = _rho_avg(g, psi, 3000, 7)
+    assert abs(np.trace(rho) - 1) < 1e-12
+    # excited population decays as exp(-t / T1)
+    assert abs(rho[1, 1].real - math.exp(-0.5 / 2.0)) < 5 / math.sqrt(3000)
+
+
+def test_channel_argument_checks():
+    with pytest.raises(ValueError):
+        G.PauliChannel(0.5, 0.4, 0.3)
+    with pytest.raises(ValueError):
+        G.AmplitudeDampingChannel(1.5)
+    with pytest.raises(TypeError):
+        G.PhaseDampingChannel('a')
+    with pytest.raises(ValueError):
+        G.DepolarizingChannel(1.4)
+    with pytest.raises(ValueError, match="completeness"):
+        G.KrausChannel('bad', [np.eye(2), np.eye(2)])
+    with pytest.raises(ValueError):
+        G.ThermalRelaxationChannel(1.0, 2.5, 0.1)
+    with pytest.raises(ValueError):
+        G.GroupedPauliChannel(np.array([[0.5, 0.4, 0.3]]))
+    assert Circuit([G.H.on(0), G.AmplitudeDampingChannel(0.1).on(0)]).is_noise_circuit
+    assert not Circuit([G.H.on(0)]).is_noise_circuit
+
+
+def noisy_circuit():
+    c = Circuit([G.H.on(0), G.RX('a').on(1), G.X.on(2, 0), G.BitFlipChannel(0.3).on(1),
+                 G.RY({'b': 2.0}).on(2), G.DepolarizingChannel(0.5, 2).on([0, 2]), G.RZ('a').on(0, 1),
+                 G.AmplitudeDampingChannel(0.4).on(1), G.PhaseDampingChannel(0.3).on(2, 0),
+                 G.PauliChannel(0.1, 0.2, 0.3).on(0), G.KrausChannel('k3', _kraus_ops()).on(2),
+                 G.ThermalRelaxationChannel(2.0, 1.5, 0.7).on(0), G.ThermalRelaxationChannel(1.0, 1.5, 0.4).on(1),
+                 G.GroupedPauliChannel(np.array([[0.2, 0.1, 0.1], [0.0, 0.3, 0.2]])).on([1, 2]), G.H.on(1),
+                 G.Rzz('c').on([0, 1])])
+    return c
+
+
+# ------------------------------------------------------------------------------------------- GPU
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [complex128, complex64])
+def test_trajectories_match_the_oracle_draw_for_draw(dtype):
+    circ = noisy_circuit()
+    pr = {'a': 0.7, 'b': -1.3, 'c': 2.1}
+    rng = np.random.default_rng(5)
+    psi = rng.normal(size=8) + 1j * rng.normal(size=8)
+    psi /= np.linalg.norm(psi)
+    tol = 1e-10 if dtype == complex128 else 1e-5
+    for seed in range(1, 41):
+        sim = Simulator('mqvector_b200', 3, dtype=dtype, seed=seed)
+        sim.set_qs(psi)
+        sim.apply_circuit(circ, pr)
+        ref = O.OracleSim(3, np.complex128, psi).apply_circuit(circ, pr, O.UniformStream(seed)).qs
+        assert np.allclose(sim.get_qs(), ref, atol=tol, rtol=0), seed
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("g", CHANNELS[3:], ids=lambda g: g.name)
+def test_noisy_sampling_frequencies(g):
+    """test_channel_with_simulator.py: outcome frequencies of channel + measurement."""
+    rng = np.random.default_rng(9)
+    psi = rng.normal(size=2) + 1j * rng.normal(size=2)
+    psi /= np.linalg.norm(psi)
+    sim = Simulator('mqvector_b200', 1, dtype=complex128, seed=11)
+    sim.set_qs(psi)
+    shots = 4000
+    res = sim.sampling(Circuit([g.on(0), G.Measure().on(0)]), shots=shots, seed=17)
+    p1 = res.data.get('1', 0) / shots
+    ref = sum(k @ np.outer(psi, psi.conj()) @ k.conj().T for k in kraus_of(g))
+    assert abs(p1 - ref[1, 1].real) < 5 * math.sqrt(0.25 / shots)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [complex128, complex64])
+def test_noisy_parameter_shift_matches_the_oracle_loop(dtype):
+    circ = Circuit([G.RX('a').on(0), G.AmplitudeDampingChannel(0.3).on(0), G.RY({'b': 2.0}).on(1),
+                    G.X.on(1, 0), G.DepolarizingChannel(0.2).on(1), G.RZ('a').on(1), G.U3('c', 0.3, 'd').on(0)])
+    hams = [Hamiltonian(QubitOperator('Z0')), Hamiltonian(QubitOperator('X1 Y0', 0.5))]
+    p = np.array([0.4, 1.1, -0.7, 2.0])
+    sim = Simulator('mqvector_b200', 2, dtype=dtype, seed=23)
+    f, g = sim.get_expectation_with_grad(hams, circ)(p)
+    ref = O.get_expectation_with_grad_parameter_shift_noisy(2, hams, circ, np.zeros((1, 0)), p, [],
+                                                            circ.params_name, O.UniformStream(23))
+    tol = 1e-10 if dtype == complex128 else 2e-3
+    assert np.allclose(f, ref[:, :, 0], atol=tol, rtol=0)
+    assert np.allclose(g, ref[:, :, 1:], atol=tol * (1 if dtype == complex128 else 10), rtol=0)
+    with pytest.raises(ValueError, match="noise circuit"):
+        sim.get_expectation_with_grad(hams, circ, Circuit([G.H.on(0)]))
