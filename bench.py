@@ -465,6 +465,34 @@ def run_workload(args, rank, local_rank):
                                 "frac": alg / (csr_ms / 1e3) / 1e9 / peak, "states": B,
                                 "bytes_model": "passes*(nnz*(4+8) + 8*(dim+1)) + B*2*S, passes = ceil(B/4)"}
         del states
+    elif args.workload == 'noise':
+        from mindquantum_b200.core import gates as G
+        from mindquantum_b200.core.circuit import Circuit
+        from mindquantum_b200.simulator import Simulator
+
+        n, layers = 20, 4
+        circ, ham, params_np = build_workload(n, layers, 1, seed=rank)
+        noisy = Circuit()
+        per_layer = 3 * n - 1
+        for k, g in enumerate(circ):
+            noisy += g
+            if (k + 1) % per_layer == 0:     # after every layer: depolarizing + amplitude damping per qubit
+                for q in range(n):
+                    noisy += G.DepolarizingChannel(0.01).on(q)
+                    noisy += G.AmplitudeDampingChannel(0.02).on(q)
+        names = circ.params_name
+        prd = dict(zip(names, params_np[0].tolist()))
+        sim_api = Simulator('mqvector_b200', n, dtype=complex64, seed=7)
+        units = 1
+
+        def step():
+            return sim_api.get_expectation(ham, noisy, pr=prd)
+
+        e2e_step = step
+        io = (params_np.nbytes, 16)
+        cfg = {"workload": f"noisy trajectories, HEA {n}q x {layers} layers with a depolarizing (p=0.01) and an "
+                           f"amplitude-damping (gamma=0.02) channel on every qubit after every layer "
+                           f"({2 * n * layers} channels), one trajectory + <H> per unit", "n_qubits": n, "batch": 1}
     elif args.workload == 'pshift':
         n, layers = 16, 2
         circ, ham, params_np = build_workload(n, layers, 1, seed=rank)
@@ -559,7 +587,7 @@ def main():
     ap.add_argument('--skip-extras', action='store_true')
     ap.add_argument('--skip-plain', action='store_true')
     ap.add_argument('--skip-cpu', action='store_true')
-    ap.add_argument('--workload', default='hea', choices=['hea', 'qnn', 'qaoa', 'uneven', 'csr', 'pshift'],
+    ap.add_argument('--workload', default='hea', choices=['hea', 'qnn', 'qaoa', 'uneven', 'csr', 'pshift', 'noise'],
                     help='hea: the headline 26-qubit HEA gradient; the others are the remaining workload families')
     args = ap.parse_args()
     rank = int(os.environ.get('RANK', 0))

@@ -190,7 +190,15 @@ MQB_API int mqb_apply_hamiltonian(const mqb_hamiltonian *ham, const void *in, vo
 MQB_API int mqb_expectation(const mqb_hamiltonian *ham, const void *bra, const void *ket, int64_t batch, double *out,
                     void *stream);
 
-/* out[b] = <a_b|b_b> as (re, im) float64 on the device. */
+/* One 2x2 complex matrix (any matrix, not only unitaries) on `qubit` of `batch` states, in place,
+ * where every bit of ctrl_mask is set.  matrix: host, 8 doubles, row-major (re, im) pairs.
+ * The sweep of ApplySingleQubitMatrix (cpu_vector_core_matrix_gate.cpp:151), used for the
+ * operators a noise channel picks: ApplyX/Y/Z, ApplyILike, ApplyXLike, QSMulValue
+ * (vector_state.tpp:491-709). */
+MQB_API int mqb_apply_matrix1(int n_qubits, int precision, void *states, int64_t batch, int qubit,
+                              uint64_t ctrl_mask, const double *matrix, void *stream);
+
+/* out[b] = <a_b|b_b> as (re, im) float64 on the device. *//* out[b] = <a_b|b_b> as (re, im) float64 on the device. */
 MQB_API int mqb_vdot(int n_qubits, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream);
 
 /* ------------------------------------------------------------------ adjoint gradient */

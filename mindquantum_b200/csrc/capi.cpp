@@ -1014,6 +1014,27 @@ int mqb_expectation(const mqb_hamiltonian *h, const void *bra, const void *ket, 
     });
 }
 
+int mqb_apply_matrix1(int n, int precision, void *states, int64_t batch, int qubit, uint64_t ctrl_mask,
+                      const double *matrix, void *stream) {
+    return guarded([&] {
+        if (!states || !matrix) fail(MQB_ERR_INVALID, "null argument");
+        if (n < 1 || n > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
+        if (qubit < 0 || qubit >= n) fail(MQB_ERR_INVALID, "qubit %d outside the register", qubit);
+        if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
+        if (n < 64 && (ctrl_mask >> n)) fail(MQB_ERR_INVALID, "control mask outside the register");
+        if (ctrl_mask >> qubit & 1) fail(MQB_ERR_INVALID, "the target qubit cannot be a control");
+        Mat1 m;
+        for (int k = 0; k < 8; ++k) m.v[k] = matrix[k];
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const int sm = sm_count_cached();
+        TimeScope ts(TK_OTHER, st);
+        if (precision == MQB_PREC_C64)
+            ck(launch_matrix1<float>(static_cast<float2 *>(states), n, qubit, ctrl_mask, batch, m, sm, st), "matrix");
+        else
+            ck(launch_matrix1<double>(static_cast<double2 *>(states), n, qubit, ctrl_mask, batch, m, sm, st), "matrix");
+    });
+}
+
 int mqb_vdot(int n, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream) {
     return guarded([&] {
         if (!a || !b || !out) fail(MQB_ERR_INVALID, "null argument");

@@ -1022,6 +1022,36 @@ cudaError_t launch_csr(const CsrArgs<R> &a, int lanes, int sm_count, cudaStream_
     return cudaSuccess;
 }
 
+// One 2x2 matrix (unitary or not) on `qubit` of `batch` states where every control bit is set:
+// the single sweep of ApplySingleQubitMatrix (cpu_vector_core_matrix_gate.cpp:151), used for the
+// operators a noise channel picks (X, Y, Z, diag(a, b), [[0, a], [b, 0]], a global factor).
+template <typename R>
+__global__ void matrix1_kernel(cplx<R> *st, int n, int qubit, uint64_t ctrl, int64_t batch, Mat1 m) {
+    const int64_t half = int64_t(1) << (n - 1), dim = int64_t(1) << n;
+    const int64_t low = (int64_t(1) << qubit) - 1;
+    const R m0r = R(m.v[0]), m0i = R(m.v[1]), m1r = R(m.v[2]), m1i = R(m.v[3]);
+    const R m2r = R(m.v[4]), m2i = R(m.v[5]), m3r = R(m.v[6]), m3i = R(m.v[7]);
+    for (int64_t w = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; w < batch * half;
+         w += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t b = w / half, l = w % half;
+        const int64_t i = ((l & ~low) << 1) | (l & low), j = i | (int64_t(1) << qubit);
+        if ((uint64_t(i) & ctrl) != ctrl) continue;
+        cplx<R> *p = st + b * dim;
+        const cplx<R> a = p[i], c = p[j];
+        p[i] = cplx<R>{m0r * a.x - m0i * a.y + m1r * c.x - m1i * c.y, m0r * a.y + m0i * a.x + m1r * c.y + m1i * c.x};
+        p[j] = cplx<R>{m2r * a.x - m2i * a.y + m3r * c.x - m3i * c.y, m2r * a.y + m2i * a.x + m3r * c.y + m3i * c.x};
+    }
+}
+
+template <typename R>
+cudaError_t launch_matrix1(cplx<R> *st, int n, int qubit, uint64_t ctrl, int64_t batch, const Mat1 &m, int sm_count,
+                           cudaStream_t s) {
+    const int64_t work = batch * (int64_t(1) << (n - 1));
+    const int blocks = int(std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, int64_t(sm_count) * 8)));
+    matrix1_kernel<R><<<blocks, 256, 0, s>>>(st, n, qubit, ctrl, batch, m);
+    return cudaGetLastError();
+}
+
 template <typename R>
 __global__ void copy_kernel(cplx<R> *dst, const cplx<R> *src, int n, int64_t batch, int64_t src_stride) {
     const int64_t dim = int64_t(1) << n;
@@ -1254,6 +1284,7 @@ cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale
                                         cudaStream_t);                                                             \
     template cudaError_t launch_copy_or_zero<R>(cplx<R> *, const cplx<R> *, int, int64_t, int64_t, cudaStream_t);  \
     template cudaError_t launch_csr<R>(const CsrArgs<R> &, int, int, cudaStream_t);                                 \
+    template cudaError_t launch_matrix1<R>(cplx<R> *, int, int, uint64_t, int64_t, const Mat1 &, int, cudaStream_t); \
     template cudaError_t launch_chunk_probs<R>(const cplx<R> *, int, int, double *, cudaStream_t);                 \
     template cudaError_t launch_sample_search<R>(const cplx<R> *, int, int, const double *, const double *,       \
                                                  int64_t, int64_t *, cudaStream_t);                                \

@@ -127,6 +127,13 @@ struct CsrArgs {
 };
 template <typename R>
 cudaError_t launch_csr(const CsrArgs<R> &a, int lanes, int sm_count, cudaStream_t s);
+// A 2x2 complex matrix by value, row-major, (re, im) pairs.
+struct Mat1 {
+    double v[8];
+};
+template <typename R>
+cudaError_t launch_matrix1(cplx<R> *st, int n, int qubit, uint64_t ctrl, int64_t batch, const Mat1 &m, int sm_count,
+                           cudaStream_t s);
 template <typename R>
 cudaError_t launch_copy_or_zero(cplx<R> *dst, const cplx<R> *src, int n, int64_t batch, int64_t src_stride,
                                 cudaStream_t s);

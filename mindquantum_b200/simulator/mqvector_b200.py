@@ -249,13 +249,19 @@ class MQVectorB200(BackendBase):
 
     # ------------------------------------------------------------------ noise channels
     def _matrix_on(self, state, m, q, ctrls=()):
-        """A constant 2x2 matrix (unitary or not) on qubit q under ``ctrls``, in place."""
-        self._apply_segment(state, Circuit([G.UnivMathGate('K', np.asarray(m, dtype=complex)).on(q, list(ctrls))]),
-                            ParameterResolver())
+        """A 2x2 matrix (unitary or not) on qubit q under ``ctrls``, in place (one device sweep)."""
+        mv = np.ascontiguousarray(np.asarray(m, dtype=np.complex128).reshape(4)).view(np.float64)
+        mask = 0
+        for c in ctrls:
+            mask |= 1 << int(c)
+        N.call('mqb_apply_matrix1', self.n_qubits, self.precision, _ptr(state), 1, int(q), mask,
+               mv.ctypes.data_as(ctypes.c_void_p), _stream())
+
+    _PAULI = (np.array([[0, 1], [1, 0]], dtype=complex), np.array([[0, -1j], [1j, 0]]),
+              np.array([[1, 0], [0, -1]], dtype=complex))
 
     def _pauli_on(self, state, which, q, ctrls=()):
-        gate = (G.X, G.Y, G.Z)[which]
-        self._apply_segment(state, Circuit([gate.on(q, list(ctrls))]), ParameterResolver())
+        self._matrix_on(state, self._PAULI[which], q, ctrls)
 
     def _one_probability(self, state, q):
         out = torch.zeros(1, dtype=torch.float64, device=self.device)

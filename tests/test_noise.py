@@ -104,6 +104,26 @@ def test_channel_argument_checks():
     assert not Circuit([G.H.on(0)]).is_noise_circuit
 
 
+@pytest.mark.parametrize("case", ['qubit', 'ctrl_on_target', 'ctrl_outside', 'batch'])
+def test_matrix_abi_rejects_invalid_arguments(case):
+    import ctypes
+    from mindquantum_b200 import _native as N
+
+    m = np.eye(2, dtype=np.complex128).reshape(4).view(np.float64)
+    q, ctrl, batch = 1, 0, 1
+    if case == 'qubit':
+        q = 3
+    elif case == 'ctrl_on_target':
+        ctrl = 1 << q
+    elif case == 'ctrl_outside':
+        ctrl = 1 << 5
+    else:
+        batch = 0
+    with pytest.raises(RuntimeError):
+        N.call('mqb_apply_matrix1', 3, N.MQB_PREC_C128, ctypes.c_void_p(16), batch, q, ctrl,
+               m.ctypes.data_as(ctypes.c_void_p), None)
+
+
 def noisy_circuit():
     c = Circuit([G.H.on(0), G.RX('a').on(1), G.X.on(2, 0), G.BitFlipChannel(0.3).on(1),
                  G.RY({'b': 2.0}).on(2), G.DepolarizingChannel(0.5, 2).on([0, 2]), G.RZ('a').on(0, 1),
