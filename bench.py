@@ -563,11 +563,12 @@ def run_workload(args, rank, local_rank):
         extras["grad_err_vs_c128"] = float((g64 - g128).abs().max().item())
         extras["f_err_vs_c128"] = float((f64[..., 0] - f128[..., 0]).abs().max().item())
         del s128
+    unit = "trajectories/s" if args.workload == 'noise' else UNIT
     line = {
-        "metric": f"grad evals/s, {args.workload} workload", "value": value, "unit": UNIT, "n_gpus": 1,
+        "metric": f"{unit}, {args.workload} workload", "value": value, "unit": unit, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic", "config": cfg,
-        "e2e": {"value": units * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(io[0]),
+        "e2e": {"value": units * args.steps / e2e_s, "unit": unit, "h2d_bytes_per_step": int(io[0]),
                 "d2h_bytes_per_step": int(io[1])},
         "kernel_ms_per_step": {k: v / args.steps for k, v in kt.ms.items() if v},
         "clocks": clocks.summary(), "gpu_launches": sum(kt.launches.values()), **extras,

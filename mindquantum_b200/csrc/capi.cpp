@@ -121,19 +121,20 @@ struct mqb_hamiltonian {
     std::vector<HamClass> classes;
     HamClass *d_classes = nullptr;
     HamTerm *d_terms = nullptr;
-    // or a CSR matrix (csr == true)
+    // or a sparse matrix (csr == true), as slices of 32 rows with column-major entries
     bool csr = false;
-    int csr_lanes = 1;
-    int64_t nnz = 0;
-    int64_t *d_indptr = nullptr;
-    int32_t *d_indices = nullptr;
-    void *d_data = nullptr;
+    int64_t nnz = 0, entries = 0;
+    int64_t *d_slice_ptr = nullptr;
+    int32_t *d_slice_len = nullptr;
+    int32_t *d_cols = nullptr;
+    void *d_vals = nullptr;
     ~mqb_hamiltonian() {
         cudaFree(d_classes);
         cudaFree(d_terms);
-        cudaFree(d_indptr);
-        cudaFree(d_indices);
-        cudaFree(d_data);
+        cudaFree(d_slice_ptr);
+        cudaFree(d_slice_len);
+        cudaFree(d_cols);
+        cudaFree(d_vals);
     }
 };
 
@@ -354,9 +355,10 @@ static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R>
     const int64_t dim = int64_t(1) << h.n;
     if (h.csr) {
         CsrArgs<R> a{};
-        a.indptr = h.d_indptr;
-        a.indices = h.d_indices;
-        a.data = static_cast<const cplx<R> *>(h.d_data);
+        a.slice_ptr = h.d_slice_ptr;
+        a.slice_len = h.d_slice_len;
+        a.cols = h.d_cols;
+        a.vals = static_cast<const cplx<R> *>(h.d_vals);
         a.dim = dim;
         a.bra = bra;
         a.ket = ket;
@@ -365,7 +367,7 @@ static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R>
         a.f_stride = f_stride;
         a.batch = batch;
         TimeScope ts(TK_HAM, st);
-        ck(launch_csr<R>(a, h.csr_lanes, sm, st), "sparse hamiltonian");
+        ck(launch_csr<R>(a, sm, st), "sparse hamiltonian");
         return;
     }
     if (h.groups.empty()) {
@@ -957,28 +959,55 @@ int mqb_ham_create_csr(int n_qubits, int precision, int64_t nnz, const int64_t *
         if (indptr[0] != 0 || indptr[dim] != nnz) fail(MQB_ERR_INVALID, "indptr must run from 0 to nnz");
         for (int64_t r = 0; r < dim; ++r)
             if (indptr[r + 1] < indptr[r]) fail(MQB_ERR_INVALID, "indptr decreases at row %lld", (long long)r);
-        std::vector<int32_t> idx(static_cast<size_t>(nnz));
-        for (int64_t j = 0; j < nnz; ++j) {
+        for (int64_t j = 0; j < nnz; ++j)
             if (indices[j] < 0 || indices[j] >= dim)
                 fail(MQB_ERR_INVALID, "column index %lld out of range at entry %lld", (long long)indices[j], (long long)j);
-            idx[size_t(j)] = int32_t(indices[j]);
+        // slices of 32 rows, entry k of row `lane` at slice_ptr + 32 k + lane, padded with
+        // (column = the row, value 0) up to the slice's longest row
+        const int64_t n_slices = (dim + 31) / 32;
+        std::vector<int64_t> sptr(static_cast<size_t>(n_slices));
+        std::vector<int32_t> slen(static_cast<size_t>(n_slices));
+        int64_t entries = 0;
+        for (int64_t sl = 0; sl < n_slices; ++sl) {
+            int64_t longest = 0;
+            for (int64_t r = sl * 32; r < std::min(dim, sl * 32 + 32); ++r) longest = std::max(longest, indptr[r + 1] - indptr[r]);
+            if (longest > INT32_MAX) fail(MQB_ERR_INVALID, "row too long");
+            sptr[size_t(sl)] = entries;
+            slen[size_t(sl)] = int32_t(longest);
+            entries += longest * 32;
+        }
+        const size_t elem = precision == MQB_PREC_C64 ? 8 : 16;
+        std::vector<int32_t> cols(static_cast<size_t>(entries));
+        std::vector<unsigned char> vals(static_cast<size_t>(entries) * elem, 0);
+        const unsigned char *src = static_cast<const unsigned char *>(data);
+        for (int64_t sl = 0; sl < n_slices; ++sl) {
+            for (int lane = 0; lane < 32; ++lane) {
+                const int64_t r = sl * 32 + lane;
+                const int64_t row_len = r < dim ? indptr[r + 1] - indptr[r] : 0;
+                for (int64_t k = 0; k < slen[size_t(sl)]; ++k) {
+                    const size_t at = size_t(sptr[size_t(sl)] + k * 32 + lane);
+                    if (k < row_len) {
+                        const int64_t j = indptr[r] + k;
+                        cols[at] = int32_t(indices[j]);
+                        std::memcpy(&vals[at * elem], src + size_t(j) * elem, elem);
+                    } else {
+                        cols[at] = int32_t(r < dim ? r : 0);
+                    }
+                }
+            }
         }
         auto h = std::make_unique<mqb_hamiltonian>();
         h->n = n_qubits;
         h->precision = precision;
         h->csr = true;
         h->nnz = nnz;
-        // lanes per row: about four entries per lane
-        const double mean = double(nnz) / double(dim);
-        int lanes = 1;
-        while (lanes < 32 && lanes * 4 < mean) lanes *= 2;
-        h->csr_lanes = lanes;
-        h->d_indptr = upload(std::vector<int64_t>(indptr, indptr + dim + 1));
-        h->d_indices = upload(idx);
-        const size_t elem = precision == MQB_PREC_C64 ? 8 : 16;
-        if (nnz > 0) {
-            ck(cudaMalloc(&h->d_data, elem * size_t(nnz)), "cudaMalloc");
-            ck(cudaMemcpy(h->d_data, data, elem * size_t(nnz), cudaMemcpyHostToDevice), "cudaMemcpy");
+        h->entries = entries;
+        h->d_slice_ptr = upload(sptr);
+        h->d_slice_len = upload(slen);
+        h->d_cols = upload(cols);
+        if (entries > 0) {
+            ck(cudaMalloc(&h->d_vals, vals.size()), "cudaMalloc");
+            ck(cudaMemcpy(h->d_vals, vals.data(), vals.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
         }
         *out = h.release();
     });

@@ -914,36 +914,41 @@ cudaError_t launch_vdot(const cplx<R> *a, const cplx<R> *b, int n, int64_t batch
 }
 
 // ------------------------------------------------------------------ sparse (CSR) Hamiltonians
-// out[b] = A ket[b] and fout[b] += <bra[b]|A ket[b]> for a CSR matrix A (Csr_Dot_Vec /
-// ExpectationOfCsr, ccsrc/include/core/sparse/algo.h:160-200).  G lanes share a row (G a power
-// of two dividing 32, chosen from the mean row length); one pass over the matrix serves up to
-// kCsrStates states, so the matrix is read ceil(batch / kCsrStates) times.  Rows run in warp-
-// uniform steps so the group reductions are full-warp shuffles.  Row sums are in the state
-// precision like the reference's; the expectation is accumulated in FP64.
+// out[b] = A ket[b] and fout[b] += <bra[b]|A ket[b]> (Csr_Dot_Vec / ExpectationOfCsr,
+// ccsrc/include/core/sparse/algo.h:160-200) with A kept as slices of 32 rows: entry k of the
+// slice's row `lane` sits at slice_ptr[s] + 32 k + lane, rows padded to the slice's longest row
+// (padding: column = the row itself, value 0).  One warp per slice, one thread per row, so the
+// matrix reads of a warp are 128-byte (columns) and 256/512-byte (values) runs, and for a matrix
+// built from Pauli strings (columns r ^ f) the state gathers of a warp land in one aligned block.
+// One pass over the matrix serves up to kCsrStates states.  Row sums are in the state precision
+// like the reference's; the expectation is accumulated in FP64.
 constexpr int kCsrStates = 4;
 
-template <typename R, int G>
-__global__ void __launch_bounds__(256) csr_kernel(CsrArgs<R> a, int64_t b0) {
+template <typename R>
+__global__ void __launch_bounds__(256) sell_kernel(CsrArgs<R> a, int64_t b0) {
     __shared__ double red[2 * kCsrStates][8];
     const int nb = int(a.batch - b0 < kCsrStates ? a.batch - b0 : kCsrStates);
-    const int lane = threadIdx.x & 31, lg = lane & (G - 1);
+    const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
     const int64_t n_warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
-    constexpr int kRowsPerWarp = 32 / G;
+    const int64_t n_slices = (a.dim + 31) >> 5;
     double fre[kCsrStates], fim[kCsrStates];
 #pragma unroll
     for (int k = 0; k < kCsrStates; ++k) fre[k] = fim[k] = 0;
-    for (int64_t base = warp * kRowsPerWarp; base < a.dim; base += n_warps * kRowsPerWarp) {
-        const int64_t row = base + lane / G;
+    for (int64_t sl = warp; sl < n_slices; sl += n_warps) {
+        const int64_t row = (sl << 5) + lane;
         const bool valid = row < a.dim;
+        const int64_t beg = a.slice_ptr[sl];
+        const int len = a.slice_len[sl];
         R ar[kCsrStates], ai[kCsrStates];
 #pragma unroll
         for (int k = 0; k < kCsrStates; ++k) ar[k] = ai[k] = 0;
         if (valid) {
-            const int64_t end = a.indptr[row + 1];
-            for (int64_t j = a.indptr[row] + lg; j < end; j += G) {
-                const int64_t col = a.indices[j];
-                const cplx<R> d = a.data[j];
+#pragma unroll 4
+            for (int e = 0; e < len; ++e) {
+                const int64_t at = beg + (int64_t(e) << 5) + lane;
+                const int64_t col = a.cols[at];
+                const cplx<R> d = a.vals[at];
 #pragma unroll
                 for (int k = 0; k < kCsrStates; ++k) {
                     if (k < nb) {
@@ -953,16 +958,6 @@ __global__ void __launch_bounds__(256) csr_kernel(CsrArgs<R> a, int64_t b0) {
                     }
                 }
             }
-        }
-#pragma unroll
-        for (int k = 0; k < kCsrStates; ++k) {
-#pragma unroll
-            for (int o = G / 2; o > 0; o >>= 1) {
-                ar[k] += __shfl_xor_sync(0xffffffffu, ar[k], o);
-                ai[k] += __shfl_xor_sync(0xffffffffu, ai[k], o);
-            }
-        }
-        if (valid && lg == 0) {
 #pragma unroll
             for (int k = 0; k < kCsrStates; ++k) {
                 if (k < nb) {
@@ -1001,21 +996,12 @@ __global__ void __launch_bounds__(256) csr_kernel(CsrArgs<R> a, int64_t b0) {
 }
 
 template <typename R>
-cudaError_t launch_csr(const CsrArgs<R> &a, int lanes, int sm_count, cudaStream_t s) {
+cudaError_t launch_csr(const CsrArgs<R> &a, int sm_count, cudaStream_t s) {
     const int threads = 256;
-    const int64_t rows_per_block = int64_t(threads / lanes);
-    const int blocks = int(std::max<int64_t>(1, std::min<int64_t>((a.dim + rows_per_block - 1) / rows_per_block,
-                                                                  int64_t(sm_count) * 8)));
+    const int64_t n_slices = (a.dim + 31) >> 5;
+    const int blocks = int(std::max<int64_t>(1, std::min<int64_t>((n_slices + 7) / 8, int64_t(sm_count) * 8)));
     for (int64_t b0 = 0; b0 < a.batch; b0 += kCsrStates) {
-        switch (lanes) {
-            case 1: csr_kernel<R, 1><<<blocks, threads, 0, s>>>(a, b0); break;
-            case 2: csr_kernel<R, 2><<<blocks, threads, 0, s>>>(a, b0); break;
-            case 4: csr_kernel<R, 4><<<blocks, threads, 0, s>>>(a, b0); break;
-            case 8: csr_kernel<R, 8><<<blocks, threads, 0, s>>>(a, b0); break;
-            case 16: csr_kernel<R, 16><<<blocks, threads, 0, s>>>(a, b0); break;
-            case 32: csr_kernel<R, 32><<<blocks, threads, 0, s>>>(a, b0); break;
-            default: return cudaErrorInvalidValue;
-        }
+        sell_kernel<R><<<blocks, threads, 0, s>>>(a, b0);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -1283,7 +1269,7 @@ cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale
     template cudaError_t launch_vdot<R>(const cplx<R> *, const cplx<R> *, int, int64_t, double *, int,             \
                                         cudaStream_t);                                                             \
     template cudaError_t launch_copy_or_zero<R>(cplx<R> *, const cplx<R> *, int, int64_t, int64_t, cudaStream_t);  \
-    template cudaError_t launch_csr<R>(const CsrArgs<R> &, int, int, cudaStream_t);                                 \
+    template cudaError_t launch_csr<R>(const CsrArgs<R> &, int, cudaStream_t);                                      \
     template cudaError_t launch_matrix1<R>(cplx<R> *, int, int, uint64_t, int64_t, const Mat1 &, int, cudaStream_t); \
     template cudaError_t launch_chunk_probs<R>(const cplx<R> *, int, int, double *, cudaStream_t);                 \
     template cudaError_t launch_sample_search<R>(const cplx<R> *, int, int, const double *, const double *,       \

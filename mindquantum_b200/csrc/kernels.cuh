@@ -110,13 +110,14 @@ cudaError_t launch_plain_grad(const cplx<R> *psi, const cplx<R> *lam, int n, int
 template <typename R>
 cudaError_t launch_vdot(const cplx<R> *a, const cplx<R> *b, int n, int64_t batch, double *out, int sm_count,
                         cudaStream_t s);
-// A CSR matrix applied to `batch` states (rows = dim = 2^n): out[b] = A ket[b] (if out) and
-// fout[b * f_stride .. +1] += <bra[b]|A ket[b]> (if fout).
+// A sparse matrix applied to `batch` states (rows = dim = 2^n), kept as slices of 32 rows with
+// column-major entries: out[b] = A ket[b] (if out), fout[b * f_stride .. +1] += <bra[b]|A ket[b]>.
 template <typename R>
 struct CsrArgs {
-    const int64_t *indptr;     // [dim + 1]
-    const int32_t *indices;    // [nnz]
-    const cplx<R> *data;       // [nnz]
+    const int64_t *slice_ptr;  // [n_slices] first entry of every slice
+    const int32_t *slice_len;  // [n_slices] entries per row of the slice (padded)
+    const int32_t *cols;       // [entries] column of entry 32 k + lane
+    const cplx<R> *vals;       // [entries]
     int64_t dim;
     const cplx<R> *bra;
     const cplx<R> *ket;
@@ -126,7 +127,7 @@ struct CsrArgs {
     int64_t batch;
 };
 template <typename R>
-cudaError_t launch_csr(const CsrArgs<R> &a, int lanes, int sm_count, cudaStream_t s);
+cudaError_t launch_csr(const CsrArgs<R> &a, int sm_count, cudaStream_t s);
 // A 2x2 complex matrix by value, row-major, (re, im) pairs.
 struct Mat1 {
     double v[8];
