@@ -944,7 +944,6 @@ __global__ void __launch_bounds__(256) sell_kernel(CsrArgs<R> a, int64_t b0) {
 #pragma unroll
         for (int k = 0; k < kCsrStates; ++k) ar[k] = ai[k] = 0;
         if (valid) {
-#pragma unroll 4
             for (int e = 0; e < len; ++e) {
                 const int64_t at = beg + (int64_t(e) << 5) + lane;
                 const int64_t col = a.cols[at];
