@@ -67,6 +67,11 @@ int sm_count_cached() {
 
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
+// State buffers are read and written as 16-byte vectors: refuse others before any device work.
+void require_aligned(const void *ptr, const char *what) {
+    if (ptr && (reinterpret_cast<uintptr_t>(ptr) & 15u)) fail(MQB_ERR_INVALID, "%s must be 16-byte aligned", what);
+}
+
 template <typename T>
 T *upload(const std::vector<T> &v) {
     if (v.empty()) return nullptr;
@@ -901,6 +906,7 @@ int mqb_apply(mqb_program *p, void *states, int64_t batch, const double *params,
               const double *custom, void *ws, size_t ws_bytes, void *stream) {
     return guarded([&] {
         if (!p || !states) fail(MQB_ERR_INVALID, "null argument");
+        require_aligned(states, "states");
         if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
         if (p->per_sample && !params && p->n_params) fail(MQB_ERR_INVALID, "parameters required");
         if (p->custom_entries && !custom) fail(MQB_ERR_INVALID, "custom gate matrices required");
@@ -1020,6 +1026,8 @@ int mqb_ham_destroy(mqb_hamiltonian *h) {
 int mqb_apply_hamiltonian(const mqb_hamiltonian *h, const void *in, void *out, int64_t batch, void *stream) {
     return guarded([&] {
         if (!h || !in || !out) fail(MQB_ERR_INVALID, "null argument");
+        require_aligned(in, "in");
+        require_aligned(out, "out");
         if (in == out) fail(MQB_ERR_INVALID, "in and out must be different buffers");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         if (h->precision == MQB_PREC_C64)
@@ -1033,6 +1041,8 @@ int mqb_apply_hamiltonian(const mqb_hamiltonian *h, const void *in, void *out, i
 int mqb_expectation(const mqb_hamiltonian *h, const void *bra, const void *ket, int64_t batch, double *out, void *stream) {
     return guarded([&] {
         if (!h || !bra || !ket || !out) fail(MQB_ERR_INVALID, "null argument");
+        require_aligned(bra, "bra");
+        require_aligned(ket, "ket");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         ck(cudaMemsetAsync(out, 0, sizeof(double) * 2 * batch, st), "memset");
         if (h->precision == MQB_PREC_C64)
@@ -1067,6 +1077,8 @@ int mqb_apply_matrix1(int n, int precision, void *states, int64_t batch, int qub
 int mqb_vdot(int n, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream) {
     return guarded([&] {
         if (!a || !b || !out) fail(MQB_ERR_INVALID, "null argument");
+        require_aligned(a, "a");
+        require_aligned(b, "b");
         const int sm = sm_count_cached();
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         if (precision == MQB_PREC_C64)
@@ -1091,6 +1103,8 @@ int mqb_expectation_with_grad(mqb_program *p, const mqb_hamiltonian *const *hams
                               void *stream) {
     return guarded([&] {
         if (!p || !hams || !f || !grad) fail(MQB_ERR_INVALID, "null argument");
+        require_aligned(init, "init_states");
+        require_aligned(ws, "workspace");
         if (n_hams < 1) fail(MQB_ERR_INVALID, "need at least one Hamiltonian");
         if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
         for (int h = 0; h < n_hams; ++h) {
@@ -1115,6 +1129,9 @@ int mqb_adjoint_with_lambda(mqb_program *p, const void *lam, int lam_batched, co
                             double *grad, int stride, void *ws, size_t ws_bytes, void *stream) {
     return guarded([&] {
         if (!p || !lam || !grad) fail(MQB_ERR_INVALID, "null argument");
+        require_aligned(lam, "lambda");
+        require_aligned(init, "init_states");
+        require_aligned(ws, "workspace");
         if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
         if (p->custom_entries && !custom) fail(MQB_ERR_INVALID, "custom gate matrices required");
         if (batch > 65535 / 12) fail(MQB_ERR_INVALID, "batch too large for one call");

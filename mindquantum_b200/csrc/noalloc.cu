@@ -55,6 +55,8 @@ extern "C" {
 MQB_API int mqb_apply_static(mqb_program *prog, void *states, int64_t batch, const double *params,
                              int64_t param_stride, const double *custom, void *stream) {
     if (!prog || !states || batch < 1) return fail_static(MQB_ERR_INVALID, "mqb_apply_static: invalid argument");
+    if (reinterpret_cast<uintptr_t>(states) & 15u)
+        return fail_static(MQB_ERR_INVALID, "mqb_apply_static: states must be 16-byte aligned");
     size_t need = 0;
     int st = mqb_apply_workspace_size(prog, batch, &need);
     if (st != MQB_OK) return st;

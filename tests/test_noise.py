@@ -124,6 +124,15 @@ def test_matrix_abi_rejects_invalid_arguments(case):
                m.ctypes.data_as(ctypes.c_void_p), None)
 
 
+def test_state_pointers_must_be_16_byte_aligned():
+    """Misaligned state buffers are refused on the host, before any device work."""
+    import ctypes
+    from mindquantum_b200 import _native as N
+
+    with pytest.raises(RuntimeError, match="16-byte aligned"):
+        N.call('mqb_vdot', 3, N.MQB_PREC_C128, ctypes.c_void_p(8), ctypes.c_void_p(32), 1, ctypes.c_void_p(64), None)
+
+
 def noisy_circuit():
     c = Circuit([G.H.on(0), G.RX('a').on(1), G.X.on(2, 0), G.BitFlipChannel(0.3).on(1),
                  G.RY({'b': 2.0}).on(2), G.DepolarizingChannel(0.5, 2).on([0, 2]), G.RZ('a').on(0, 1),
