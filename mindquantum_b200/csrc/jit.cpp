@@ -312,7 +312,7 @@ void emit_backward_op(std::ostringstream &o, const StageOp &so, int NH, int gid)
         for (int a = 0; a < 3; ++a) {
             if (!((G >> a) & 1)) continue;
             o << "      for (int h = 0; h < NH; ++h) {\n"
-              << "        const double x = warp_sum(double(acc[" << a << "][h]));\n"
+              << "        const double x = double(warp_sum_acc(acc[" << a << "][h]));\n"
               << "        if (lane == 0) wacc[(warp * NLS + " << (so.lslot + r) << ") * NH + h] += x;\n"
               << "      }\n";
             ++r;
@@ -539,7 +539,7 @@ void emit_backward_run(std::ostringstream &o, const std::vector<const StageOp *>
                 }
             }
             if (so.lslot >= 0)
-                o << "        for (int h = 0; h < NH; ++h) {\n          const double x = warp_sum(double(acc[0][h]));\n"
+                o << "        for (int h = 0; h < NH; ++h) {\n          const double x = double(warp_sum_acc(acc[0][h]));\n"
                   << "          if (lane == 0) wacc[(warp * NLS + " << so.lslot << ") * NH + h] += x;\n        }\n";
             o << "      }\n";
         }

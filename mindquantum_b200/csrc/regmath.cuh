@@ -68,6 +68,15 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Sum over a warp in the accumulator's own precision: one 32-bit shuffle per step for
+// complex64 partials (each already a sum of at most 32 products), FP64 from the warp partial up.
+__device__ __forceinline__ float warp_sum_acc(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_sum_acc(double v) { return warp_sum(v); }
+
 // Register index j takes part in a gate on position P controlled by the positions in CM.
 template <int P, unsigned CM>
 __device__ __forceinline__ constexpr bool pair_on(int j) {
