@@ -30,6 +30,7 @@ namespace mqb {
 namespace {
 
 using reg::warp_sum;
+using reg::warp_sum_acc;
 
 using mqb::tile::swz;
 using mqb::tile::tile_base;
@@ -209,11 +210,11 @@ __global__ void __launch_bounds__(256, 2) fused_bwd2_kernel(const Bwd2Args<R> a)
                         if (!(so.grad_mask >> an & 1)) continue;
 #pragma unroll
                         for (int h = 0; h < NH; ++h) {
-                            double x = 0;
+                            R xr = 0;
 #pragma unroll
                             for (int q = 0; q < 3; ++q)
-                                if (q == an) x = double(acc[q][h]);
-                            x = warp_sum(x);
+                                if (q == an) xr = acc[q][h];
+                            const double x = double(warp_sum_acc(xr));   // FP32 across the warp for complex64
                             if (lane == 0) wacc[(warp * nls + so.lslot + r) * NH + h] += x;
                         }
                         ++r;
