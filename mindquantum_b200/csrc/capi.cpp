@@ -944,8 +944,11 @@ int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const ui
         h->precision = precision;
         std::vector<HamClass> classes;
         std::vector<HamTerm> hterms;
-        build_ham_groups(n_qubits, default_tile_bits(precision, 1), contiguity_bits(precision), mx, my, mz, ny, cf,
-                         h->groups, classes, hterms);
+        // complex64: 2^12-amplitude tiles, 256 threads of 16 registers each, so two blocks
+        // (125 registers a thread) share an SM and one's tile loads overlap the other's math
+        const int hk = precision == MQB_PREC_C64 ? std::min(12, default_tile_bits(precision, 1))
+                                                 : default_tile_bits(precision, 1);
+        build_ham_groups(n_qubits, hk, contiguity_bits(precision), mx, my, mz, ny, cf, h->groups, classes, hterms);
         h->classes = classes;
         h->d_classes = upload(classes);
         h->d_terms = upload(hterms);
