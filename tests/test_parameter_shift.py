@@ -189,3 +189,27 @@ def test_parameter_shift_at_sixteen_qubits_matches_adjoint():
     f_ad, g_ad = sim.get_expectation_with_grad(ham, circ)(params[0])
     assert np.allclose(f, f_ad, atol=1e-10)
     assert np.allclose(g, g_ad, atol=1e-9)
+
+
+@pytest.mark.parametrize("n_thread", [1, 2, 3])
+def test_noiseless_stream_advance_matches_the_reference_loop(n_thread):
+    """The noiseless batched path advances the simulator's stream by
+    n_prs * (1 + groups + n_hams * (1 + 4 E)) draws: the count the reference's loop consumes."""
+    circ = Circuit([G.RX('a').on(0), G.RY({'b': 2.0}).on(1), G.X.on(1, 0), G.U3('c', 0.3, 'd').on(0),
+                    G.RZ('a').on(1, 0)])
+    hams = [Hamiltonian(QubitOperator('Z0')), Hamiltonian(QubitOperator('X1')), Hamiltonian(QubitOperator('Y0 Y1'))]
+
+    class Counting:
+        def __init__(self):
+            self.n, self.s = 0, O.UniformStream(5)
+
+        def __call__(self):
+            self.n += 1
+            return self.s()
+
+    draw = Counting()
+    O.get_expectation_with_grad_parameter_shift_noisy(2, hams, circ, np.zeros((1, 0)), [0.1, 0.2, 0.3, 0.4], [],
+                                                      circ.params_name, draw, n_thread=n_thread)
+    E = ShiftPlan(circ, circ.params_name).n_shifts
+    groups = -(-len(hams) // n_thread)
+    assert draw.n == 1 + groups + len(hams) * (1 + 4 * E)
