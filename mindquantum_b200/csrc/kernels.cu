@@ -484,6 +484,7 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
     const int64_t total = a.batch * n_tiles;
     const uint32_t lowmask = (1u << c) - 1u;
     const int hi_shift = K - NRB;
+    const bool bra_is_ket = a.bra == a.ket;
     for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
         const int64_t b = w >> g.n_out;
         const uint64_t t = uint64_t(w) & uint64_t(n_tiles - 1);
@@ -555,7 +556,8 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
             const uint32_t L = uint32_t(tid + T * r);
             const uint64_t gL = base + tab[L >> c] + (L & lowmask);
             if (a.fout) {
-                const V bv = a.bra[b * dim + gL];
+                // <psi|H psi> (bra == ket): the bra amplitudes are the staged tile's
+                const V bv = bra_is_ket ? ket[L] : a.bra[b * dim + gL];
                 fr += double(bv.x) * double(ar[r]) + double(bv.y) * double(ai[r]);
                 fi += double(bv.x) * double(ai[r]) - double(bv.y) * double(ar[r]);
             }
