@@ -473,6 +473,9 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
     V *tcoef = reinterpret_cast<V *>(smem + o);
     o = align16(o + size_t(nt) * sizeof(V));
     uint32_t *tmask = reinterpret_cast<uint32_t *>(smem + o);
+    // groups after the first add to the output: their previous sum is staged with the tile
+    V *prev = nullptr;
+    if (a.accumulate && a.out) prev = reinterpret_cast<V *>(smem + align16(o + size_t(nt) * sizeof(uint32_t)));
     const int nw = T / 32, warp = tid / 32, lane = tid % 32;
     build_table(tab, g);
     for (int i = tid; i < nw * 2; i += T) wf[i] = 0;
@@ -490,6 +493,7 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
         const uint64_t t = uint64_t(w) & uint64_t(n_tiles - 1);
         const uint64_t base = tile_base(g, t);
         load_tile(ket, a.ket + b * dim, base, tab, K, c);
+        if (prev) load_tile(prev, a.out + b * a.out_batch_stride, base, tab, K, c);
         for (int q = tid; q < nt; q += T) {
             const HamTerm &ht = a.terms[a.term_begin + q];
             const bool neg = __popcll(base & ht.omask) & 1;
@@ -567,7 +571,7 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
                 v.x = ar[r];
                 v.y = ai[r];
                 if (a.accumulate) {
-                    const V old = *op;
+                    const V old = prev[L];
                     v.x += old.x;
                     v.y += old.y;
                 }
@@ -601,13 +605,15 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
 
 static size_t align_up16(size_t x) { return (x + 15) & ~size_t(15); }
 
-static size_t ham2_smem(const TileGeom &g, int elem_bytes, int threads, int n_classes, int n_terms) {
+static size_t ham2_smem(const TileGeom &g, int elem_bytes, int threads, int n_classes, int n_terms, bool staged_out) {
     size_t s = align_up16((size_t(1) << g.K) * elem_bytes);
     s = align_up16(s + (size_t(1) << (g.K - g.c)) * sizeof(uint64_t));
     s = align_up16(s + size_t(threads / 32) * 2 * sizeof(double));
     s = align_up16(s + size_t(n_classes) * sizeof(HamClass));
     s = align_up16(s + size_t(n_terms) * elem_bytes);
-    return s + size_t(n_terms) * sizeof(uint32_t);
+    s += size_t(n_terms) * sizeof(uint32_t);
+    if (staged_out) s = align_up16(s) + (size_t(1) << g.K) * elem_bytes;   // the previous groups' sum
+    return s;
 }
 
 template <typename R>
@@ -615,7 +621,8 @@ cudaError_t launch_ham(const HamArgs<R> &a, int sm_count, cudaStream_t s) {
     if (a.g.c < 1 || a.g.K > kMaxTileBits || a.g.K < 1) return cudaErrorInvalidValue;  // 16-byte tile accesses need a contiguous low qubit
     if (a.g.K >= 5 + kHamRegBits && (a.g.K - kHamRegBits) <= (sizeof(R) == 4 ? 9 : 8)) {
         const int threads = 1 << (a.g.K - kHamRegBits);
-        const size_t smem2 = ham2_smem(a.g, int(sizeof(cplx<R>)), threads, a.n_classes, a.n_terms);
+        const size_t smem2 = ham2_smem(a.g, int(sizeof(cplx<R>)), threads, a.n_classes, a.n_terms,
+                                       a.accumulate && a.out);
         if (smem2 <= 160 * 1024) {
             auto kern = ham2_kernel<R, kHamRegBits>;
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem2));
