@@ -539,8 +539,12 @@ class MQVectorB200(BackendBase):
         return f, g[:, :, :len(param_names)]
 
     def _choose_stride(self, prog, batch, n_hams):
-        """Store the state after every pass when it fits in 85% of free memory, else every sqrt(P) passes."""
+        """Store the state after every pass when it fits in 85% of free memory, else every sqrt(P) passes.
+
+        Free memory counts what torch's caching allocator holds unused (the previous call's
+        workspace), which the driver reports as taken."""
         free, _ = torch.cuda.mem_get_info(self.device)
+        free += torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
         for stride in (1, max(2, int(math.ceil(math.sqrt(max(1, prog.grad_passes(n_hams)[0]))))), 0):
             ws = ctypes.c_size_t()
             N.call('mqb_grad_workspace_size', prog.handle, batch, n_hams, stride, ctypes.byref(ws))
