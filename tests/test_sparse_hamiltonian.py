@@ -260,3 +260,19 @@ def test_random_csr_apply_and_expectation_against_oracle(dtype):
     out = sim.get_qs()
     ref_v = O.apply_terms(psi, n, ham)
     assert np.allclose(out, ref_v, atol=100 * TOL[dtype], rtol=0)
+
+
+@pytest.mark.gpu
+def test_circuit_batch_with_sparse_matrix_hamiltonians():
+    """Graph-captured CircuitBatch members whose Hamiltonians are CSR matrices."""
+    from mindquantum_b200.simulator.batch import CircuitBatch
+
+    members = W.uneven_u3(4, 8, 11, layers=2, n_terms=8, seed=3)
+    batch = CircuitBatch([(n, c, Hamiltonian(W.pauli_csr(h, n))) for n, c, h, _ in members], dtype=complex128,
+                         graph=True, streams=2)
+    params = [p for _, _, _, p in members]
+    fs, gs = batch(params)
+    for (n, c, h, _), p, f, g in zip(members, params, fs, gs):
+        ref = O.get_expectation_with_grad(n, [h], c, np.zeros((1, 0)), p, [], c.params_name)
+        assert abs(f[0].item() - ref[0, 0, 0]) < 1e-10
+        assert np.allclose(g[0].cpu().numpy(), ref[0, 0, 1:].real, atol=1e-10, rtol=0)
