@@ -411,3 +411,49 @@ def test_qram_operator_matches_oracle():
         assert np.allclose(out[s].detach().numpy(), ref[0, :, 0].real, atol=1e-10)
         g_ref += np.einsum('mp,m->p', ref[0, :, 1:].real, w[s].numpy())
     assert np.allclose(ans.grad.numpy(), g_ref, atol=1e-9)
+
+
+@pytest.mark.parametrize("dtype", [complex128, complex64])
+def test_non_hermitian_gradient_batched_encoder(dtype):
+    """Three encoder samples through the batched lambda-injection sweeps, each against central
+    finite differences of <phi|U_l^dag H U_r|psi> computed with the oracle."""
+    n = 3
+    rng = np.random.default_rng(29)
+    psi0 = rng.normal(size=8) + 1j * rng.normal(size=8)
+    psi0 /= np.linalg.norm(psi0)
+    circ_r = Circuit([G.RX('x0').on(0), G.RY('x1').on(1), G.X.on(2, 0), G.RZ({'w0': 1.0, 'x0': 0.5}).on(2),
+                      G.H.on(1), G.Ryy('w1').on([0, 2])]).as_encoder()
+    for g in circ_r:
+        for p in g.get_parameters():
+            for k in p.params_name:
+                if k.startswith('w'):
+                    p.ansatz_part(k)
+    circ_r = Circuit(list(circ_r))
+    circ_l = Circuit([G.H.on(0), G.RX('w1').on(2), G.X.on(1, 2)])
+    ham = Hamiltonian(QubitOperator('X0 Z2', 0.6) + QubitOperator('Y1', -0.8))
+    hmat = np.array([O.apply_terms(np.eye(8, dtype=np.complex128)[k].copy(), n, ham) for k in range(8)]).T
+
+    def f_of(pr):
+        r = O.OracleSim(n, np.complex128, psi0).apply_circuit(circ_r, pr).qs
+        l = O.OracleSim(n, np.complex128, psi0).apply_circuit(circ_l, pr).qs
+        return np.vdot(l, hmat @ r)
+
+    sim = Simulator('mqvector_b200', n, dtype=dtype)
+    sim.set_qs(psi0)
+    ops = sim.get_expectation_with_grad(ham, circ_r, circ_l)
+    enc_names, ans_names = ops.encoder_params_name, ops.ansatz_params_name
+    enc = rng.uniform(0, 2 * np.pi, (3, len(enc_names)))
+    ans = rng.uniform(0, 2 * np.pi, len(ans_names))
+    f, ge, ga = ops(enc, ans)
+    tol = 1e-7 if dtype == complex128 else 5e-5
+    for s in range(3):
+        pr = dict(zip(enc_names, enc[s]))
+        pr.update(zip(ans_names, ans))
+        assert abs(f[s, 0] - f_of(pr)) < tol
+        for k, name in enumerate(enc_names + ans_names):
+            pp, pm = dict(pr), dict(pr)
+            pp[name] += 1e-6
+            pm[name] -= 1e-6
+            fd = (f_of(pp) - f_of(pm)) / 2e-6
+            got = ge[s, 0, k] if k < len(enc_names) else ga[s, 0, k - len(enc_names)]
+            assert abs(got - fd) < (1e-7 if dtype == complex128 else 1e-4), (s, name, got, fd)
