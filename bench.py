@@ -17,7 +17,6 @@ port of the mqvector CPU kernels) on the host cores, one bounded sample per step
 import argparse
 import ctypes
 import json
-import math
 import os
 import subprocess
 import sys

@@ -19,7 +19,7 @@ from ..core import gates as G
 from ..core.circuit import Circuit
 from ..core.operators import Hamiltonian, HowTo
 from ..core.parameterresolver import ParameterResolver, to_pr
-from ..dtype import complex64, complex128, to_mq_type
+from ..dtype import complex64, complex128
 from .backend_base import BackendBase
 from .lowering import lowered, native_ham
 from .measure_result import MeasureResult

@@ -10,7 +10,7 @@ import torch
 
 from mindquantum_b200 import complex64, complex128
 from mindquantum_b200.core import gates as G
-from mindquantum_b200.core.circuit import UN, Circuit
+from mindquantum_b200.core.circuit import Circuit
 from mindquantum_b200.core.operators import Hamiltonian, QubitOperator
 from mindquantum_b200.simulator import Simulator, inner_product
 from oracle import oracle as O

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from mindquantum_b200.core import gates as G
-from mindquantum_b200.core.circuit import UN, Circuit
+from mindquantum_b200.core.circuit import Circuit
 from mindquantum_b200.core.operators import Hamiltonian, QubitOperator
 from oracle import oracle as O
 from reference_circuits import generate_test_circuit, mul_qubit_circuit, multi_params_circuit
