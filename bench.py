@@ -122,18 +122,71 @@ def _peaks():
         return 6650.0, 'fallback'
 
 
-def _traffic_from_profiles():
-    """DRAM bytes per state byte of one adjoint launch, from the committed ncu summary (a smaller
-    case of the same kernel; traffic grows with the state bytes a launch processes)."""
-    import re
+# DRAM bytes per state byte moved by one adjoint pass launch (psi read, lambda read + write: 3 x
+# S*B algorithmic), from an ncu capture of the same kernel on the HEA 24-qubit, batch-2 case; a
+# launch's traffic grows in proportion to the state bytes it processes.  None: not captured for
+# the kernels built from the current sources.
+ADJ_DRAM_BYTES_PER_STATE_BYTE = None
 
-    path = os.path.join(ROOT, 'profiles', 'mqb_adj_pass_hea24_c64.md')
-    try:
-        with open(path, encoding='utf8') as f:
-            m = re.search(r'^dram_bytes_per_state_byte:\s*([0-9.]+)', f.read(), re.M)
-        return float(m.group(1)) if m else None
-    except OSError:
-        return None
+
+def oracle_fixture_errors(n, layers, batch, seed, f_c64, g_c64, f_c128=None, g_c128=None):
+    """max |delta| of <H> and the gradient of parameter set 0 against the FP64 oracle's result for the
+    same workload (tests/golden/hea26_oracle.json, made by tests/golden/make_oracle_fixtures.py)."""
+    path = os.path.join(ROOT, 'tests', 'golden', f'hea{n}_oracle.json')
+    if seed != 0 or not os.path.exists(path):
+        return {}
+    with open(path, encoding='utf8') as f:
+        fx = json.load(f)
+    if fx.get('layers') != layers or fx.get('batch') != batch:
+        return {}
+    row = fx['samples'][0]
+    ref_g = np.array(row['grad'])
+    out = {"oracle_fixture": os.path.relpath(path, ROOT),
+           "f_err_vs_oracle_c64": abs(float(f_c64) - row['f']),
+           "grad_err_vs_oracle_c64": float(np.max(np.abs(np.asarray(g_c64) - ref_g)))}
+    if g_c128 is not None:
+        out["f_err_vs_oracle_c128"] = abs(float(f_c128) - row['f'])
+        out["grad_err_vs_oracle_c128"] = float(np.max(np.abs(np.asarray(g_c128) - ref_g)))
+    return out
+
+
+def apply_throughput(sim, circ, names, params, n, B, reps, peak):
+    """Fused gate application alone: the circuit applied in place to B resident states (mqb_apply,
+    one generated kernel per pass), gates/s and the HBM fraction of its passes."""
+    import torch
+
+    from mindquantum_b200 import _native as N
+    from mindquantum_b200.simulator import lowering
+
+    prog = lowering.lowered(circ, n, sim.precision, names, None, True)
+    states = torch.zeros((B, 1 << n), dtype=sim.torch_dtype, device=sim.device)
+    states[:, 0] = 1
+    ws_b = ctypes.c_size_t()
+    N.call('mqb_apply_workspace_size', prog.handle, B, ctypes.byref(ws_b))
+    ws = torch.empty(max(256, ws_b.value), dtype=torch.uint8, device=sim.device)
+    st = torch.cuda.current_stream()
+
+    def run():
+        N.call('mqb_apply', prog.handle, ctypes.c_void_p(states.data_ptr()), B, ctypes.c_void_p(params.data_ptr()),
+               params.shape[1], None, ctypes.c_void_p(ws.data_ptr()), ws_b.value, ctypes.c_void_p(st.cuda_stream))
+
+    for _ in range(3):
+        run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        run()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    S = (1 << n) * states.element_size() * B
+    passes = prog.info.n_passes
+    alg = 2 * S * passes
+    del states, ws
+    return {"gates_per_s": len(circ) * B / (ms / 1e3), "ms_per_apply": ms, "gates": len(circ), "states": B,
+            "passes": passes, "tile_bits": prog.info.tile_bits, "alg_bytes": alg,
+            "achieved_gbs": alg / (ms / 1e3) / 1e9, "frac": alg / (ms / 1e3) / 1e9 / peak,
+            "bytes_model": "passes x 2 x S x B (every pass reads and writes each state once)"}
 
 
 def cpu_reference_sample(n, layers_total, threads, steps=1, warmup=0, dtype=np.complex64):
@@ -280,11 +333,11 @@ def run_b200(args, rank, world, local_rank):
     peak, peak_kind = _peaks()
     achieved = alg.get(dom, 0) * args.steps / (kt.ms[dom] / 1e3) / 1e9 if kt.ms[dom] else None
     total_alg = sum(alg.values()) * args.steps
-    traffic = _traffic_from_profiles()
+    traffic = ADJ_DRAM_BYTES_PER_STATE_BYTE
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
                 "traffic": (traffic * S if (traffic and dom == 'fused_backward') else None),
-                "traffic_source": "profiles/mqb_adj_pass_hea24_c64.md: dram bytes per state byte x S*B",
+                "traffic_source": "ncu dram bytes per state byte of the adjoint pass (24-qubit capture) x S*B",
                 "alg_bytes_per_launch": alg.get(dom, 0) / max(1, kt.launches[dom] // args.steps),
                 "avg_launch_ms": kt.ms[dom] / max(1, kt.launches[dom]), "peak_source": peak_kind,
                 "step_hbm_gbs": total_alg / (ms / 1e3) / 1e9 if world == 1 else None,
@@ -322,6 +375,10 @@ def run_b200(args, rank, world, local_rank):
         extras["f_err_vs_c128"] = float((f[:1, :, 0] - f128[:, :, 0]).abs().max().item())
         extras["grad_max_abs"] = float(g128.abs().max().item())
         extras["c128_fused"] = {"value": 1.0 / t128, "unit": UNIT, "batch": 1}
+        extras.update(oracle_fixture_errors(n, layers, B, rank, f[0, 0, 0].item(), g[0, 0].cpu().numpy(),
+                                            f128[0, 0, 0].item(), g128[0, 0].cpu().numpy()))
+        extras["apply"] = apply_throughput(sim, circ, names, params, n, B, 5, peak)
+        extras["device_error"] = N.device_error()
         if not args.skip_plain:
             # the plain complex128 single-circuit path: one kernel per gate, per-gate reductions
             sp = MQVectorB200('mqvector_b200', n, dtype=complex128, device=dev, fuse=False)

@@ -120,6 +120,11 @@ MQB_API int mqb_device_sm_count(int *out);
  * synchronizes, writes total milliseconds and launch counts per kind and stops timing. */
 MQB_API int mqb_timing_begin(void);
 MQB_API int mqb_timing_end(double *ms, int64_t *launches, int n_kinds);
+/* Error word of the generated pass kernels on the current device: *code = 0, or
+ * MQB_DEV_ERR_TIMEOUT (1) when a kernel gave up a wait on its tile pipeline (the call's results
+ * are then invalid); clear != 0 resets it.  Synchronizes the device.  No reference counterpart:
+ * the reference's kernels have no bounded waits. */
+MQB_API int mqb_device_error(int *code, int clear);
 /* sizeof of mqb_gate_desc, mqb_param_term, mqb_program_options, mqb_program_info (ABI check). */
 MQB_API int mqb_abi_struct_sizes(int64_t *out, int n);
 

@@ -73,6 +73,7 @@ SIGNATURES = {
     'mqb_device_sm_count': [_P],
     'mqb_timing_begin': [],
     'mqb_timing_end': [_P, _P, _I],
+    'mqb_device_error': [_P, _I],
     'mqb_abi_struct_sizes': [_P, _I],
     'mqb_program_create': [_I, _I, _P, _I, _P, _I, _I, _P, _I64, _P, _P],
     'mqb_program_destroy': [_P],
@@ -165,3 +166,11 @@ class KernelTimer:
         self.ms = {k: ms[i] for i, k in enumerate(TIMING_KINDS)}
         self.launches = {k: cnt[i] for i, k in enumerate(TIMING_KINDS)}
         return False
+
+
+def device_error(clear=True):
+    """Error word of the generated pass kernels on the current device (0: none; 1: a tile-pipeline
+    wait gave up, the results since the last check are invalid).  Synchronizes the device."""
+    code = ctypes.c_int()
+    call('mqb_device_error', ctypes.byref(code), 1 if clear else 0)
+    return code.value

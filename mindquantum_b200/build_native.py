@@ -19,9 +19,10 @@ LIB = os.path.join(HERE, 'libmqb200.so')
 FUSED = ['fused_fwd_c64.cu', 'fused_fwd_c128.cu', 'fused_bwd_c64.cu', 'fused_bwd_c128.cu']
 SOURCES = ['kernels.cu', *FUSED, 'capi.cpp', 'scheduler.cpp', 'noalloc.cu', 'jit.cpp']
 HEADERS = ['kernels.cuh', 'mqb_internal.h', 'mqb_gate_ids.h', 'fused_impl.cuh', 'regops.cuh', 'regmath.cuh',
-           'tile.cuh', 'jit_abi.h', 'jit.h']
+           'tile.cuh', 'jit_abi.h', 'jit.h', 'pipe.cuh']
 # headers compiled again at run time by NVRTC for the generated pass kernels (embedded as text)
-JIT_HEADERS = [('kJitRegmath', 'regmath.cuh'), ('kJitTile', 'tile.cuh'), ('kJitAbi', 'jit_abi.h')]
+JIT_HEADERS = [('kJitRegmath', 'regmath.cuh'), ('kJitTile', 'tile.cuh'), ('kJitAbi', 'jit_abi.h'),
+               ('kJitPipe', 'pipe.cuh')]
 # NVRTC from the CUDA toolkit the library is built with (found again at run time through the rpath)
 CUDA_LIB = '/usr/local/cuda/lib64'
 NVRTC_LIBS = [f'-L{CUDA_LIB}', '-lnvrtc', '-Xlinker', f'-rpath={CUDA_LIB}']
@@ -89,13 +90,26 @@ def build(force=False, verbose=False):
     compiles.append([_nvcc(), *common, '-x', 'c++', '-c', embed, '-o', obj('jit_embed.cpp')])
     link = [_nvcc(), *ARCH, '-shared', '-cudart', 'static', '-ccbin', 'g++',
             *[obj(f) for f in SOURCES], obj('jit_embed.cpp'), *NVRTC_LIBS, '-lpthread', '-ldl', '-o', LIB + '.tmp']
-    headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, 'mqb200.h')]
-    newest_header = max(os.path.getmtime(h) for h in headers)
+    def newest_dep(src):
+        # the source and every header it includes, transitively (quoted includes of this tree)
+        seen, todo, newest = set(), [src], 0.0
+        while todo:
+            f = todo.pop()
+            if f in seen or not os.path.exists(f):
+                continue
+            seen.add(f)
+            newest = max(newest, os.path.getmtime(f))
+            with open(f, encoding='utf8') as fh:
+                for line in fh:
+                    line = line.strip()
+                    if line.startswith('#include "'):
+                        todo.append(os.path.normpath(os.path.join(os.path.dirname(f), line.split('"')[1])))
+        return newest
 
     def stale(cmd):
         out = cmd[cmd.index('-o') + 1]
         src = cmd[cmd.index('-c') + 1]
-        return force or not os.path.exists(out) or os.path.getmtime(out) < max(os.path.getmtime(src), newest_header)
+        return force or not os.path.exists(out) or os.path.getmtime(out) < newest_dep(src)
 
     def run(cmd):
         if verbose:

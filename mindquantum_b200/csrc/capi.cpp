@@ -284,9 +284,7 @@ static void run_forward_pass(const mqb_program &p, const SchedDev &sd, size_t pi
         a.batch = batch;
         a.src_batch_stride = src_stride;
         TimeScope ts(TK_FWD, st);
-        ck(jit_launch(jk, &a, 1 << (ps.K - ps.f_reg_bits), jit_forward_smem(ps, p.precision), sm,
-                      (long long)batch << a.g.n_out, st),
-           "generated forward pass");
+        ck(jit_launch_forward<cplx<R>>(jk, a, ps, p.precision, sm, st), "generated forward pass");
         return;
     }
     if (ps.fused) {
@@ -511,9 +509,7 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
             a.n_local_slots = ps.n_slots;
             a.batch = batch;
             TimeScope ts(TK_BWD, st);
-            ck(jit_launch((*jb)[q], &a, 1 << (ps.K - ps.reg_bits), jit_backward_smem(ps, p.precision, n_hams), sm,
-                          (long long)batch << a.g.n_out, st),
-               "generated backward pass");
+            ck(jit_launch_backward<V>((*jb)[q], a, ps, p.precision, n_hams, sm, st), "generated backward pass");
         } else if (ps.fused) {
             Bwd2Args<R> a{};
             a.g = make_geom(p.n, ps.qbits);
@@ -670,6 +666,17 @@ extern "C" {
 const char *mqb_last_error(void) { return g_last_error.c_str(); }
 
 int mqb_version(void) { return 100; }
+
+int mqb_device_error(int *code, int clear) {
+    return guarded([&] {
+        if (!code) fail(MQB_ERR_INVALID, "mqb_device_error: null output");
+        int *w = jit_error_word();
+        ck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        ck(cudaMemcpy(code, w, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+        if (clear) ck(cudaMemset(w, 0, sizeof(int)), "cudaMemset");
+        ck(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    });
+}
 
 int mqb_timing_begin(void) {
     return guarded([&] {

@@ -9,8 +9,14 @@
 // the gates of a stage.
 #include "jit.h"
 
+#include <cuda.h>   // CUtensorMap and its enums; the encoder is fetched from the driver at run time
 #include <cuda_runtime.h>
 #include <nvrtc.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
 
 #include <algorithm>
 #include <atomic>
@@ -23,10 +29,11 @@
 
 namespace mqb {
 
-// Header texts for NVRTC, embedded at build time from regmath.cuh, tile.cuh and jit_abi.h.
+// Header texts for NVRTC, embedded at build time from regmath.cuh, tile.cuh, jit_abi.h and pipe.cuh.
 extern const char *const kJitRegmath;
 extern const char *const kJitTile;
 extern const char *const kJitAbi;
+extern const char *const kJitPipe;
 
 namespace {
 
@@ -54,18 +61,6 @@ std::string lt_expr(const StageDesc &sd, int TB) {
     for (int i = 0; i < TB; ++i) o << " | (((tid >> " << i << ") & 1u) << " << int(sd.tbits[i]) << ")";
     o << ")";
     return o.str();
-}
-
-// Swizzled shared-memory offsets of the thread's register amplitudes (XOR with swz(Lt)).
-std::vector<uint32_t> reg_offsets(const StageDesc &sd, int RB, int precision) {
-    std::vector<uint32_t> off(size_t(1) << RB);
-    for (int j = 0; j < (1 << RB); ++j) {
-        uint32_t L = 0;
-        for (int i = 0; i < RB; ++i)
-            if (j >> i & 1) L |= 1u << sd.rbits[i];
-        off[j] = smem_swizzle(L, precision);
-    }
-    return off;
 }
 
 std::string off_bit_expr(int src, int val) {
@@ -552,71 +547,361 @@ void emit_backward_run(std::ostringstream &o, const std::vector<const StageOp *>
     o << "    }\n";
 }
 
-// Blocks per SM the register budget is sized for: 512 threads per SM at 128 registers each.
-int min_blocks(int TB) { return std::max(1, 512 >> TB); }
+// ------------------------------------------------------------------------- tile movement (TMA)
+// A tile lives in shared memory in one of two layouts: LAY_SWZ, the XOR-swizzled layout of the
+// stage exchanges, and LAY_LAND, the order in which the TMA lands a tile and stores it from.
+enum { LAY_SWZ = 0, LAY_LAND = 1 };
+
+struct PassPlan {
+    TmaGeom tg{};
+    int box_lg[5] = {0, 0, 0, 0, 0};   // log2 of each dimension's box, in amplitudes
+    std::vector<int> land;             // tile bit -> landing-layout bit
+    int precision = MQB_PREC_C64;
+};
+
+// A box holds at most 256 elements per dimension (8-byte elements; complex128 takes two).
+int max_box_bits(int precision) { return precision == MQB_PREC_C64 ? 8 : 7; }
+
+// The tensor-map geometry of a pass's tile: the tile qubits split into runs of consecutive qubits
+// (at most max_box_bits long); the run at qubit 0 and the four longest others become dimensions
+// of the tensor map, the qubits of any further runs are fetched as separate boxes.
+PassPlan pass_plan(const std::vector<int> &qbits, int precision) {
+    PassPlan pl;
+    pl.precision = precision;
+    const int K = int(qbits.size());
+    if (K == 0 || qbits[0] != 0) throw std::runtime_error("generated pass kernel: the tile must hold qubit 0");
+    struct Chunk {
+        int start, len, first;   // first global qubit, length, tile bit of the first qubit
+    };
+    std::vector<Chunk> ch;
+    const int mb = max_box_bits(precision);
+    for (int i = 0; i < K;) {
+        int j = i;
+        while (j + 1 < K && qbits[j + 1] == qbits[j] + 1) ++j;
+        for (int s0 = i; s0 <= j; s0 += mb) ch.push_back({qbits[s0], std::min(mb, j - s0 + 1), s0});
+        i = j + 1;
+    }
+    std::vector<char> keep(ch.size(), 0);
+    keep[0] = 1;
+    std::vector<int> rest;
+    for (size_t k = 1; k < ch.size(); ++k) rest.push_back(int(k));
+    std::stable_sort(rest.begin(), rest.end(), [&](int x, int y) { return ch[x].len > ch[y].len; });
+    for (size_t k = 0; k < rest.size() && k < 4; ++k) keep[rest[k]] = 1;
+    pl.land.assign(K, -1);
+    int pos = 0, nd = 0;
+    for (size_t k = 0; k < ch.size(); ++k) {
+        if (!keep[k]) continue;
+        pl.tg.shift[nd] = ch[k].start;
+        pl.box_lg[nd] = ch[k].len;
+        ++nd;
+        for (int b = 0; b < ch[k].len; ++b) pl.land[ch[k].first + b] = pos++;
+    }
+    const int dim_bits = pos;
+    int nl = 0;
+    for (size_t k = 0; k < ch.size(); ++k) {
+        if (keep[k]) continue;
+        for (int b = 0; b < ch[k].len; ++b) {
+            pl.tg.loop_q[nl++] = ch[k].start + b;
+            pl.land[ch[k].first + b] = pos++;
+        }
+    }
+    pl.tg.nd = nd;
+    pl.tg.n_loop = nl;
+    pl.tg.epa = precision == MQB_PREC_C64 ? 1 : 2;
+    pl.tg.box_bytes = (1 << dim_bits) * elem_bytes(precision);
+    return pl;
+}
+
+uint32_t lay_index(const PassPlan &pl, int lay, uint32_t L) {
+    if (lay == LAY_SWZ) return smem_swizzle(L, pl.precision);
+    uint32_t o = 0;
+    for (size_t i = 0; i < pl.land.size(); ++i)
+        if (L >> i & 1) o |= 1u << pl.land[i];
+    return o;
+}
+
+// Shared-memory index of the thread's base amplitude Lt under a layout, as an expression.
+std::string lay_lt_expr(const PassPlan &pl, int lay, const StageDesc &sd, int TB) {
+    if (lay == LAY_SWZ) return "tile::swz<V>(Lt)";
+    std::ostringstream o;
+    o << "(0u";
+    for (int i = 0; i < TB; ++i) o << " | (((tid >> " << i << ") & 1u) << " << pl.land[sd.tbits[i]] << ")";
+    o << ")";
+    return o.str();
+}
+
+// Whether the lanes of one shared-memory wavefront (a half-warp for 8-byte, a quarter-warp for
+// 16-byte amplitudes) fall on distinct banks when a stage accesses a layout: the lanes' layout
+// offsets must span the low 4 (3) index bits.
+bool lay_conflict_free(const PassPlan &pl, int lay, const StageDesc &sd, int TB) {
+    const int lanes = pl.precision == MQB_PREC_C64 ? 4 : 3;
+    if (TB < lanes) return false;
+    uint32_t rows[4] = {0, 0, 0, 0};
+    for (int i = 0; i < lanes; ++i) rows[i] = lay_index(pl, lay, 1u << sd.tbits[i]) & ((1u << lanes) - 1u);
+    int rank = 0;
+    for (int bit = lanes - 1; bit >= 0; --bit) {
+        int piv = -1;
+        for (int i = rank; i < lanes; ++i)
+            if (rows[i] >> bit & 1) {
+                piv = i;
+                break;
+            }
+        if (piv < 0) continue;
+        std::swap(rows[rank], rows[piv]);
+        for (int i = 0; i < lanes; ++i)
+            if (i != rank && (rows[i] >> bit & 1)) rows[i] ^= rows[rank];
+        ++rank;
+    }
+    return rank == lanes;
+}
+
+// Layouts of the stages of a kernel (in execution order): the first stage reads the landing
+// layout and the last one writes it where that is free of bank conflicts; otherwise the tile is
+// relaid in place (relayout_in / relayout_out) and the stage uses the swizzled layout.
+struct LayPlan {
+    std::vector<int> in, out;
+    bool relayout_in = false, relayout_out = false;
+};
+
+LayPlan plan_layouts(const PassPlan &pl, const std::vector<const StageDesc *> &ex, int TB) {
+    LayPlan lp;
+    const size_t S = ex.size();
+    lp.in.assign(S, LAY_SWZ);
+    lp.out.assign(S, LAY_SWZ);
+    if (lay_conflict_free(pl, LAY_LAND, *ex[0], TB)) lp.in[0] = LAY_LAND;
+    else lp.relayout_in = true;
+    if (lay_conflict_free(pl, LAY_LAND, *ex[S - 1], TB)) lp.out[S - 1] = LAY_LAND;
+    else lp.relayout_out = true;
+    return lp;
+}
+
+// In-place relayout of the n_tiles tiles at `tbase` between the landing and the swizzled layout.
+// Every consumer thread moves 16-byte vectors (two complex64 or one complex128 amplitude): it reads
+// all of its vectors, the consumers meet at a barrier, then it writes them.  Landing slot u holds
+// tile amplitudes L(u) = landing^-1(apv u) (and L(u) ^ 1), L is linear in u, and so is the
+// swizzled position Q(u) = swz(L(u)); a complex64 pair lands swapped where Q(u) is odd.
+void emit_relayout(std::ostringstream &o, const PassPlan &pl, int K, int TB, int n_tiles, bool to_swz) {
+    const int apv = pl.precision == MQB_PREC_C64 ? 2 : 1;
+    const int sh = apv == 2 ? 1 : 0;
+    const int ubits = K - sh, nvec = 1 << (ubits - TB);
+    std::vector<int> inv(K);
+    for (int i = 0; i < K; ++i) inv[pl.land[i]] = i;
+    std::vector<uint32_t> qv(ubits);
+    for (int k = 0; k < ubits; ++k) qv[k] = smem_swizzle(1u << inv[k + sh], pl.precision);
+    o << "   {   // relayout " << (to_swz ? "landing -> swizzled" : "swizzled -> landing") << "\n";
+    o << "    const unsigned qt = 0u";
+    for (int k = 0; k < TB; ++k) o << " ^ (((tid >> " << k << ") & 1u) * " << qv[k] << "u)";
+    o << ";\n    uint4 rv[" << n_tiles * nvec << "];\n";
+    auto qk_of = [&](int k) {
+        uint32_t q = 0;
+        for (int bit = 0; bit < ubits - TB; ++bit)
+            if (k >> bit & 1) q ^= qv[TB + bit];
+        return q;
+    };
+    auto ptr = [&](int r) { return "reinterpret_cast<uint4 *>(tbase + " + std::to_string(r) + " * TS)"; };
+    for (int r = 0; r < n_tiles; ++r)
+        for (int k = 0; k < nvec; ++k) {
+            const int idx = r * nvec + k;
+            if (to_swz) o << "    rv[" << idx << "] = " << ptr(r) << "[tid + " << (k << TB) << "u];\n";
+            else o << "    rv[" << idx << "] = " << ptr(r) << "[(qt ^ " << qk_of(k) << "u) >> " << sh << "];\n";
+        }
+    o << "    pipe::consumers_sync(NT);\n";
+    for (int r = 0; r < n_tiles; ++r)
+        for (int k = 0; k < nvec; ++k) {
+            const int idx = r * nvec + k;
+            if (apv == 2)
+                o << "    if ((qt ^ " << qk_of(k) << "u) & 1u) rv[" << idx << "] = make_uint4(rv[" << idx << "].z, rv[" << idx
+                  << "].w, rv[" << idx << "].x, rv[" << idx << "].y);\n";
+            if (to_swz) o << "    " << ptr(r) << "[(qt ^ " << qk_of(k) << "u) >> " << sh << "] = rv[" << idx << "];\n";
+            else o << "    " << ptr(r) << "[tid + " << (k << TB) << "u] = rv[" << idx << "];\n";
+        }
+    o << "    pipe::consumers_sync(NT);\n   }\n";
+}
+
+// Buffers of the tile ring: the forward kernels keep two (three blocks per SM at 2^12 complex64),
+// the adjoint kernels as many as fit beside one block's tables (up to three).  The environment
+// variables MQB_PIPE_FWD_BUFFERS / MQB_PIPE_BWD_BUFFERS override the counts (tuning).
+int fwd_buffers() {
+    const char *e = std::getenv("MQB_PIPE_FWD_BUFFERS");
+    return e ? std::max(1, std::min(4, std::atoi(e))) : 2;
+}
+
+size_t bwd_fixed_smem(const Pass &p, int precision, int n_hams) {
+    const size_t eb = elem_bytes(precision);
+    const int nw = (1 << (p.K - p.reg_bits)) / 32;
+    return a16(size_t(p.mtab_entries) * eb) + a16(size_t(nw) * std::max(1, p.n_slots) * n_hams * sizeof(double)) + 8 * 8;
+}
+
+int bwd_buffers(const Pass &p, int precision, int n_hams) {
+    const size_t buf = (size_t(1) << p.K) * elem_bytes(precision) * (1 + n_hams);
+    const size_t fixed = bwd_fixed_smem(p, precision, n_hams);
+    int nb = 1;
+    while (nb < 3 && (nb + 1) * buf + fixed <= size_t(200) << 10) ++nb;
+    if (const char *e = std::getenv("MQB_PIPE_BWD_BUFFERS")) {
+        int want = std::max(1, std::min(4, std::atoi(e)));
+        while (want > 1 && want * buf + fixed > size_t(227) << 10) --want;
+        nb = want;
+    }
+    return nb;
+}
 
 void emit_header(std::ostringstream &o, int precision) {
-    o << "#include \"regmath.cuh\"\n#include \"tile.cuh\"\n"
+    o << "#include \"regmath.cuh\"\n#include \"tile.cuh\"\n#include \"pipe.cuh\"\n"
       << "using namespace mqb;\nusing namespace mqb::reg;\n"
       << "typedef " << vname(precision) << " V;\ntypedef " << rname(precision) << " R;\n";
 }
 
-void emit_stage_load(std::ostringstream &o, const StageDesc &sd, int RB, int TB, int precision, int NH) {
-    const auto off = reg_offsets(sd, RB, precision);
-    o << "   {\n    const unsigned Lt = " << lt_expr(sd, TB) << ";\n"
-      << "    const unsigned pLt = tile::swz<V>(Lt);\n    V v[NR];\n";
-    if (NH) o << "    V l[NH][NR];\n";
-    for (int j = 0; j < (1 << RB); ++j) {
-        if (NH) {
-            o << "    v[" << j << "] = psi[pLt ^ " << off[j] << "u];";
-            o << " for (int h = 0; h < NH; ++h) l[h][" << j << "] = lam[h * TS + (pLt ^ " << off[j] << "u)];\n";
-        } else {
-            o << "    v[" << j << "] = tl[pLt ^ " << off[j] << "u];\n";
-        }
-    }
+uint32_t reg_local(const StageDesc &sd, int RB, int j) {
+    uint32_t L = 0;
+    for (int i = 0; i < RB; ++i)
+        if (j >> i & 1) L |= 1u << sd.rbits[i];
+    return L;
 }
 
-void emit_stage_store(std::ostringstream &o, const StageDesc &sd, int RB, int precision, int NH) {
-    const auto off = reg_offsets(sd, RB, precision);
+void emit_stage_load(std::ostringstream &o, const PassPlan &pl, const StageDesc &sd, int RB, int TB, int NH, int lay,
+                     bool zero_start) {
+    o << "   {\n    const unsigned Lt = " << lt_expr(sd, TB) << ";\n"
+      << "    const unsigned pLt = " << lay_lt_expr(pl, lay, sd, TB) << ";\n    V v[NR];\n";
+    if (NH) o << "    V l[NH][NR];\n";
+    if (zero_start) {
+        o << "    if (zero) {\n      v[0] = (base == 0 && Lt == 0u) ? cval<V>(1, 0) : cval<V>(0, 0);\n";
+        for (int j = 1; j < (1 << RB); ++j) o << "      v[" << j << "] = cval<V>(0, 0);\n";
+        o << "    } else {\n";
+    }
     for (int j = 0; j < (1 << RB); ++j) {
+        const uint32_t off = lay_index(pl, lay, reg_local(sd, RB, j));
         if (NH) {
-            o << "    psi[pLt ^ " << off[j] << "u] = v[" << j << "];";
-            o << " for (int h = 0; h < NH; ++h) lam[h * TS + (pLt ^ " << off[j] << "u)] = l[h][" << j << "];\n";
+            o << "    v[" << j << "] = psi[pLt ^ " << off << "u];";
+            o << " for (int h = 0; h < NH; ++h) l[h][" << j << "] = lam[h * TS + (pLt ^ " << off << "u)];\n";
         } else {
-            o << "    tl[pLt ^ " << off[j] << "u] = v[" << j << "];\n";
+            o << "    v[" << j << "] = tl[pLt ^ " << off << "u];\n";
         }
     }
-    o << "    __syncthreads();\n   }\n";
+    if (zero_start) o << "    }\n";
+}
+
+void emit_stage_store(std::ostringstream &o, const PassPlan &pl, const StageDesc &sd, int RB, int TB, int NH, int lay_in,
+                      int lay_out, bool barrier_after) {
+    if (lay_out != lay_in)
+        o << "    pipe::consumers_sync(NT);\n    const unsigned pLo = " << lay_lt_expr(pl, lay_out, sd, TB) << ";\n";
+    else
+        o << "    const unsigned pLo = pLt;\n";
+    for (int j = 0; j < (1 << RB); ++j) {
+        const uint32_t off = lay_index(pl, lay_out, reg_local(sd, RB, j));
+        if (NH) {
+            o << "    psi[pLo ^ " << off << "u] = v[" << j << "];";
+            o << " for (int h = 0; h < NH; ++h) lam[h * TS + (pLo ^ " << off << "u)] = l[h][" << j << "];\n";
+        } else {
+            o << "    tl[pLo ^ " << off << "u] = v[" << j << "];\n";
+        }
+    }
+    if (barrier_after) o << "    pipe::consumers_sync(NT);\n";
+    o << "   }\n";
+}
+
+// Producer (one thread of the extra warp): the tile ring's loads and stores.  `load_body` issues
+// the copies of tile k into buffer sb, `store_body` those of tile i from buffer sb; both see
+// b (sample) and tb (the tile's outside bits).  A buffer is handed to the consumers through its
+// `full` barrier: with the TMA's transaction bytes, or (forward passes that start from |0...0>
+// and load nothing) with a plain arrival once the buffer's previous store has been read out.
+void emit_producer(std::ostringstream &o, const std::string &load_body, const std::string &store_body, bool zero_opt) {
+    o << "  if (tid >= NT) {\n   if (tid == NT) {\n"
+      << "    const long long first = blockIdx.x, cnt = first < total ? (total - 1 - first) / gridDim.x + 1 : 0;\n"
+      << "    const int n = a.g.n;\n"
+      << "    auto tile_of = [&](long long k, long long &b, tile::u64 &tb) {\n"
+      << "     const long long w = first + k * gridDim.x;\n"
+      << "     b = w >> a.g.n_out;\n"
+      << "     tb = tile::tile_base(a.g, tile::u64(w) & tile::u64(n_tiles - 1));\n"
+      << "    };\n"
+      << "    auto load = [&](long long k) {\n"
+      << "     const int sb = int(k % NB);\n     long long b;\n     tile::u64 tb;\n     tile_of(k, b, tb);\n"
+      << "     unsigned char *buf = smem + sb * BUFB;\n";
+    if (zero_opt) o << "     if (zero) {\n      pipe::mbar_arrive(full + sb);\n      return;\n     }\n";
+    o << "     pipe::mbar_expect_tx(full + sb, BUFB);\n"
+      << load_body << "    };\n"
+      << "    long long issued = 0, i = 0;\n    bool ok = true;\n"
+      << "    for (; issued < cnt && issued < NB; ++issued) load(issued);\n"
+      << "    for (; i < cnt; ++i) {\n"
+      << "     const int sb = int(i % NB);\n"
+      << "     if (!pipe::mbar_wait(done + sb, unsigned(i / NB) & 1u)) {\n"
+      << "      pipe::report(a.err, MQB_DEV_ERR_TIMEOUT);\n      ok = false;\n      break;\n     }\n"
+      << "     long long b;\n     tile::u64 tb;\n     tile_of(i, b, tb);\n"
+      << "     const unsigned char *buf = smem + sb * BUFB;\n"
+      << store_body
+      << "     pipe::bulk_commit();\n"
+      << "     if (issued < cnt) {\n      pipe::bulk_wait_read_all();\n      load(issued);\n      ++issued;\n     }\n"
+      << "    }\n"
+      << "    if (!ok)   // let the loads still in flight land before the block exits\n"
+      << "     for (long long k = i; k < issued; ++k) pipe::mbar_wait(full + k % NB, unsigned(k / NB) & 1u);\n"
+      << "    pipe::bulk_wait_all();\n"
+      << "   }\n   return;\n  }\n";
+}
+
+// Consumers' wait for buffer sb of tile i: one thread polls the mbarrier, the outcome is shared
+// through a barrier reduction, then every thread observes the completed phase itself.
+void emit_consumer_wait(std::ostringstream &o, const std::string &indent) {
+    o << indent << "if (!pipe::consumers_and(NT, tid != 0u || pipe::mbar_wait(full + sb, par))) {\n"
+      << indent << " if (tid == 0u) pipe::report(a.err, MQB_DEV_ERR_TIMEOUT);\n"
+      << indent << " break;\n"
+      << indent << "}\n"
+      << indent << "pipe::mbar_test(full + sb, par);\n";
+}
+
+size_t fwd_smem(const Pass &p, int precision) {
+    const size_t eb = elem_bytes(precision);
+    return size_t(fwd_buffers()) * ((size_t(1) << p.K) * eb) + a16(size_t(p.f_mtab_entries) * eb) + 8 * 8;
 }
 
 std::string forward_source(const Schedule &s, const Pass &p, int precision) {
     const int RB = p.f_reg_bits, K = p.K, TB = K - RB;
+    const PassPlan pl = pass_plan(p.qbits, precision);
+    const int NB = fwd_buffers();
+    std::vector<const StageDesc *> ex;
+    for (int si = 0; si < p.f_n_stages; ++si) ex.push_back(&s.f_stages[p.f_stage_begin + si]);
+    const LayPlan lp = plan_layouts(pl, ex, TB);
+    // blocks per SM that the shared-memory ring allows: the register budget is sized for them
+    const int min_blocks = int(std::max<size_t>(1, std::min<size_t>(3, (size_t(220) << 10) / fwd_smem(p, precision))));
     std::ostringstream o;
     emit_header(o, precision);
-    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) << ", " << min_blocks(TB)
-      << ") mqb_fwd_pass(const JitFwdArgs<V> a) {\n"
-      << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", C = " << p.c << ";\n"
-      << "  constexpr int NV = NR / (16 / int(sizeof(V)));\n"
-      << "  extern __shared__ __align__(16) unsigned char smem[];\n"
-      << "  V *tl = reinterpret_cast<V *>(smem);\n"
-      << "  tile::u64 o = tile::align16((tile::u64(1) << K) * sizeof(V));\n"
-      << "  V *mt = reinterpret_cast<V *>(smem + o);\n"
-      << "  o = tile::align16(o + tile::u64(a.mtab_entries) * sizeof(V));\n"
-      << "  tile::u64 *tab = reinterpret_cast<tile::u64 *>(smem + o);\n"
-      << "  tile::build_table(tab, a.g);\n  __syncthreads();\n"
+    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) + 32 << ", " << min_blocks
+      << ") mqb_fwd_pass(const JitFwdArgs<V> a, "
+      << "const __grid_constant__ pipe::TMap m_src, const __grid_constant__ pipe::TMap m_dst) {\n"
+      << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", NT = 1 << (K - RB), NB = " << NB
+      << ", TS = 1 << K;\n"
+      << "  constexpr unsigned BUFB = TS * sizeof(V);\n"
+      << "  extern __shared__ __align__(1024) unsigned char smem[];\n"
+      << "  V *mt = reinterpret_cast<V *>(smem + NB * BUFB);\n"
+      << "  pipe::u64 *full = reinterpret_cast<pipe::u64 *>(smem + NB * BUFB + tile::align16(tile::u64(a.mtab_entries) * "
+         "sizeof(V)));\n"
+      << "  pipe::u64 *done = full + NB;\n"
       << "  const unsigned tid = threadIdx.x;\n"
-      << "  const long long n_tiles = 1ll << a.g.n_out, dim = 1ll << a.g.n;\n"
-      << "  long long cached_b = -1;\n"
-      << "  for (long long w = blockIdx.x; w < a.batch * n_tiles; w += gridDim.x) {\n"
+      << "  if (tid == 0) {\n   for (int k = 0; k < NB; ++k) {\n    pipe::mbar_init(full + k, 1);\n"
+      << "    pipe::mbar_init(done + k, NT);\n   }\n   pipe::fence_mbar_init();\n  }\n  __syncthreads();\n"
+      << "  const long long n_tiles = 1ll << a.g.n_out, total = a.batch * n_tiles;\n"
+      << "  const bool zero = a.src == nullptr;\n";
+    emit_producer(o,
+                  "     const tile::u64 bs = a.src_batch_stride ? tile::u64(b) : 0;\n"
+                  "     pipe::load_tile(&m_src, a.tg, (bs << n) | tb, buf, full + sb);\n",
+                  "     pipe::store_tile(&m_dst, a.tg, (tile::u64(b) << n) | tb, buf);\n", true);
+    o << "  long long cached_b = -1, i = 0;\n"
+      << "  for (long long w = blockIdx.x; w < total; w += gridDim.x, ++i) {\n"
       << "   const long long b = w >> a.g.n_out;\n"
       << "   const tile::u64 base = tile::tile_base(a.g, tile::u64(w) & tile::u64(n_tiles - 1));\n"
-      << "   if (b != cached_b) {\n    tile::load_mtab(mt, a.mt, a.n_mt, a.mats + b * a.mats_stride, a.cpool);\n"
-      << "    cached_b = b;\n   }\n"
-      << "   if (a.src) tile::stage_in<V, NV>(tl, a.src + b * a.src_batch_stride, base, tab, C);\n"
-      << "   else tile::stage_zero(tl, base, K);\n   __syncthreads();\n";
-    for (int si = 0; si < p.f_n_stages; ++si) {
-        const StageDesc &sd = s.f_stages[p.f_stage_begin + si];
-        emit_stage_load(o, sd, RB, TB, precision, 0);
+      << "   const int sb = int(i % NB);\n   const unsigned par = unsigned(i / NB) & 1u;\n"
+      << "   V *tl = reinterpret_cast<V *>(smem + sb * BUFB);\n"
+      << "   if (b != cached_b) {\n    pipe::consumers_sync(NT);\n"
+      << "    pipe::load_mtab(mt, a.mt, a.n_mt, a.mats + b * a.mats_stride, a.cpool, tid, NT);\n"
+      << "    cached_b = b;\n    pipe::consumers_sync(NT);\n   }\n";
+    emit_consumer_wait(o, "   ");
+    if (lp.relayout_in) {
+        o << "   if (!zero) {\n    V *tbase = tl;\n";
+        emit_relayout(o, pl, K, TB, 1, true);
+        o << "   }\n";
+    }
+    for (size_t si = 0; si < ex.size(); ++si) {
+        const StageDesc &sd = *ex[si];
+        const bool last = si + 1 == ex.size();
+        emit_stage_load(o, pl, sd, RB, TB, 0, lp.in[si], si == 0);
         for (int k = sd.op_begin; k < sd.op_end;) {
             std::vector<const StageOp *> run;
             int e = k;
@@ -629,47 +914,74 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
                 ++k;
             }
         }
-        emit_stage_store(o, sd, RB, precision, 0);
+        emit_stage_store(o, pl, sd, RB, TB, 0, lp.in[si], lp.out[si], !last || lp.relayout_out);
     }
-    o << "   tile::stage_out<V, NV>(tl, a.dst + b * dim, base, tab, C);\n   __syncthreads();\n  }\n}\n";
+    if (lp.relayout_out) {
+        o << "   {\n    V *tbase = tl;\n";
+        emit_relayout(o, pl, K, TB, 1, false);
+        o << "   }\n";
+    }
+    o << "   pipe::fence_async_smem();\n   pipe::mbar_arrive(done + sb);\n  }\n}\n";
     return o.str();
 }
 
 std::string backward_source(const Schedule &s, const Pass &p, int precision, int NH, const std::vector<DevOp> &ops) {
     const int RB = p.reg_bits, K = p.K, TB = K - RB;
     const int NLS = std::max(1, p.n_slots);
+    const PassPlan pl = pass_plan(p.qbits, precision);
+    const int NB = bwd_buffers(p, precision, NH);
+    std::vector<const StageDesc *> ex;
+    for (int si = p.n_stages - 1; si >= 0; --si) ex.push_back(&s.stages[p.stage_begin + si]);
+    const LayPlan lp = plan_layouts(pl, ex, TB);
     std::ostringstream o;
     emit_header(o, precision);
-    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) << ", " << min_blocks(TB)
-      << ") mqb_adj_pass(const JitBwdArgs<V> a) {\n"
-      << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", C = " << p.c << ", NH = " << NH
-      << ", NLS = " << NLS << ", TS = 1 << K;\n"
-      << "  constexpr int NV = NR / (16 / int(sizeof(V)));\n"
-      << "  extern __shared__ __align__(16) unsigned char smem[];\n"
-      << "  V *psi = reinterpret_cast<V *>(smem);\n  V *lam = psi + TS;\n"
-      << "  tile::u64 o = tile::align16(tile::u64(TS) * sizeof(V) * (1 + NH));\n"
+    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) + 32 << ", 1) mqb_adj_pass(const JitBwdArgs<V> a, "
+      << "const __grid_constant__ pipe::TMap m_psi, const __grid_constant__ pipe::TMap m_lam, "
+      << "const __grid_constant__ pipe::TMap m_pdst) {\n"
+      << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", NH = " << NH << ", NLS = " << NLS
+      << ", TS = 1 << K, NT = 1 << (K - RB), NB = " << NB << ";\n"
+      << "  constexpr unsigned TILEB = TS * sizeof(V), BUFB = TILEB * (1 + NH);\n"
+      << "  extern __shared__ __align__(1024) unsigned char smem[];\n"
+      << "  tile::u64 o = tile::u64(NB) * BUFB;\n"
       << "  V *mt = reinterpret_cast<V *>(smem + o);\n"
       << "  o = tile::align16(o + tile::u64(a.mtab_entries) * sizeof(V));\n"
-      << "  tile::u64 *tab = reinterpret_cast<tile::u64 *>(smem + o);\n"
-      << "  o = tile::align16(o + (tile::u64(1) << (K - C)) * sizeof(tile::u64));\n"
       << "  double *wacc = reinterpret_cast<double *>(smem + o);\n"
-      << "  const int nw = blockDim.x / 32, warp = threadIdx.x / 32, lane = threadIdx.x % 32;\n"
-      << "  tile::build_table(tab, a.g);\n"
-      << "  for (int i = threadIdx.x; i < nw * NLS * NH; i += blockDim.x) wacc[i] = 0;\n  __syncthreads();\n"
+      << "  o = tile::align16(o + tile::u64(NT / 32) * NLS * NH * sizeof(double));\n"
+      << "  pipe::u64 *full = reinterpret_cast<pipe::u64 *>(smem + o), *done = full + NB;\n"
       << "  const unsigned tid = threadIdx.x;\n"
-      << "  const long long n_tiles = 1ll << a.g.n_out, dim = 1ll << a.g.n, total = a.batch * n_tiles;\n"
-      << "  long long cached_b = -1;\n"
-      << "  for (long long w = blockIdx.x; w < total; w += gridDim.x) {\n"
+      << "  const int nw = NT / 32, warp = int(tid) / 32, lane = int(tid) % 32;\n"
+      << "  if (tid == 0) {\n   for (int k = 0; k < NB; ++k) {\n    pipe::mbar_init(full + k, 1);\n"
+      << "    pipe::mbar_init(done + k, NT);\n   }\n   pipe::fence_mbar_init();\n  }\n"
+      << "  for (int i = int(tid); i < nw * NLS * NH; i += int(blockDim.x)) wacc[i] = 0;\n  __syncthreads();\n"
+      << "  const long long n_tiles = 1ll << a.g.n_out, total = a.batch * n_tiles;\n";
+    emit_producer(o,
+                  "     pipe::load_tile(&m_psi, a.tg, (tile::u64(b) << n) | tb, buf, full + sb);\n"
+                  "     for (int h = 0; h < NH; ++h)\n"
+                  "      pipe::load_tile(&m_lam, a.tg, (tile::u64(h * a.batch + b) << n) | tb, buf + (1 + h) * TILEB, "
+                  "full + sb);\n",
+                  "     for (int h = 0; h < NH; ++h)\n"
+                  "      pipe::store_tile(&m_lam, a.tg, (tile::u64(h * a.batch + b) << n) | tb, buf + (1 + h) * TILEB);\n"
+                  "     if (a.psi_dst) pipe::store_tile(&m_pdst, a.tg, (tile::u64(b) << n) | tb, buf);\n",
+                  false);
+    o << "  long long cached_b = -1, i = 0;\n"
+      << "  for (long long w = blockIdx.x; w < total; w += gridDim.x, ++i) {\n"
       << "   const long long b = w >> a.g.n_out;\n"
       << "   const tile::u64 base = tile::tile_base(a.g, tile::u64(w) & tile::u64(n_tiles - 1));\n"
-      << "   if (b != cached_b) {\n    tile::load_mtab(mt, a.mt, a.n_mt, a.mats + b * a.mats_stride, a.cpool);\n"
-      << "    cached_b = b;\n   }\n"
-      << "   tile::stage_in<V, NV>(psi, a.psi_src + b * dim, base, tab, C);\n"
-      << "   for (int h = 0; h < NH; ++h) tile::stage_in<V, NV>(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, C);\n"
-      << "   __syncthreads();\n";
-    for (int si = p.n_stages - 1; si >= 0; --si) {
-        const StageDesc &sd = s.stages[p.stage_begin + si];
-        emit_stage_load(o, sd, RB, TB, precision, NH);
+      << "   const int sb = int(i % NB);\n   const unsigned par = unsigned(i / NB) & 1u;\n"
+      << "   V *psi = reinterpret_cast<V *>(smem + sb * BUFB);\n   V *lam = psi + TS;\n"
+      << "   if (b != cached_b) {\n    pipe::consumers_sync(NT);\n"
+      << "    pipe::load_mtab(mt, a.mt, a.n_mt, a.mats + b * a.mats_stride, a.cpool, tid, NT);\n"
+      << "    cached_b = b;\n    pipe::consumers_sync(NT);\n   }\n";
+    emit_consumer_wait(o, "   ");
+    if (lp.relayout_in) {
+        o << "   {\n    V *tbase = psi;\n";
+        emit_relayout(o, pl, K, TB, 1 + NH, true);
+        o << "   }\n";
+    }
+    for (size_t si = 0; si < ex.size(); ++si) {
+        const StageDesc &sd = *ex[si];
+        const bool last = si + 1 == ex.size();
+        emit_stage_load(o, pl, sd, RB, TB, NH, lp.in[si], false);
         for (int k = sd.op_end - 1; k >= sd.op_begin;) {
             std::vector<const StageOp *> run;
             std::vector<int> gids;
@@ -690,29 +1002,40 @@ std::string backward_source(const Schedule &s, const Pass &p, int precision, int
                 --k;
             }
         }
-        emit_stage_store(o, sd, RB, precision, NH);
+        emit_stage_store(o, pl, sd, RB, TB, NH, lp.in[si], lp.out[si], !last || lp.relayout_out);
     }
-    o << "   for (int h = 0; h < NH; ++h) tile::stage_out<V, NV>(lam + h * TS, a.lam + (h * a.batch + b) * dim, base, tab, C);\n"
-      << "   if (a.psi_dst) tile::stage_out<V, NV>(psi, a.psi_dst + b * dim, base, tab, C);\n"
+    if (lp.relayout_out) {
+        o << "   {\n    V *tbase = psi;\n";
+        emit_relayout(o, pl, K, TB, 1 + NH, false);
+        o << "   }\n";
+    }
+    o << "   pipe::fence_async_smem();\n   pipe::mbar_arrive(done + sb);\n"
       << "   const long long nxt = w + gridDim.x;\n"
-      << "   const bool flush = (nxt >= total) || ((nxt >> a.g.n_out) != b);\n"
-      << "   __syncthreads();\n"
-      << "   if (flush) {\n"
-      << "    for (int i = threadIdx.x; i < a.n_local_slots * NH; i += blockDim.x) {\n"
+      << "   if ((nxt >= total) || ((nxt >> a.g.n_out) != b)) {\n"
+      << "    pipe::consumers_sync(NT);\n"
+      << "    for (int i = int(tid); i < a.n_local_slots * NH; i += NT) {\n"
       << "     double sum = 0;\n"
       << "     for (int ww = 0; ww < nw; ++ww) {\n"
       << "      sum += wacc[ww * NLS * NH + i];\n      wacc[ww * NLS * NH + i] = 0;\n     }\n"
       << "     const int ls = i / NH, h = i % NH;\n"
       << "     if (sum != 0) atomicAdd(&a.gslots[(b * a.n_slots + a.slot_map[ls]) * a.n_hams + h], sum);\n"
-      << "    }\n    __syncthreads();\n   }\n  }\n}\n";
+      << "    }\n    pipe::consumers_sync(NT);\n   }\n  }\n}\n";
     return o.str();
 }
 
 void compile_entry(Entry &e) {
+    // MQB_JIT_DUMP=<directory>: write every generated source there (for reading them)
+    if (const char *dir = std::getenv("MQB_JIT_DUMP")) {
+        const std::string path = std::string(dir) + "/mqb_pass_" + std::to_string(std::hash<std::string>()(e.src)) + ".cu";
+        if (FILE *f = std::fopen(path.c_str(), "w")) {
+            std::fwrite(e.src.data(), 1, e.src.size(), f);
+            std::fclose(f);
+        }
+    }
     nvrtcProgram prog = nullptr;
-    const char *hdrs[3] = {kJitRegmath, kJitTile, kJitAbi};
-    const char *names[3] = {"regmath.cuh", "tile.cuh", "jit_abi.h"};
-    if (nvrtcCreateProgram(&prog, e.src.c_str(), "mqb_pass.cu", 3, hdrs, names) != NVRTC_SUCCESS) {
+    const char *hdrs[4] = {kJitRegmath, kJitTile, kJitAbi, kJitPipe};
+    const char *names[4] = {"regmath.cuh", "tile.cuh", "jit_abi.h", "pipe.cuh"};
+    if (nvrtcCreateProgram(&prog, e.src.c_str(), "mqb_pass.cu", 4, hdrs, names) != NVRTC_SUCCESS) {
         e.log = "nvrtcCreateProgram failed";
         return;
     }
@@ -830,34 +1153,132 @@ int jit_compile_check(const Schedule &s, int precision, int n_hams, const std::v
     return int(es.size());
 }
 
-size_t jit_forward_smem(const Pass &p, int precision) {
-    const size_t eb = elem_bytes(precision);
-    size_t o = a16((size_t(1) << p.K) * eb);
-    o = a16(o + size_t(p.f_mtab_entries) * eb);
-    return o + (size_t(1) << (p.K - p.c)) * 8;
-}
+size_t jit_forward_smem(const Pass &p, int precision) { return fwd_smem(p, precision); }
 
 size_t jit_backward_smem(const Pass &p, int precision, int n_hams) {
-    const size_t eb = elem_bytes(precision);
-    const int threads = 1 << (p.K - p.reg_bits);
-    size_t o = a16((size_t(1) << p.K) * eb * (1 + n_hams));
-    o = a16(o + size_t(p.mtab_entries) * eb);
-    o = a16(o + (size_t(1) << (p.K - p.c)) * 8);
-    return o + size_t(threads / 32) * std::max(1, p.n_slots) * n_hams * sizeof(double);
+    const size_t buf = (size_t(1) << p.K) * elem_bytes(precision) * (1 + n_hams);
+    return size_t(bwd_buffers(p, precision, n_hams)) * buf + bwd_fixed_smem(p, precision, n_hams);
 }
 
-cudaError_t jit_launch(const void *kernel, void *args, int threads, size_t smem, int sm_count, long long work,
-                       cudaStream_t st) {
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled, taken from the driver through the runtime (the library does not link
+// libcuda itself).
+EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(f);
+    });
+    if (!fn) throw std::runtime_error("generated pass kernel: cuTensorMapEncodeTiled is not available from the driver");
+    return fn;
+}
+
+// Tensor map of the amplitudes at `base` ([outer][2^n]) for the tiles of plan pl: dimension j
+// holds the index bits [shift[j], shift[j+1]) (the last one all bits above, times outer), its box
+// the tile qubits at the bottom of that range.
+void encode_map(CUtensorMap *m, const void *base, int n, long long outer, const PassPlan &pl) {
+    std::memset(m, 0, sizeof(*m));
+    if (!base) return;   // a map the kernel never uses (no such buffer in this launch)
+    const TmaGeom &t = pl.tg;
+    cuuint64_t dims[5], strides[4];
+    cuuint32_t box[5], es[5];
+    const uint64_t eb = 8;   // tensor elements: 8-byte words
+    for (int j = 0; j < t.nd; ++j) {
+        const int lo = t.shift[j], hi = j + 1 < t.nd ? t.shift[j + 1] : n;
+        uint64_t d = (uint64_t(1) << (hi - lo)) * (j == 0 ? uint64_t(t.epa) : 1);
+        if (j + 1 == t.nd) d *= uint64_t(outer);
+        if (d > (uint64_t(1) << 32)) throw std::runtime_error("generated pass kernel: tensor dimension above 2^32");
+        dims[j] = d;
+        box[j] = (1u << pl.box_lg[j]) * (j == 0 ? unsigned(t.epa) : 1u);
+        es[j] = 1;
+        if (j > 0) strides[j - 1] = (uint64_t(1) << lo) * eb * uint64_t(t.epa);
+    }
+    const CUresult r = tensor_map_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, cuuint32_t(t.nd), const_cast<void *>(base),
+                                            dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        throw std::runtime_error("generated pass kernel: cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+}
+
+std::mutex g_err_mu;
+int *g_err_word[64] = {nullptr};
+
+cudaError_t launch_pipe(const void *kernel, void **argv, int threads, size_t smem, int sm_count, long long work,
+                        cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     const long long blocks = std::max<long long>(1, std::min<long long>((long long)sm_count * per_sm, work));
-    void *argv[] = {args};
     e = cudaLaunchKernel(kernel, dim3(unsigned(blocks)), dim3(unsigned(threads)), argv, smem, st);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
+
+}  // namespace
+
+int *jit_error_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) throw std::runtime_error("jit_error_word: no device");
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    if (!g_err_word[dev]) {
+        int *w = nullptr;
+        if (cudaMalloc(&w, sizeof(int)) != cudaSuccess || cudaMemset(w, 0, sizeof(int)) != cudaSuccess ||
+            cudaDeviceSynchronize() != cudaSuccess)
+            throw std::runtime_error("jit_error_word: allocating the error word failed");
+        g_err_word[dev] = w;
+    }
+    return g_err_word[dev];
+}
+
+template <typename V>
+cudaError_t jit_launch_forward(const void *kernel, JitFwdArgs<V> a, const Pass &p, int precision, int sm_count,
+                               cudaStream_t st) {
+    const PassPlan pl = pass_plan(p.qbits, precision);
+    const long long dim = 1ll << a.g.n;
+    if (a.src && a.src_batch_stride != 0 && a.src_batch_stride != dim)
+        throw std::runtime_error("generated forward pass: source batch stride must be 0 or the state size");
+    a.tg = pl.tg;
+    a.err = jit_error_word();
+    CUtensorMap ms, md;
+    encode_map(&ms, a.src, a.g.n, a.src_batch_stride ? a.batch : 1, pl);
+    encode_map(&md, a.dst, a.g.n, a.batch, pl);
+    void *argv[] = {&a, &ms, &md};
+    return launch_pipe(kernel, argv, (1 << (p.K - p.f_reg_bits)) + 32, jit_forward_smem(p, precision), sm_count,
+                       a.batch << a.g.n_out, st);
+}
+
+template <typename V>
+cudaError_t jit_launch_backward(const void *kernel, JitBwdArgs<V> a, const Pass &p, int precision, int n_hams,
+                                int sm_count, cudaStream_t st) {
+    const PassPlan pl = pass_plan(p.qbits, precision);
+    a.tg = pl.tg;
+    a.err = jit_error_word();
+    CUtensorMap mp, ml, md;
+    encode_map(&mp, a.psi_src, a.g.n, a.batch, pl);
+    encode_map(&ml, a.lam, a.g.n, a.batch * n_hams, pl);
+    encode_map(&md, a.psi_dst, a.g.n, a.batch, pl);
+    void *argv[] = {&a, &mp, &ml, &md};
+    return launch_pipe(kernel, argv, (1 << (p.K - p.reg_bits)) + 32, jit_backward_smem(p, precision, n_hams), sm_count,
+                       a.batch << a.g.n_out, st);
+}
+
+template cudaError_t jit_launch_forward<float2>(const void *, JitFwdArgs<float2>, const Pass &, int, int, cudaStream_t);
+template cudaError_t jit_launch_forward<double2>(const void *, JitFwdArgs<double2>, const Pass &, int, int, cudaStream_t);
+template cudaError_t jit_launch_backward<float2>(const void *, JitBwdArgs<float2>, const Pass &, int, int, int,
+                                                 cudaStream_t);
+template cudaError_t jit_launch_backward<double2>(const void *, JitBwdArgs<double2>, const Pass &, int, int, int,
+                                                  cudaStream_t);
 
 }  // namespace mqb

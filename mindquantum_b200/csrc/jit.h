@@ -23,9 +23,19 @@ std::vector<const void *> jit_backward_kernels(const Schedule &s, int precision,
 size_t jit_forward_smem(const Pass &p, int precision);
 size_t jit_backward_smem(const Pass &p, int precision, int n_hams);
 
-// Launch a generated kernel over `work` tiles with 2^(K - RB) threads.
-cudaError_t jit_launch(const void *kernel, void *args, int threads, size_t smem, int sm_count, long long work,
-                       cudaStream_t st);
+// Launch the generated kernel of pass p over every tile of the batch: 2^(K - RB) consumer threads
+// plus one producer warp, the TMA tensor maps of the launch's buffers encoded here, and the
+// kernel's error word filled in (jit_error_word).
+template <typename V>
+cudaError_t jit_launch_forward(const void *kernel, JitFwdArgs<V> a, const Pass &p, int precision, int sm_count,
+                               cudaStream_t st);
+template <typename V>
+cudaError_t jit_launch_backward(const void *kernel, JitBwdArgs<V> a, const Pass &p, int precision, int n_hams,
+                                int sm_count, cudaStream_t st);
+
+// The error word the generated kernels of the current device report to (MQB_DEV_ERR_*; 0: none),
+// allocated on first use.
+int *jit_error_word();
 
 // Generate and compile (without loading: no GPU needed) the kernels of every fused pass, the
 // backward ones too when n_hams > 0; returns the number of distinct kernels.

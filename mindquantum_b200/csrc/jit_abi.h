@@ -16,6 +16,23 @@ struct TileGeom {
     signed char outside[64];
 };
 
+// How the TMA moves one tile: the state (and the batch above it) is seen as a tensor of nd <= 5
+// dimensions; dimension j holds the global index bits [shift[j], shift[j+1]) (the last one also
+// the batch), and its box covers the tile qubits at the bottom of that range.  Tile qubits that
+// got no dimension (n_loop of them, at most when a tile has more than five qubit ranges) are
+// fetched as 2^n_loop separate boxes, box v at shared offset v * box_bytes.
+struct TmaGeom {
+    int nd;
+    int n_loop;
+    int epa;                // 8-byte tensor elements per amplitude (complex64 1, complex128 2)
+    int box_bytes;
+    int shift[5];
+    int loop_q[13];
+};
+
+// Error codes the generated kernels leave in their error word (0: none).
+enum { MQB_DEV_ERR_TIMEOUT = 1 };
+
 // Where one op's matrices come from and where they go in the pass's shared-memory table.
 struct JitMtab {
     int moff;               // offset in the table (complex entries)
@@ -38,6 +55,8 @@ struct JitFwdArgs {
     V *dst;
     long long batch;
     long long src_batch_stride;
+    TmaGeom tg;
+    int *err;               // error word (MQB_DEV_ERR_*), set once
 };
 
 template <typename V>
@@ -58,6 +77,8 @@ struct JitBwdArgs {
     int n_hams;
     int n_local_slots;
     long long batch;
+    TmaGeom tg;
+    int *err;
 };
 
 }  // namespace mqb

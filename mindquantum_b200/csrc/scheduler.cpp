@@ -331,9 +331,11 @@ void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int 
                     if (!(Rm >> b & 1) && b % res_mod == r) ++cnt;
                 return cnt;
             };
+            // (ties go to the highest bit: the low contiguous bits stay thread bits, so a stage can
+            // read and write the tile in the order the TMA lands it without bank conflicts)
             while (popc(R) < RB) {
                 int best = -1, best_score = -1;
-                for (int b = 0; b < K; ++b) {
+                for (int b = K - 1; b >= 0; --b) {
                     if (R >> b & 1) continue;
                     const int score = thread_residue_count(R, b % res_mod);
                     if (score > best_score) {
