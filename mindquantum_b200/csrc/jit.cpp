@@ -705,7 +705,7 @@ void emit_relayout(std::ostringstream &o, const PassPlan &pl, int K, int TB, int
             if (to_swz) o << "    rv[" << idx << "] = " << ptr(r) << "[tid + " << (k << TB) << "u];\n";
             else o << "    rv[" << idx << "] = " << ptr(r) << "[(qt ^ " << qk_of(k) << "u) >> " << sh << "];\n";
         }
-    o << "    pipe::consumers_sync(NT);\n";
+    o << "    pipe::consumers_sync(BAR, NT);\n";
     for (int r = 0; r < n_tiles; ++r)
         for (int k = 0; k < nvec; ++k) {
             const int idx = r * nvec + k;
@@ -715,33 +715,58 @@ void emit_relayout(std::ostringstream &o, const PassPlan &pl, int K, int TB, int
             if (to_swz) o << "    " << ptr(r) << "[(qt ^ " << qk_of(k) << "u) >> " << sh << "] = rv[" << idx << "];\n";
             else o << "    " << ptr(r) << "[tid + " << (k << TB) << "u] = rv[" << idx << "];\n";
         }
-    o << "    pipe::consumers_sync(NT);\n   }\n";
+    o << "    pipe::consumers_sync(BAR, NT);\n   }\n";
 }
 
-// Buffers of the tile ring: the forward kernels keep two (three blocks per SM at 2^12 complex64),
-// the adjoint kernels as many as fit beside one block's tables (up to three).  The environment
-// variables MQB_PIPE_FWD_BUFFERS / MQB_PIPE_BWD_BUFFERS override the counts (tuning).
-int fwd_buffers() {
-    const char *e = std::getenv("MQB_PIPE_FWD_BUFFERS");
-    return e ? std::max(1, std::min(4, std::atoi(e))) : 2;
+// Shape of a kernel's tile ring: G consumer groups of 2^(K - RB) threads share one block's ring
+// of NB >= G tile buffers and take its tiles in turn (tile i goes to group i mod G and buffer
+// i mod NB); each group has its own matrix table (and, in the adjoint, gradient slots).  There is
+// no producer warp: a group stores its own tiles and refills their buffers, so a block of 16
+// warps keeps 128 registers per thread.  Defaults: forward kernels one group of 2^(K - RB) threads
+// and two buffers (three blocks per SM at 2^12 complex64), adjoint kernels two groups and three
+// buffers.  MQB_PIPE_{FWD,BWD}_{GROUPS,BUFFERS} override them (tuning).
+int env_int(const char *name, int dflt, int lo, int hi) {
+    const char *e = std::getenv(name);
+    return e ? std::max(lo, std::min(hi, std::atoi(e))) : dflt;
+}
+
+int max_groups(int nt) { return std::max(1, std::min(15, 1024 / nt)); }
+
+int fwd_groups(const Pass &p) {
+    const int nt = 1 << (p.K - p.f_reg_bits);
+    return std::min(max_groups(nt), env_int("MQB_PIPE_FWD_GROUPS", 1, 1, 15));
+}
+
+int fwd_buffers(const Pass &p) { return std::max(fwd_groups(p), env_int("MQB_PIPE_FWD_BUFFERS", 2, 1, 8)); }
+
+size_t fwd_smem(const Pass &p, int precision) {
+    const size_t eb = elem_bytes(precision);
+    return size_t(fwd_buffers(p)) * ((size_t(1) << p.K) * eb) +
+           size_t(fwd_groups(p)) * a16(size_t(p.f_mtab_entries) * eb) + 8 * 16;
+}
+
+int bwd_groups(const Pass &p) {
+    const int nt = 1 << (p.K - p.reg_bits);
+    return std::min(max_groups(nt), env_int("MQB_PIPE_BWD_GROUPS", 2, 1, 15));
 }
 
 size_t bwd_fixed_smem(const Pass &p, int precision, int n_hams) {
     const size_t eb = elem_bytes(precision);
     const int nw = (1 << (p.K - p.reg_bits)) / 32;
-    return a16(size_t(p.mtab_entries) * eb) + a16(size_t(nw) * std::max(1, p.n_slots) * n_hams * sizeof(double)) + 8 * 8;
+    return size_t(bwd_groups(p)) *
+               (a16(size_t(p.mtab_entries) * eb) + a16(size_t(nw) * std::max(1, p.n_slots) * n_hams * sizeof(double))) +
+           8 * 16;
 }
 
+// Buffers of the adjoint ring: G + 1 where they fit in 227 KB, else as many as fit (at least G).
 int bwd_buffers(const Pass &p, int precision, int n_hams) {
     const size_t buf = (size_t(1) << p.K) * elem_bytes(precision) * (1 + n_hams);
     const size_t fixed = bwd_fixed_smem(p, precision, n_hams);
-    int nb = 1;
-    while (nb < 3 && (nb + 1) * buf + fixed <= size_t(200) << 10) ++nb;
-    if (const char *e = std::getenv("MQB_PIPE_BWD_BUFFERS")) {
-        int want = std::max(1, std::min(4, std::atoi(e)));
-        while (want > 1 && want * buf + fixed > size_t(227) << 10) --want;
-        nb = want;
-    }
+    const int G = bwd_groups(p);
+    int nb = env_int("MQB_PIPE_BWD_BUFFERS", G + 1, 1, 8);
+    while (nb > G && nb * buf + fixed > size_t(227) << 10) --nb;
+    if (nb * buf + fixed > size_t(227) << 10)
+        throw std::runtime_error("generated adjoint pass: the tile ring does not fit in shared memory");
     return nb;
 }
 
@@ -783,7 +808,7 @@ void emit_stage_load(std::ostringstream &o, const PassPlan &pl, const StageDesc 
 void emit_stage_store(std::ostringstream &o, const PassPlan &pl, const StageDesc &sd, int RB, int TB, int NH, int lay_in,
                       int lay_out, bool barrier_after) {
     if (lay_out != lay_in)
-        o << "    pipe::consumers_sync(NT);\n    const unsigned pLo = " << lay_lt_expr(pl, lay_out, sd, TB) << ";\n";
+        o << "    pipe::consumers_sync(BAR, NT);\n    const unsigned pLo = " << lay_lt_expr(pl, lay_out, sd, TB) << ";\n";
     else
         o << "    const unsigned pLo = pLt;\n";
     for (int j = 0; j < (1 << RB); ++j) {
@@ -795,67 +820,71 @@ void emit_stage_store(std::ostringstream &o, const PassPlan &pl, const StageDesc
             o << "    tl[pLo ^ " << off << "u] = v[" << j << "];\n";
         }
     }
-    if (barrier_after) o << "    pipe::consumers_sync(NT);\n";
+    if (barrier_after) o << "    pipe::consumers_sync(BAR, NT);\n";
     o << "   }\n";
 }
 
-// Producer (one thread of the extra warp): the tile ring's loads and stores.  `load_body` issues
-// the copies of tile k into buffer sb, `store_body` those of tile i from buffer sb; both see
-// b (sample) and tb (the tile's outside bits).  A buffer is handed to the consumers through its
-// `full` barrier: with the TMA's transaction bytes, or (forward passes that start from |0...0>
-// and load nothing) with a plain arrival once the buffer's previous store has been read out.
-void emit_producer(std::ostringstream &o, const std::string &load_body, const std::string &store_body, bool zero_opt) {
-    o << "  if (tid >= NT) {\n   if (tid == NT) {\n"
-      << "    const long long first = blockIdx.x, cnt = first < total ? (total - 1 - first) / gridDim.x + 1 : 0;\n"
-      << "    const int n = a.g.n;\n"
-      << "    auto tile_of = [&](long long k, long long &b, tile::u64 &tb) {\n"
-      << "     const long long w = first + k * gridDim.x;\n"
-      << "     b = w >> a.g.n_out;\n"
-      << "     tb = tile::tile_base(a.g, tile::u64(w) & tile::u64(n_tiles - 1));\n"
-      << "    };\n"
-      << "    auto load = [&](long long k) {\n"
-      << "     const int sb = int(k % NB);\n     long long b;\n     tile::u64 tb;\n     tile_of(k, b, tb);\n"
-      << "     unsigned char *buf = smem + sb * BUFB;\n";
-    if (zero_opt) o << "     if (zero) {\n      pipe::mbar_arrive(full + sb);\n      return;\n     }\n";
-    o << "     pipe::mbar_expect_tx(full + sb, BUFB);\n"
-      << load_body << "    };\n"
-      << "    long long issued = 0, i = 0;\n    bool ok = true;\n"
-      << "    for (; issued < cnt && issued < NB; ++issued) load(issued);\n"
-      << "    for (; i < cnt; ++i) {\n"
-      << "     const int sb = int(i % NB);\n"
-      << "     if (!pipe::mbar_wait(done + sb, unsigned(i / NB) & 1u)) {\n"
-      << "      pipe::report(a.err, MQB_DEV_ERR_TIMEOUT);\n      ok = false;\n      break;\n     }\n"
-      << "     long long b;\n     tile::u64 tb;\n     tile_of(i, b, tb);\n"
-      << "     const unsigned char *buf = smem + sb * BUFB;\n"
-      << store_body
-      << "     pipe::bulk_commit();\n"
-      << "     if (issued < cnt) {\n      pipe::bulk_wait_read_all();\n      load(issued);\n      ++issued;\n     }\n"
-      << "    }\n"
-      << "    if (!ok)   // let the loads still in flight land before the block exits\n"
-      << "     for (long long k = i; k < issued; ++k) pipe::mbar_wait(full + k % NB, unsigned(k / NB) & 1u);\n"
-      << "    pipe::bulk_wait_all();\n"
-      << "   }\n   return;\n  }\n";
+// The tile ring of a kernel, by its consumer groups (no producer warp).  Tile k of this block (its
+// tiles are blockIdx.x + k gridDim.x) goes to group k mod G and buffer k mod NB; the buffer is
+// handed over through its `full` mbarrier, with the TMA's transaction bytes, or (forward passes that
+// start from |0...0> and load nothing) with a plain arrival.  Thread 0 of block issues the first
+// NB tiles; after that the group that finished tile k stores it (thread 0 of the group, after a
+// group barrier) and, at the start of its next tile, refills the buffer with tile k + NB once the
+// store has read it out.  Every thread 0 remembers the last tile it put in each buffer and waits
+// for those copies before the block exits.
+//
+// `issue_body` issues the copies of tile k into buffer sb (b: sample, tb: the tile's outside bits);
+// `store_body` those of the finished tile from buffer sb.
+void emit_ring_prologue(std::ostringstream &o, const std::string &issue_body, bool zero_opt) {
+    o << "  const int grp = int(threadIdx.x) / NT, BAR = 1 + grp;\n"
+      << "  const unsigned tid = threadIdx.x % NT;\n"
+      << "  const long long first = blockIdx.x, cnt = first < total ? (total - 1 - first) / gridDim.x + 1 : 0;\n"
+      << "  const int n = a.g.n;\n"
+      << "  long long mine[NB];\n"
+      << "  for (int k = 0; k < NB; ++k) mine[k] = -1;\n"
+      << "  auto issue = [&](long long k) {\n"
+      << "   const int sb = int(k % NB);\n"
+      << "   const long long w = first + k * gridDim.x, b = w >> a.g.n_out;\n"
+      << "   const tile::u64 tb = tile::tile_base(a.g, tile::u64(w) & tile::u64(n_tiles - 1));\n"
+      << "   unsigned char *buf = smem + sb * BUFB;\n"
+      << "   mine[sb] = k;\n";
+    if (zero_opt) o << "   if (zero) {\n    pipe::mbar_arrive(full + sb);\n    return;\n   }\n";
+    o << "   pipe::mbar_expect_tx(full + sb, BUFB);\n" << issue_body << "  };\n"
+      << "  if (threadIdx.x == 0)\n   for (long long k = 0; k < cnt && k < NB; ++k) issue(k);\n"
+      << "  long long prev = -1;   // this group's last tile\n";
 }
 
-// Consumers' wait for buffer sb of tile i: one thread polls the mbarrier, the outcome is shared
-// through a barrier reduction, then every thread observes the completed phase itself.
-void emit_consumer_wait(std::ostringstream &o, const std::string &indent) {
-    o << indent << "if (!pipe::consumers_and(NT, tid != 0u || pipe::mbar_wait(full + sb, par))) {\n"
-      << indent << " if (tid == 0u) pipe::report(a.err, MQB_DEV_ERR_TIMEOUT);\n"
-      << indent << " break;\n"
-      << indent << "}\n"
-      << indent << "pipe::mbar_test(full + sb, par);\n";
+// Start of a group's tile i: refill the buffer of its previous tile, then wait (together) for tile i.
+void emit_ring_wait(std::ostringstream &o) {
+    o << "   if (tid == 0u && prev >= 0 && prev + NB < cnt) {\n"
+      << "    pipe::bulk_wait_read_all();\n    issue(prev + NB);\n   }\n"
+      << "   if (!pipe::consumers_and(BAR, NT, tid != 0u || pipe::mbar_wait(full + sb, par))) {\n"
+      << "    if (tid == 0u) pipe::report(a.err, MQB_DEV_ERR_TIMEOUT);\n"
+      << "    break;\n"
+      << "   }\n"
+      << "   pipe::mbar_test(full + sb, par);\n";
 }
 
-size_t fwd_smem(const Pass &p, int precision) {
-    const size_t eb = elem_bytes(precision);
-    return size_t(fwd_buffers()) * ((size_t(1) << p.K) * eb) + a16(size_t(p.f_mtab_entries) * eb) + 8 * 8;
+// End of a group's tile i: every thread's writes made visible to the TMA, then thread 0 stores.
+void emit_ring_store(std::ostringstream &o, const std::string &store_body) {
+    o << "   pipe::fence_async_smem();\n   pipe::consumers_sync(BAR, NT);\n"
+      << "   if (tid == 0u) {\n    const unsigned char *buf = smem + sb * BUFB;\n" << store_body
+      << "    pipe::bulk_commit();\n   }\n   prev = i;\n";
+}
+
+void emit_ring_exit(std::ostringstream &o) {
+    o << "  if (tid == 0u) {\n"
+      << "   if (prev >= 0 && prev + NB < cnt) {   // a buffer nobody else refills (only when NB < G)\n"
+      << "    pipe::bulk_wait_read_all();\n    issue(prev + NB);\n   }\n"
+      << "   for (int k = 0; k < NB; ++k)   // the copies this thread started have landed\n"
+      << "    if (mine[k] >= 0) pipe::mbar_wait(full + k, unsigned(mine[k] / NB) & 1u);\n"
+      << "   pipe::bulk_wait_all();\n  }\n";
 }
 
 std::string forward_source(const Schedule &s, const Pass &p, int precision) {
     const int RB = p.f_reg_bits, K = p.K, TB = K - RB;
     const PassPlan pl = pass_plan(p.qbits, precision);
-    const int NB = fwd_buffers();
+    const int NB = fwd_buffers(p), G = fwd_groups(p);
     std::vector<const StageDesc *> ex;
     for (int si = 0; si < p.f_n_stages; ++si) ex.push_back(&s.f_stages[p.f_stage_begin + si]);
     const LayPlan lp = plan_layouts(pl, ex, TB);
@@ -863,36 +892,34 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
     const int min_blocks = int(std::max<size_t>(1, std::min<size_t>(3, (size_t(220) << 10) / fwd_smem(p, precision))));
     std::ostringstream o;
     emit_header(o, precision);
-    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) + 32 << ", " << min_blocks
+    o << "extern \"C\" __global__ void __launch_bounds__(" << G * (1 << TB) << ", " << min_blocks
       << ") mqb_fwd_pass(const JitFwdArgs<V> a, "
       << "const __grid_constant__ pipe::TMap m_src, const __grid_constant__ pipe::TMap m_dst) {\n"
       << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", NT = 1 << (K - RB), NB = " << NB
-      << ", TS = 1 << K;\n"
+      << ", G = " << G << ", TS = 1 << K;\n"
       << "  constexpr unsigned BUFB = TS * sizeof(V);\n"
       << "  extern __shared__ __align__(1024) unsigned char smem[];\n"
-      << "  V *mt = reinterpret_cast<V *>(smem + NB * BUFB);\n"
-      << "  pipe::u64 *full = reinterpret_cast<pipe::u64 *>(smem + NB * BUFB + tile::align16(tile::u64(a.mtab_entries) * "
-         "sizeof(V)));\n"
-      << "  pipe::u64 *done = full + NB;\n"
-      << "  const unsigned tid = threadIdx.x;\n"
-      << "  if (tid == 0) {\n   for (int k = 0; k < NB; ++k) {\n    pipe::mbar_init(full + k, 1);\n"
-      << "    pipe::mbar_init(done + k, NT);\n   }\n   pipe::fence_mbar_init();\n  }\n  __syncthreads();\n"
+      << "  const tile::u64 mtb = tile::align16(tile::u64(a.mtab_entries) * sizeof(V));\n"
+      << "  pipe::u64 *full = reinterpret_cast<pipe::u64 *>(smem + NB * BUFB + G * mtb);\n"
+      << "  if (threadIdx.x == 0) {\n   for (int k = 0; k < NB; ++k) pipe::mbar_init(full + k, 1);\n"
+      << "   pipe::fence_mbar_init();\n  }\n  __syncthreads();\n"
       << "  const long long n_tiles = 1ll << a.g.n_out, total = a.batch * n_tiles;\n"
       << "  const bool zero = a.src == nullptr;\n";
-    emit_producer(o,
-                  "     const tile::u64 bs = a.src_batch_stride ? tile::u64(b) : 0;\n"
-                  "     pipe::load_tile(&m_src, a.tg, (bs << n) | tb, buf, full + sb);\n",
-                  "     pipe::store_tile(&m_dst, a.tg, (tile::u64(b) << n) | tb, buf);\n", true);
-    o << "  long long cached_b = -1, i = 0;\n"
-      << "  for (long long w = blockIdx.x; w < total; w += gridDim.x, ++i) {\n"
-      << "   const long long b = w >> a.g.n_out;\n"
+    emit_ring_prologue(o,
+                       "   const tile::u64 bs = a.src_batch_stride ? tile::u64(b) : 0;\n"
+                       "   pipe::load_tile(&m_src, a.tg, (bs << n) | tb, buf, full + sb);\n",
+                       true);
+    o << "  V *mt = reinterpret_cast<V *>(smem + NB * BUFB + grp * mtb);\n"
+      << "  long long cached_b = -1;\n"
+      << "  for (long long i = grp; i < cnt; i += G) {\n"
+      << "   const long long w = first + i * gridDim.x, b = w >> a.g.n_out;\n"
       << "   const tile::u64 base = tile::tile_base(a.g, tile::u64(w) & tile::u64(n_tiles - 1));\n"
       << "   const int sb = int(i % NB);\n   const unsigned par = unsigned(i / NB) & 1u;\n"
       << "   V *tl = reinterpret_cast<V *>(smem + sb * BUFB);\n"
-      << "   if (b != cached_b) {\n    pipe::consumers_sync(NT);\n"
+      << "   if (b != cached_b) {\n    pipe::consumers_sync(BAR, NT);\n"
       << "    pipe::load_mtab(mt, a.mt, a.n_mt, a.mats + b * a.mats_stride, a.cpool, tid, NT);\n"
-      << "    cached_b = b;\n    pipe::consumers_sync(NT);\n   }\n";
-    emit_consumer_wait(o, "   ");
+      << "    cached_b = b;\n    pipe::consumers_sync(BAR, NT);\n   }\n";
+    emit_ring_wait(o);
     if (lp.relayout_in) {
         o << "   if (!zero) {\n    V *tbase = tl;\n";
         emit_relayout(o, pl, K, TB, 1, true);
@@ -921,7 +948,10 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
         emit_relayout(o, pl, K, TB, 1, false);
         o << "   }\n";
     }
-    o << "   pipe::fence_async_smem();\n   pipe::mbar_arrive(done + sb);\n  }\n}\n";
+    emit_ring_store(o, "    pipe::store_tile(&m_dst, a.tg, (tile::u64(b) << n) | base, buf);\n");
+    o << "  }\n";
+    emit_ring_exit(o);
+    o << "}\n";
     return o.str();
 }
 
@@ -929,50 +959,46 @@ std::string backward_source(const Schedule &s, const Pass &p, int precision, int
     const int RB = p.reg_bits, K = p.K, TB = K - RB;
     const int NLS = std::max(1, p.n_slots);
     const PassPlan pl = pass_plan(p.qbits, precision);
-    const int NB = bwd_buffers(p, precision, NH);
+    const int NB = bwd_buffers(p, precision, NH), G = bwd_groups(p);
     std::vector<const StageDesc *> ex;
     for (int si = p.n_stages - 1; si >= 0; --si) ex.push_back(&s.stages[p.stage_begin + si]);
     const LayPlan lp = plan_layouts(pl, ex, TB);
     std::ostringstream o;
     emit_header(o, precision);
-    o << "extern \"C\" __global__ void __launch_bounds__(" << (1 << TB) + 32 << ", 1) mqb_adj_pass(const JitBwdArgs<V> a, "
+    o << "extern \"C\" __global__ void __launch_bounds__(" << G * (1 << TB) << ", 1) mqb_adj_pass(const JitBwdArgs<V> a, "
       << "const __grid_constant__ pipe::TMap m_psi, const __grid_constant__ pipe::TMap m_lam, "
       << "const __grid_constant__ pipe::TMap m_pdst) {\n"
       << "  constexpr int RB = " << RB << ", NR = 1 << RB, K = " << K << ", NH = " << NH << ", NLS = " << NLS
-      << ", TS = 1 << K, NT = 1 << (K - RB), NB = " << NB << ";\n"
+      << ", TS = 1 << K, NT = 1 << (K - RB), NB = " << NB << ", G = " << G << ";\n"
       << "  constexpr unsigned TILEB = TS * sizeof(V), BUFB = TILEB * (1 + NH);\n"
+      << "  constexpr int nw = NT / 32, WS = (nw * NLS * NH + 1) / 2 * 2;   // gradient slots of a group\n"
       << "  extern __shared__ __align__(1024) unsigned char smem[];\n"
-      << "  tile::u64 o = tile::u64(NB) * BUFB;\n"
-      << "  V *mt = reinterpret_cast<V *>(smem + o);\n"
-      << "  o = tile::align16(o + tile::u64(a.mtab_entries) * sizeof(V));\n"
-      << "  double *wacc = reinterpret_cast<double *>(smem + o);\n"
-      << "  o = tile::align16(o + tile::u64(NT / 32) * NLS * NH * sizeof(double));\n"
-      << "  pipe::u64 *full = reinterpret_cast<pipe::u64 *>(smem + o), *done = full + NB;\n"
-      << "  const unsigned tid = threadIdx.x;\n"
-      << "  const int nw = NT / 32, warp = int(tid) / 32, lane = int(tid) % 32;\n"
-      << "  if (tid == 0) {\n   for (int k = 0; k < NB; ++k) {\n    pipe::mbar_init(full + k, 1);\n"
-      << "    pipe::mbar_init(done + k, NT);\n   }\n   pipe::fence_mbar_init();\n  }\n"
-      << "  for (int i = int(tid); i < nw * NLS * NH; i += int(blockDim.x)) wacc[i] = 0;\n  __syncthreads();\n"
+      << "  const tile::u64 mtb = tile::align16(tile::u64(a.mtab_entries) * sizeof(V));\n"
+      << "  double *wacc0 = reinterpret_cast<double *>(smem + NB * BUFB + G * mtb);\n"
+      << "  pipe::u64 *full = reinterpret_cast<pipe::u64 *>(wacc0 + G * WS);\n"
+      << "  if (threadIdx.x == 0) {\n   for (int k = 0; k < NB; ++k) pipe::mbar_init(full + k, 1);\n"
+      << "   pipe::fence_mbar_init();\n  }\n"
+      << "  for (int i = int(threadIdx.x); i < G * WS; i += int(blockDim.x)) wacc0[i] = 0;\n  __syncthreads();\n"
       << "  const long long n_tiles = 1ll << a.g.n_out, total = a.batch * n_tiles;\n";
-    emit_producer(o,
-                  "     pipe::load_tile(&m_psi, a.tg, (tile::u64(b) << n) | tb, buf, full + sb);\n"
-                  "     for (int h = 0; h < NH; ++h)\n"
-                  "      pipe::load_tile(&m_lam, a.tg, (tile::u64(h * a.batch + b) << n) | tb, buf + (1 + h) * TILEB, "
-                  "full + sb);\n",
-                  "     for (int h = 0; h < NH; ++h)\n"
-                  "      pipe::store_tile(&m_lam, a.tg, (tile::u64(h * a.batch + b) << n) | tb, buf + (1 + h) * TILEB);\n"
-                  "     if (a.psi_dst) pipe::store_tile(&m_pdst, a.tg, (tile::u64(b) << n) | tb, buf);\n",
-                  false);
-    o << "  long long cached_b = -1, i = 0;\n"
-      << "  for (long long w = blockIdx.x; w < total; w += gridDim.x, ++i) {\n"
-      << "   const long long b = w >> a.g.n_out;\n"
+    emit_ring_prologue(o,
+                       "   pipe::load_tile(&m_psi, a.tg, (tile::u64(b) << n) | tb, buf, full + sb);\n"
+                       "   for (int h = 0; h < NH; ++h)\n"
+                       "    pipe::load_tile(&m_lam, a.tg, (tile::u64(h * a.batch + b) << n) | tb, buf + (1 + h) * TILEB, "
+                       "full + sb);\n",
+                       false);
+    o << "  const int warp = int(tid) / 32, lane = int(tid) % 32;\n"
+      << "  V *mt = reinterpret_cast<V *>(smem + NB * BUFB + grp * mtb);\n"
+      << "  double *wacc = wacc0 + grp * WS;\n"
+      << "  long long cached_b = -1;\n"
+      << "  for (long long i = grp; i < cnt; i += G) {\n"
+      << "   const long long w = first + i * gridDim.x, b = w >> a.g.n_out;\n"
       << "   const tile::u64 base = tile::tile_base(a.g, tile::u64(w) & tile::u64(n_tiles - 1));\n"
       << "   const int sb = int(i % NB);\n   const unsigned par = unsigned(i / NB) & 1u;\n"
       << "   V *psi = reinterpret_cast<V *>(smem + sb * BUFB);\n   V *lam = psi + TS;\n"
-      << "   if (b != cached_b) {\n    pipe::consumers_sync(NT);\n"
+      << "   if (b != cached_b) {\n    pipe::consumers_sync(BAR, NT);\n"
       << "    pipe::load_mtab(mt, a.mt, a.n_mt, a.mats + b * a.mats_stride, a.cpool, tid, NT);\n"
-      << "    cached_b = b;\n    pipe::consumers_sync(NT);\n   }\n";
-    emit_consumer_wait(o, "   ");
+      << "    cached_b = b;\n    pipe::consumers_sync(BAR, NT);\n   }\n";
+    emit_ring_wait(o);
     if (lp.relayout_in) {
         o << "   {\n    V *tbase = psi;\n";
         emit_relayout(o, pl, K, TB, 1 + NH, true);
@@ -1009,17 +1035,22 @@ std::string backward_source(const Schedule &s, const Pass &p, int precision, int
         emit_relayout(o, pl, K, TB, 1 + NH, false);
         o << "   }\n";
     }
-    o << "   pipe::fence_async_smem();\n   pipe::mbar_arrive(done + sb);\n"
-      << "   const long long nxt = w + gridDim.x;\n"
-      << "   if ((nxt >= total) || ((nxt >> a.g.n_out) != b)) {\n"
-      << "    pipe::consumers_sync(NT);\n"
-      << "    for (int i = int(tid); i < a.n_local_slots * NH; i += NT) {\n"
+    emit_ring_store(o,
+                    "    for (int h = 0; h < NH; ++h)\n"
+                    "     pipe::store_tile(&m_lam, a.tg, (tile::u64(h * a.batch + b) << n) | base, buf + (1 + h) * TILEB);\n"
+                    "    if (a.psi_dst) pipe::store_tile(&m_pdst, a.tg, (tile::u64(b) << n) | base, buf);\n");
+    o << "   const long long nxt = i + G;\n"
+      << "   if (nxt >= cnt || ((first + nxt * gridDim.x) >> a.g.n_out) != b) {\n"
+      << "    pipe::consumers_sync(BAR, NT);\n"
+      << "    for (int s2 = int(tid); s2 < a.n_local_slots * NH; s2 += NT) {\n"
       << "     double sum = 0;\n"
       << "     for (int ww = 0; ww < nw; ++ww) {\n"
-      << "      sum += wacc[ww * NLS * NH + i];\n      wacc[ww * NLS * NH + i] = 0;\n     }\n"
-      << "     const int ls = i / NH, h = i % NH;\n"
+      << "      sum += wacc[ww * NLS * NH + s2];\n      wacc[ww * NLS * NH + s2] = 0;\n     }\n"
+      << "     const int ls = s2 / NH, h = s2 % NH;\n"
       << "     if (sum != 0) atomicAdd(&a.gslots[(b * a.n_slots + a.slot_map[ls]) * a.n_hams + h], sum);\n"
-      << "    }\n    pipe::consumers_sync(NT);\n   }\n  }\n}\n";
+      << "    }\n    pipe::consumers_sync(BAR, NT);\n   }\n  }\n";
+    emit_ring_exit(o);
+    o << "}\n";
     return o.str();
 }
 
@@ -1255,7 +1286,7 @@ cudaError_t jit_launch_forward(const void *kernel, JitFwdArgs<V> a, const Pass &
     encode_map(&ms, a.src, a.g.n, a.src_batch_stride ? a.batch : 1, pl);
     encode_map(&md, a.dst, a.g.n, a.batch, pl);
     void *argv[] = {&a, &ms, &md};
-    return launch_pipe(kernel, argv, (1 << (p.K - p.f_reg_bits)) + 32, jit_forward_smem(p, precision), sm_count,
+    return launch_pipe(kernel, argv, fwd_groups(p) * (1 << (p.K - p.f_reg_bits)), jit_forward_smem(p, precision), sm_count,
                        a.batch << a.g.n_out, st);
 }
 
@@ -1270,7 +1301,8 @@ cudaError_t jit_launch_backward(const void *kernel, JitBwdArgs<V> a, const Pass 
     encode_map(&ml, a.lam, a.g.n, a.batch * n_hams, pl);
     encode_map(&md, a.psi_dst, a.g.n, a.batch, pl);
     void *argv[] = {&a, &mp, &ml, &md};
-    return launch_pipe(kernel, argv, (1 << (p.K - p.reg_bits)) + 32, jit_backward_smem(p, precision, n_hams), sm_count,
+    return launch_pipe(kernel, argv, bwd_groups(p) * (1 << (p.K - p.reg_bits)), jit_backward_smem(p, precision, n_hams),
+                       sm_count,
                        a.batch << a.g.n_out, st);
 }
 

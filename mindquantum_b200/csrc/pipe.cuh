@@ -73,20 +73,20 @@ __device__ __forceinline__ bool mbar_wait(u64 *bar, unsigned parity) {
     return true;
 }
 
-// Barrier 1 among the n consumer threads (barrier 0 is __syncthreads).
-__device__ __forceinline__ void consumers_sync(int n) {
-    asm volatile("bar.sync 1, %0;" ::"r"(n) : "memory");
+// Named barrier `id` (1 + consumer group; 0 is __syncthreads) among the n threads of a group.
+__device__ __forceinline__ void consumers_sync(int id, int n) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
 
-// Barrier 1 among the n consumer threads, returning whether q holds on every one of them: the
-// consumers take every wait's outcome together, so no thread leaves the tile loop alone and none
-// is left waiting at a later barrier.
-__device__ __forceinline__ bool consumers_and(int n, bool q) {
+// Named barrier `id` among the n threads of a consumer group, returning whether q holds on every
+// one of them: a group takes every wait's outcome together, so no thread leaves the tile loop
+// alone and none is left waiting at a later barrier.
+__device__ __forceinline__ bool consumers_and(int id, int n, bool q) {
     unsigned r;
     asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}"
+        "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.and.pred p, %2, %3, q;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(r)
-        : "r"(static_cast<unsigned>(q)), "r"(n)
+        : "r"(static_cast<unsigned>(q)), "r"(id), "r"(n)
         : "memory");
     return r != 0;
 }

@@ -11,6 +11,7 @@
 // the current pass blocks all its qubits for the rest of the scan, so no later gate sharing a
 // qubit with it can overtake it.
 #include <algorithm>
+#include <cstdlib>
 #include <stdexcept>
 
 #include "mqb_internal.h"
@@ -21,7 +22,12 @@ static inline int popc(uint64_t x) { return __builtin_popcountll(x); }
 
 int contiguity_bits(int precision) { return precision == MQB_PREC_C64 ? 4 : 3; }
 
-int fwd_reg_bits(int precision) { return precision == MQB_PREC_C64 ? 5 : 4; }
+// MQB_FWD_REG_BITS (2..5) overrides the complex64 forward register bits (tuning).
+int fwd_reg_bits(int precision) {
+    if (precision == MQB_PREC_C64)
+        if (const char *e = std::getenv("MQB_FWD_REG_BITS")) return std::max(2, std::min(5, std::atoi(e)));
+    return precision == MQB_PREC_C64 ? 5 : 4;
+}
 
 int bwd_reg_bits(int precision, int n_hams) {
     if (n_hams <= 1) return precision == MQB_PREC_C64 ? 4 : 3;
