@@ -847,7 +847,8 @@ void emit_ring_prologue(std::ostringstream &o, const std::string &issue_body, bo
       << "   const long long w = first + k * gridDim.x, b = w >> a.g.n_out;\n"
       << "   const tile::u64 tb = tile::tile_base(a.g, tile::u64(w) & tile::u64(n_tiles - 1));\n"
       << "   unsigned char *buf = smem + sb * BUFB;\n"
-      << "   mine[sb] = k;\n";
+      << "   mine[sb] = k;\n"
+      << "   ticket[sb] = k;\n";
     if (zero_opt) o << "   if (zero) {\n    pipe::mbar_arrive(full + sb);\n    return;\n   }\n";
     o << "   pipe::mbar_expect_tx(full + sb, BUFB);\n" << issue_body << "  };\n"
       << "  if (threadIdx.x == 0)\n   for (long long k = 0; k < cnt && k < NB; ++k) issue(k);\n"
@@ -858,7 +859,7 @@ void emit_ring_prologue(std::ostringstream &o, const std::string &issue_body, bo
 void emit_ring_wait(std::ostringstream &o) {
     o << "   if (tid == 0u && prev >= 0 && prev + NB < cnt) {\n"
       << "    pipe::bulk_wait_read_all();\n    issue(prev + NB);\n   }\n"
-      << "   if (!pipe::consumers_and(BAR, NT, tid != 0u || pipe::mbar_wait(full + sb, par))) {\n"
+      << "   if (!pipe::consumers_and(BAR, NT, tid != 0u || (pipe::wait_ticket(ticket + sb, i) && pipe::mbar_wait(full + sb, par)))) {\n"
       << "    if (tid == 0u) pipe::report(a.err, MQB_DEV_ERR_TIMEOUT);\n"
       << "    break;\n"
       << "   }\n"
@@ -901,7 +902,8 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
       << "  extern __shared__ __align__(1024) unsigned char smem[];\n"
       << "  const tile::u64 mtb = tile::align16(tile::u64(a.mtab_entries) * sizeof(V));\n"
       << "  pipe::u64 *full = reinterpret_cast<pipe::u64 *>(smem + NB * BUFB + G * mtb);\n"
-      << "  if (threadIdx.x == 0) {\n   for (int k = 0; k < NB; ++k) pipe::mbar_init(full + k, 1);\n"
+      << "  volatile long long *ticket = reinterpret_cast<volatile long long *>(full + NB);\n"
+      << "  if (threadIdx.x == 0) {\n   for (int k = 0; k < NB; ++k) {\n    pipe::mbar_init(full + k, 1);\n    ticket[k] = -1;\n   }\n"
       << "   pipe::fence_mbar_init();\n  }\n  __syncthreads();\n"
       << "  const long long n_tiles = 1ll << a.g.n_out, total = a.batch * n_tiles;\n"
       << "  const bool zero = a.src == nullptr;\n";
@@ -976,7 +978,8 @@ std::string backward_source(const Schedule &s, const Pass &p, int precision, int
       << "  const tile::u64 mtb = tile::align16(tile::u64(a.mtab_entries) * sizeof(V));\n"
       << "  double *wacc0 = reinterpret_cast<double *>(smem + NB * BUFB + G * mtb);\n"
       << "  pipe::u64 *full = reinterpret_cast<pipe::u64 *>(wacc0 + G * WS);\n"
-      << "  if (threadIdx.x == 0) {\n   for (int k = 0; k < NB; ++k) pipe::mbar_init(full + k, 1);\n"
+      << "  volatile long long *ticket = reinterpret_cast<volatile long long *>(full + NB);\n"
+      << "  if (threadIdx.x == 0) {\n   for (int k = 0; k < NB; ++k) {\n    pipe::mbar_init(full + k, 1);\n    ticket[k] = -1;\n   }\n"
       << "   pipe::fence_mbar_init();\n  }\n"
       << "  for (int i = int(threadIdx.x); i < G * WS; i += int(blockDim.x)) wacc0[i] = 0;\n  __syncthreads();\n"
       << "  const long long n_tiles = 1ll << a.g.n_out, total = a.batch * n_tiles;\n";

@@ -73,6 +73,18 @@ __device__ __forceinline__ bool mbar_wait(u64 *bar, unsigned parity) {
     return true;
 }
 
+// Wait until a buffer's ticket names tile k (the tile whose copies were last started into it);
+// false when kWaitLimitNs passed first.  A buffer's mbarrier tells phases apart by parity only, so
+// a consumer may test it only once the buffer's previous tile has been handed over: the issuer
+// writes the ticket after it has finished with that previous tile.
+__device__ __forceinline__ bool wait_ticket(const volatile long long *slot, long long k) {
+    if (*slot == k) return true;
+    const u64 t0 = now_ns();
+    while (*slot != k)
+        if (now_ns() - t0 > kWaitLimitNs) return false;
+    return true;
+}
+
 // Named barrier `id` (1 + consumer group; 0 is __syncthreads) among the n threads of a group.
 __device__ __forceinline__ void consumers_sync(int id, int n) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
