@@ -830,8 +830,10 @@ void emit_stage_store(std::ostringstream &o, const PassPlan &pl, const StageDesc
 // start from |0...0> and load nothing) with a plain arrival.  Thread 0 of block issues the first
 // NB tiles; after that the group that finished tile k stores it (thread 0 of the group, after a
 // group barrier) and, at the start of its next tile, refills the buffer with tile k + NB once the
-// store has read it out.  Every thread 0 remembers the last tile it put in each buffer and waits
-// for those copies before the block exits.
+// store has read it out.  Before the issuer arms a buffer it writes the tile's index into the
+// buffer's ticket; a consumer tests the mbarrier's parity only once the ticket names its tile (the
+// parity alone cannot tell a phase from the one two fills later).  A group that gave up a wait
+// lets the copies it started into buffers whose ticket still names them land before it exits.
 //
 // `issue_body` issues the copies of tile k into buffer sb (b: sample, tb: the tile's outside bits);
 // `store_body` those of the finished tile from buffer sb.
@@ -852,7 +854,8 @@ void emit_ring_prologue(std::ostringstream &o, const std::string &issue_body, bo
     if (zero_opt) o << "   if (zero) {\n    pipe::mbar_arrive(full + sb);\n    return;\n   }\n";
     o << "   pipe::mbar_expect_tx(full + sb, BUFB);\n" << issue_body << "  };\n"
       << "  if (threadIdx.x == 0)\n   for (long long k = 0; k < cnt && k < NB; ++k) issue(k);\n"
-      << "  long long prev = -1;   // this group's last tile\n";
+      << "  long long prev = -1;   // this group's last tile\n"
+      << "  bool failed = false;\n";
 }
 
 // Start of a group's tile i: refill the buffer of its previous tile, then wait (together) for tile i.
@@ -861,6 +864,7 @@ void emit_ring_wait(std::ostringstream &o) {
       << "    pipe::bulk_wait_read_all();\n    issue(prev + NB);\n   }\n"
       << "   if (!pipe::consumers_and(BAR, NT, tid != 0u || (pipe::wait_ticket(ticket + sb, i) && pipe::mbar_wait(full + sb, par)))) {\n"
       << "    if (tid == 0u) pipe::report(a.err, MQB_DEV_ERR_TIMEOUT);\n"
+      << "    failed = true;\n"
       << "    break;\n"
       << "   }\n"
       << "   pipe::mbar_test(full + sb, par);\n";
@@ -877,8 +881,12 @@ void emit_ring_exit(std::ostringstream &o) {
     o << "  if (tid == 0u) {\n"
       << "   if (prev >= 0 && prev + NB < cnt) {   // a buffer nobody else refills (only when NB < G)\n"
       << "    pipe::bulk_wait_read_all();\n    issue(prev + NB);\n   }\n"
-      << "   for (int k = 0; k < NB; ++k)   // the copies this thread started have landed\n"
-      << "    if (mine[k] >= 0) pipe::mbar_wait(full + k, unsigned(mine[k] / NB) & 1u);\n"
+      << "   // after a timeout, copies this thread started may still be in flight (on the normal path every\n"
+      << "   // copy is consumed before its group finishes); a buffer whose ticket moved on was refilled by\n"
+      << "   // its consumer, so this thread's copy into it has landed\n"
+      << "   if (failed)\n"
+      << "    for (int k = 0; k < NB; ++k)\n"
+      << "     if (mine[k] >= 0 && ticket[k] == mine[k]) pipe::mbar_wait(full + k, unsigned(mine[k] / NB) & 1u);\n"
       << "   pipe::bulk_wait_all();\n  }\n";
 }
 
