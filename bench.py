@@ -124,9 +124,10 @@ def _peaks():
 
 # DRAM bytes per state byte moved by one adjoint pass launch (psi read, lambda read + write: 3 x
 # S*B algorithmic), from an ncu capture of the same kernel on the HEA 24-qubit, batch-2 case; a
-# launch's traffic grows in proportion to the state bytes it processes.  None: not captured for
+# launch's traffic grows in proportion to the state bytes it processes (760.9 and 761.6 MB read +
+# written for S*B = 268.4 MB in the two captured launches).  None: not captured for
 # the kernels built from the current sources.
-ADJ_DRAM_BYTES_PER_STATE_BYTE = None
+ADJ_DRAM_BYTES_PER_STATE_BYTE = 2.84
 
 
 def oracle_fixture_errors(n, layers, batch, seed, f_c64, g_c64, f_c128=None, g_c128=None):
