@@ -125,6 +125,11 @@ MQB_API int mqb_timing_end(double *ms, int64_t *launches, int n_kinds);
  * are then invalid); clear != 0 resets it.  Synchronizes the device.  No reference counterpart:
  * the reference's kernels have no bounded waits. */
 MQB_API int mqb_device_error(int *code, int clear);
+/* Fault injection for tests, on the calling thread: after `after` more successful device
+ * allocations of the library, the next one fails with MQB_ERR_ALLOC as if the device were out of
+ * memory; after < 0 disarms it.  No reference counterpart (the reference does not check its
+ * allocations: gpu_vector_core_policy.cu:36-49). */
+MQB_API int mqb_inject_alloc_failure(int after);
 /* sizeof of mqb_gate_desc, mqb_param_term, mqb_program_options, mqb_program_info (ABI check). */
 MQB_API int mqb_abi_struct_sizes(int64_t *out, int n);
 
@@ -157,13 +162,16 @@ MQB_API int mqb_jit_check(int n_qubits, int precision, const mqb_gate_desc *gate
 MQB_API int mqb_apply_workspace_size(const mqb_program *prog, int64_t batch, size_t *bytes);
 
 /* The same as mqb_apply, without a workspace argument and without allocating: for callers that
- * cannot allocate device memory while they apply a circuit (a framework recording a CUDA graph
- * that forbids allocations during capture, a runtime whose device memory is a fixed pool, a thin
- * binding that only owns the state buffers).  No counterpart in the reference.  The gate matrices
- * go to a fixed 4 MiB array inside the library (held on every GPU that loads it until exit);
- * batches whose matrices need more are rejected with MQB_ERR_WORKSPACE.  The first call on a
- * device looks the array up and should come before any stream capture.  All calls share the
- * array, so calls whose work overlaps on the GPU race. */
+ * cannot allocate device memory while they apply a circuit (a runtime that reserves all device
+ * memory in a fixed pool at start-up, a thin language binding that only owns the state buffers it
+ * passes in, a real-time loop that must not call into the allocator).  No counterpart in the
+ * reference.  The gate matrices go to a fixed 4 MiB array inside the library (held on every GPU
+ * that loads it until exit); batches whose matrices need more are rejected with
+ * MQB_ERR_WORKSPACE.  The first call on a device looks the array's address up and caches it (this
+ * first call should come before any stream capture); a device reset invalidates that cached
+ * address, so the entry point must not be used after cudaDeviceReset.  It runs the precompiled
+ * tile kernels only (loading a generated kernel would allocate).  All calls share the array, so
+ * calls whose work overlaps on the GPU race. */
 MQB_API int mqb_apply_static(mqb_program *prog, void *states, int64_t batch, const double *params,
                              int64_t param_stride, const double *custom, void *stream);
 
@@ -215,6 +223,15 @@ MQB_API int mqb_grad_workspace_size(const mqb_program *prog, int64_t batch, int 
  * init_states[b] when init_batched, else init_states[0]); f[b][h] = <psi|H_h|psi> as (re, im);
  * grad[b][h][p] = d f / d params[p] (real, the reference's 2 Re <psi|H dU|psi>).
  * f: device [batch][n_hams][2] float64, grad: device [batch][n_hams][n_params] float64. */
+/* FP64 norm checks of the complex64 state made by the last mqb_expectation_with_grad or
+ * mqb_adjoint_with_lambda call that used this workspace (same batch, n_hams, stride): out[k][b] =
+ * <psi_b|psi_b> at check k, for *n_checks checks (0 for complex128 programs).  The checks come
+ * after every ceil(sqrt(P))-th forward pass and the last one, then (stride 0 or > 1) at every
+ * ceil(sqrt(P))-th state the backward sweep rebuilds by applying passes in reverse.  With out ==
+ * NULL only *n_checks is set.  Copies to the host and synchronizes the stream.  No reference
+ * counterpart: the reference keeps no record of the norm. */
+MQB_API int mqb_grad_norm_checks(mqb_program *prog, const void *workspace, size_t workspace_bytes, int64_t batch,
+                                 int n_hams, int stride, double *out, int capacity, int *n_checks, void *stream);
 MQB_API int mqb_expectation_with_grad(mqb_program *prog, const mqb_hamiltonian *const *hams, int n_hams,
                               const void *init_states, int init_batched, int64_t batch, const double *params,
                               int64_t param_stride, const double *custom, double *f, double *grad,

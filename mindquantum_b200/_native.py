@@ -74,6 +74,8 @@ SIGNATURES = {
     'mqb_timing_begin': [],
     'mqb_timing_end': [_P, _P, _I],
     'mqb_device_error': [_P, _I],
+    'mqb_inject_alloc_failure': [_I],
+    'mqb_grad_norm_checks': [_P, _P, _SZ, _I64, _I, _I, _P, _I, _P, _P],
     'mqb_abi_struct_sizes': [_P, _I],
     'mqb_program_create': [_I, _I, _P, _I, _P, _I, _I, _P, _I64, _P, _P],
     'mqb_program_destroy': [_P],

@@ -72,11 +72,31 @@ void require_aligned(const void *ptr, const char *what) {
     if (ptr && (reinterpret_cast<uintptr_t>(ptr) & 15u)) fail(MQB_ERR_INVALID, "%s must be 16-byte aligned", what);
 }
 
+// Device allocations of the library (program and Hamiltonian tables): an out-of-memory error is
+// MQB_ERR_ALLOC.  mqb_inject_alloc_failure arms a countdown on the calling thread: after that many
+// successful allocations the next one fails as if the device were out of memory (host-side fault
+// injection for tests; nothing reaches the device).
+thread_local long long t_alloc_countdown = -1;
+
+void dev_alloc(void **ptr, size_t bytes, const char *what) {
+    if (t_alloc_countdown == 0) {
+        t_alloc_countdown = -1;
+        fail(MQB_ERR_ALLOC, "%s: out of device memory (%zu bytes; injected failure)", what, bytes);
+    }
+    const cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        fail(MQB_ERR_ALLOC, "%s: out of device memory (%zu bytes)", what, bytes);
+    }
+    ck(e, what);
+    if (t_alloc_countdown > 0) --t_alloc_countdown;
+}
+
 template <typename T>
 T *upload(const std::vector<T> &v) {
     if (v.empty()) return nullptr;
     T *d = nullptr;
-    ck(cudaMalloc(&d, sizeof(T) * v.size()), "cudaMalloc");
+    dev_alloc(reinterpret_cast<void **>(&d), sizeof(T) * v.size(), "cudaMalloc");
     ck(cudaMemcpy(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
     return d;
 }
@@ -402,10 +422,13 @@ static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R>
 }
 
 struct GradLayout {
-    size_t mats = 0, gslots = 0, lam = 0, w = 0, ckpt = 0, total = 0;
+    size_t mats = 0, gslots = 0, lam = 0, w = 0, ckpt = 0, norms = 0, total = 0;
     int n_ckpt = 0;
     bool need_w = false;
     std::vector<int> ckpt_index;   // p (1..P) -> checkpoint buffer index or -1
+    // FP64 norm checks of the complex64 state: the states after these forward passes, and the
+    // states before these passes that the backward rebuilds by reverse application
+    std::vector<int> norm_fwd, norm_bwd;
 };
 
 static GradLayout grad_layout(const mqb_program &p, const Schedule &s, int64_t batch, int n_hams, int stride) {
@@ -421,12 +444,21 @@ static GradLayout grad_layout(const mqb_program &p, const Schedule &s, int64_t b
     for (const Pass &ps : s.passes)
         if (!ps.fused) L.need_w = true;
     if (P == 0) L.need_w = true;
+    if (p.precision == MQB_PREC_C64 && P > 0) {
+        // every ceil(sqrt(P)) passes (and the last state of the forward sweep)
+        const int sn = std::max(1, int(std::ceil(std::sqrt(double(P)))));
+        for (int q = 1; q <= P; ++q)
+            if (q % sn == 0 || q == P) L.norm_fwd.push_back(q);
+        for (int q = P - 1; q >= 1; --q)
+            if (L.ckpt_index[q] < 0 && q % sn == 0) L.norm_bwd.push_back(q);
+    }
     L.mats = align_up(size_t(batch) * p.per_sample * p.elem());
     L.gslots = align_up(size_t(batch) * std::max(1, p.n_slots) * n_hams * sizeof(double));
     L.lam = align_up(state * n_hams);
     L.w = L.need_w ? align_up(state) : 0;
     L.ckpt = align_up(state) * L.n_ckpt;
-    L.total = L.mats + L.gslots + L.lam + L.w + L.ckpt;
+    L.norms = align_up((L.norm_fwd.size() + L.norm_bwd.size()) * size_t(batch) * 2 * sizeof(double));
+    L.total = L.mats + L.gslots + L.lam + L.w + L.ckpt + L.norms;
     return L;
 }
 
@@ -459,6 +491,16 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
 
     ck(cudaMemsetAsync(gslots, 0, L.gslots, st), "memset");
     if (f) ck(cudaMemsetAsync(f, 0, sizeof(double) * 2 * n_hams * batch, st), "memset");
+    // norm checks: <psi|psi> in FP64 per sample, [check][batch][re, im]
+    double *norms = reinterpret_cast<double *>(ck0 + L.ckpt);
+    if (L.norms) ck(cudaMemsetAsync(norms, 0, L.norms, st), "memset");
+    size_t n_checked = 0;
+    auto norm_check = [&](const V *state) {
+        TimeScope ts(TK_OTHER, st);
+        ck(launch_vdot<R>(state, state, p.n, batch, norms + 2 * batch * n_checked, sm, st), "norm check");
+        ++n_checked;
+    };
+    size_t next_fwd = 0, next_bwd = 0;
     run_matgen<R>(p, params, param_stride, custom, batch, mats, st);
 
     // forward: psi_{q+1} = pass_q(psi_q), psi_0 = init (or |0...0>)
@@ -470,6 +512,10 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
         const V *src = (q == 0) ? init_v : loc(q);
         const int64_t sstr = (q == 0) ? init_stride : dim;
         run_forward_pass<R>(p, sd, q, jf ? (*jf)[q] : nullptr, mats, src, sstr, loc(q + 1), batch, st);
+        if (next_fwd < L.norm_fwd.size() && L.norm_fwd[next_fwd] == q + 1) {
+            norm_check(loc(q + 1));
+            ++next_fwd;
+        }
     }
     V *psiP = W;
     if (P > 0) {
@@ -559,6 +605,10 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
                 ck(launch_plain_apply<R>(lam + h * batch * dim, p.n, batch, op, mats, p.per_sample, cpool, true, sm, st),
                    "gate kernel");
             }
+        }
+        if (next_bwd < L.norm_bwd.size() && L.norm_bwd[next_bwd] == q) {
+            norm_check(W);   // psi before pass q, rebuilt by reverse application
+            ++next_bwd;
         }
     }
     TimeScope ts(TK_SCATTER, st);
@@ -666,6 +716,11 @@ extern "C" {
 const char *mqb_last_error(void) { return g_last_error.c_str(); }
 
 int mqb_version(void) { return 100; }
+
+int mqb_inject_alloc_failure(int after) {
+    t_alloc_countdown = after < 0 ? -1 : after;
+    return MQB_OK;
+}
 
 int mqb_device_error(int *code, int clear) {
     return guarded([&] {
@@ -931,6 +986,10 @@ int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const ui
         if (!out) fail(MQB_ERR_INVALID, "out is null");
         *out = nullptr;
         if (n_qubits < 1 || n_qubits > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
+        if (precision != MQB_PREC_C64 && precision != MQB_PREC_C128) fail(MQB_ERR_INVALID, "bad precision %d", precision);
+        if (n_terms < 0) fail(MQB_ERR_INVALID, "n_terms must be >= 0, got %d", n_terms);
+        if (n_terms > 0 && (!mask_x || !mask_y || !mask_z || !num_y || !coeff))
+            fail(MQB_ERR_INVALID, "null term arrays for %d terms", n_terms);
         const uint64_t allq = (uint64_t(1) << n_qubits) - 1;
         std::vector<uint64_t> mx, my, mz;
         std::vector<int> ny;
@@ -1022,7 +1081,7 @@ int mqb_ham_create_csr(int n_qubits, int precision, int64_t nnz, const int64_t *
         h->d_slice_len = upload(slen);
         h->d_cols = upload(cols);
         if (entries > 0) {
-            ck(cudaMalloc(&h->d_vals, vals.size()), "cudaMalloc");
+            dev_alloc(&h->d_vals, vals.size(), "cudaMalloc");
             ck(cudaMemcpy(h->d_vals, vals.data(), vals.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
         }
         *out = h.release();
@@ -1104,6 +1163,27 @@ int mqb_grad_workspace_size(const mqb_program *p, int64_t batch, int n_hams, int
         if (n_hams < 1) fail(MQB_ERR_INVALID, "need at least one Hamiltonian");
         SchedDev &sd = grad_schedule(const_cast<mqb_program &>(*p), n_hams);
         *bytes = grad_layout(*p, sd.s, batch, n_hams, stride).total;
+    });
+}
+
+int mqb_grad_norm_checks(mqb_program *p, const void *ws, size_t ws_bytes, int64_t batch, int n_hams, int stride,
+                         double *out, int capacity, int *n_checks, void *stream) {
+    return guarded([&] {
+        if (!p || !n_checks) fail(MQB_ERR_INVALID, "null argument");
+        if (n_hams < 1 || batch < 1) fail(MQB_ERR_INVALID, "invalid batch or number of Hamiltonians");
+        SchedDev &sd = grad_schedule(*p, n_hams);
+        const GradLayout L = grad_layout(*p, sd.s, batch, n_hams, stride);
+        const int n = int(L.norm_fwd.size() + L.norm_bwd.size());
+        *n_checks = n;
+        if (n == 0 || !out) return;
+        if (!ws || ws_bytes < L.total) fail(MQB_ERR_WORKSPACE, "workspace too small (%zu < %zu)", ws_bytes, L.total);
+        if (capacity < n) fail(MQB_ERR_INVALID, "capacity %d below the %d checks", capacity, n);
+        const unsigned char *base = static_cast<const unsigned char *>(ws) + L.mats + L.gslots + L.lam + L.w + L.ckpt;
+        std::vector<double> raw(size_t(n) * batch * 2);
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        ck(cudaMemcpyAsync(raw.data(), base, raw.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        for (size_t i = 0; i < size_t(n) * batch; ++i) out[i] = raw[2 * i];
     });
 }
 

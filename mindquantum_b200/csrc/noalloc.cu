@@ -2,16 +2,16 @@
 //
 // mqb_apply needs a caller-provided workspace for the per-sample gate matrices that the matrix
 // generation kernel writes and the tile kernels read.  Some callers cannot call cudaMalloc (or
-// any allocating routine) when they apply a circuit: code that runs while a framework is
-// recording a CUDA graph and forbids allocations during the capture, runtimes that reserve all
-// device memory in a fixed pool at start-up, and thin language bindings that only own the state
-// buffers they pass in.  This entry point uses a fixed scratch array that lives in the library's
-// own device memory instead.
+// any allocating routine) when they apply a circuit: runtimes that reserve all device memory in a
+// fixed pool at start-up, thin language bindings that only own the state buffers they pass in,
+// and real-time loops that must not call into the allocator.  This entry point uses a fixed
+// scratch array that lives in the library's own device memory instead.
 //
 // The scratch is a file-scope __device__ array of kStaticScratchBytes (4 MiB).  Every GPU that
 // loads this library holds it until the process exits.  Its device address is looked up once per
 // device with cudaGetSymbolAddress the first time the entry point runs with that device current,
-// so that first call should come before any stream capture.  All calls share the one array:
+// so that first call should come before any stream capture; a device reset invalidates the cached
+// address (the entry point must not be used after cudaDeviceReset).  All calls share the one array:
 // calls whose work overlaps on the GPU (different streams, or different host threads without
 // ordering) race on it.  Nothing in it needs to start at zero: every call overwrites the
 // matrices it reads before reading them.

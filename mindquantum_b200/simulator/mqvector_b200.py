@@ -58,6 +58,11 @@ def _split_inputs(version, enc_names, ans_names, inputs_):
     return enc, ans
 
 
+# |<psi|psi> - 1| above which a complex64 gradient whose backward sweep rebuilt states by reverse
+# application warns (its gradients then carry errors of the same order)
+NORM_DRIFT_WARN = 1e-4
+
+
 def _require_cuda():
     if not torch.cuda.is_available():
         raise RuntimeError("the mqvector_b200 backend needs a CUDA device (B200, sm_100a); none is visible")
@@ -536,7 +541,32 @@ class MQVectorB200(BackendBase):
         N.call('mqb_expectation_with_grad', prog.handle, ham_arr, len(nh), _ptr(init), init_batched, batch,
                _ptr(params), params.shape[1] if params.dim() == 2 else 0, _ptr(custom), _ptr(f), _ptr(g), stride,
                _ptr(ws), ws_bytes.value, _stream())
+        # the workspace keeps this call's FP64 norm checks until the next call (norm_checks())
+        self._last_grad = (prog, ws, ws_bytes.value, batch, len(nh), stride)
         return f, g[:, :, :len(param_names)]
+
+    def norm_checks(self):
+        """<psi|psi> in FP64 at the norm checks of the last complex64 gradient call: [checks][batch].
+
+        The checks follow every ceil(sqrt(P))-th of the P forward passes and the last one, then every
+        ceil(sqrt(P))-th state the backward sweep rebuilds by applying passes in reverse (checkpoint
+        stride 0 or > 1).  Empty for complex128.  Synchronizes the stream."""
+        if getattr(self, '_last_grad', None) is None:
+            return np.zeros((0, 0))
+        prog, ws, ws_bytes, batch, n_hams, stride = self._last_grad
+        n = ctypes.c_int()
+        N.call('mqb_grad_norm_checks', prog.handle, _ptr(ws), ws_bytes, batch, n_hams, stride, None, 0,
+               ctypes.byref(n), _stream())
+        out = np.zeros((max(1, n.value), batch), dtype=np.float64)
+        if n.value:
+            N.call('mqb_grad_norm_checks', prog.handle, _ptr(ws), ws_bytes, batch, n_hams, stride,
+                   out.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n), _stream())
+        return out[:n.value]
+
+    def norm_drift(self):
+        """max |<psi|psi> - 1| over the norm checks of the last gradient call (0.0 without checks)."""
+        c = self.norm_checks()
+        return float(np.max(np.abs(c - 1.0))) if c.size else 0.0
 
     def _choose_stride(self, prog, batch, n_hams):
         """Store the state after every pass when it fits in 85% of free memory, else every sqrt(P) passes.
@@ -600,6 +630,13 @@ class MQVectorB200(BackendBase):
             f, g = sim.expectation_with_grad_tensor(hams, circ_right, torch.as_tensor(params), names, init_state=init)
             f = f.cpu().numpy()
             g = g.cpu().numpy()
+            if sim.precision == N.MQB_PREC_C64 and sim._last_grad[5] != 1:
+                # states rebuilt by reverse application: report a norm that moved
+                drift = sim.norm_drift() if init is None else 0.0
+                if drift > NORM_DRIFT_WARN:
+                    warnings.warn(f"complex64 gradient: the state's norm drifted by {drift:.2e} while the backward "
+                                  f"sweep rebuilt it (checkpoint stride {sim._last_grad[5]}); use complex128 or "
+                                  f"more memory for stored states", RuntimeWarning, stacklevel=2)
             fc = f[..., 0] + 1j * f[..., 1]
             gc = g.astype(np.complex128)
             if version == 'both':

@@ -1,9 +1,10 @@
 """The allocation-free entry point mqb_apply_static against mqb_apply (GPU).
 
 mqb_apply_static serves callers that cannot allocate device memory when they apply a circuit
-(for example while a framework records a CUDA graph, or inside a runtime whose device memory is
-a fixed pool): it keeps the per-sample gate matrices in a fixed 4 MiB array inside the library
-instead of a caller workspace.  This file is collected last so a failure here does not stop the
+(a runtime whose device memory is a fixed pool, a binding that only owns the state buffers): it
+keeps the per-sample gate matrices in a fixed 4 MiB array inside the library instead of a caller
+workspace, and runs the precompiled tile kernels only.  At 18 qubits and more mqb_apply runs the
+generated pass kernels instead, so that case compares two kernel families.  This file is collected last so a failure here does not stop the
 other tests; it also passes when run alone in a fresh process.
 """
 import ctypes
@@ -39,10 +40,11 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
 
 
+@pytest.mark.parametrize("n", [14, 18])
 @pytest.mark.parametrize("precision,tol", [(N.MQB_PREC_C64, 1e-6), (N.MQB_PREC_C128, 1e-12)])
-def test_static_scratch_matches_workspace_path(precision, tol):
+def test_static_scratch_matches_workspace_path(precision, tol, n):
     L = _lib()
-    n, batch = 14, 3
+    batch = 3
     circ = _circuit(n, 3)
     names = circ.params_name
     prog = lowering.Program(circ, n, precision, names)
