@@ -378,6 +378,10 @@ def run_b200(args, rank, world, local_rank):
         extras["c128_fused"] = {"value": 1.0 / t128, "unit": UNIT, "batch": 1}
         extras.update(oracle_fixture_errors(n, layers, B, rank, f[0, 0, 0].item(), g[0, 0].cpu().numpy(),
                                             f128[0, 0, 0].item(), g128[0, 0].cpu().numpy()))
+        checks = sim.norm_checks()   # the last timed step's FP64 norm checks (complex64 state)
+        extras["norm_check"] = {"checks": int(checks.shape[0]), "states_per_check": B,
+                                "max_abs_norm2_minus_1": float(np.max(np.abs(checks - 1.0))) if checks.size else None,
+                                "cadence": "after every ceil(sqrt(passes))-th forward pass and the last"}
         extras["apply"] = apply_throughput(sim, circ, names, params, n, B, 5, peak)
         extras["device_error"] = N.device_error()
         if not args.skip_plain:
