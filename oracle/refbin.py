@@ -1,0 +1,109 @@
+"""The reference's own CPU simulator (built from its sources by oracle/Makefile into
+oracle/_ref/libmqref.so).  TEST INFRASTRUCTURE ONLY: tests/ use it to pin the oracle (and the CUDA
+path) to the reference itself, and bench.py times it as the CPU baseline; the product never does.
+
+Supported gates: X, Y, Z, H (at most one control), RX, RY, RZ, Rzz and PhaseShift whose angle is
+``coeff * p + const`` of at most one parameter.  Hamiltonians: Pauli strings with real coefficients.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref.so')
+_KINDS = {'X': 0, 'H': 1, 'RX': 2, 'RY': 3, 'RZ': 4, 'Z': 5, 'Rzz': 6, 'Y': 7, 'PS': 8}
+_lib = None
+
+
+def available():
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib  # pylint: disable=global-statement
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} is not built (make -C oracle ref, with the reference checkout)")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        L.mqref_apply.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, ctypes.c_int, P]
+        for fn in (L.mqref_grad, L.mqref_grad_c64):
+            fn.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, P, P, P, ctypes.c_int,
+                                                                    ctypes.c_int, P, ctypes.c_int, P]
+        _lib = L
+    return _lib
+
+
+def _gate_table(circ, names):
+    cols = {k: [] for k in ('kind', 'o0', 'o1', 'ctrl', 'param', 'coeff', 'cst')}
+    for g in circ:
+        name = 'PS' if g.name in ('PS', 'PhaseShift') else g.name
+        if name not in _KINDS or len(g.ctrl_qubits) > 1:
+            raise ValueError(f"gate {g.name} is not supported by the reference harness")
+        cols['kind'].append(_KINDS[name])
+        cols['o0'].append(int(g.obj_qubits[0]))
+        cols['o1'].append(int(g.obj_qubits[1]) if len(g.obj_qubits) > 1 else -1)
+        cols['ctrl'].append(int(g.ctrl_qubits[0]) if g.ctrl_qubits else -1)
+        prs = getattr(g, 'prs', None)
+        if prs:
+            pr = prs[0]
+            keys = list(pr.params_name)
+            if len(keys) > 1:
+                raise ValueError("one parameter per angle")
+            cols['param'].append(names.index(keys[0]) if keys else -1)
+            cols['coeff'].append(float(np.real(pr[keys[0]])) if keys else 0.0)
+            cols['cst'].append(float(np.real(pr.const)))
+        else:
+            cols['param'].append(-1)
+            cols['coeff'].append(0.0)
+            cols['cst'].append(0.0)
+    ints = {k: np.ascontiguousarray(cols[k], dtype=np.int32) for k in ('kind', 'o0', 'o1', 'ctrl', 'param')}
+    dbls = {k: np.ascontiguousarray(cols[k], dtype=np.float64) for k in ('coeff', 'cst')}
+    return ints, dbls
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def apply(n, circ, params, threads=0):
+    """VectorState::ApplyCircuit from |0...0> with parameter values ``params`` (circ.params_name order)."""
+    names = list(circ.params_name)
+    ints, dbls = _gate_table(circ, names)
+    out = np.zeros(2 << n, dtype=np.float64)
+    p = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+    st = lib().mqref_apply(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
+                           _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), len(names), _p(p), threads, _p(out))
+    if st != 0:
+        raise RuntimeError(f"mqref_apply failed ({st})")
+    return out[0::2] + 1j * out[1::2]
+
+
+def grad(n, circ, ham, params, threads=0, complex64=False):
+    """VectorState::GetExpectationWithGradMultiMulti for one Hamiltonian, every parameter an encoder
+    input: params [samples][n_params] -> [samples][1 + n_params] complex (f, then the gradient)."""
+    names = list(circ.params_name)
+    ints, dbls = _gate_table(circ, names)
+    tl, tq, tp, tc = [], [], [], []
+    for term, c in ham.ham_termlist:
+        tl.append(len(term))
+        tc.append(float(c))
+        for q, pch in term:
+            tq.append(int(q))
+            tp.append(pch)
+    tl = np.ascontiguousarray(tl, dtype=np.int32)
+    tq = np.ascontiguousarray(tq if tq else [0], dtype=np.int32)
+    tc = np.ascontiguousarray(tc, dtype=np.float64)
+    tpb = ctypes.create_string_buffer(''.join(tp).encode() or b'\0')
+    params = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
+    S = params.shape[0]
+    out = np.zeros(S * (1 + len(names)) * 2, dtype=np.float64)
+    fn = lib().mqref_grad_c64 if complex64 else lib().mqref_grad
+    st = fn(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']), _p(ints['param']),
+            _p(dbls['coeff']), _p(dbls['cst']), len(tl), _p(tl), _p(tq), ctypes.cast(tpb, ctypes.c_void_p), _p(tc),
+            len(names), S, _p(params), threads, _p(out))
+    if st != 0:
+        raise RuntimeError(f"mqref_grad failed ({st})")
+    out = out.reshape(S, 1 + len(names), 2)
+    return out[..., 0] + 1j * out[..., 1]

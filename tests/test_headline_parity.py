@@ -118,3 +118,29 @@ def test_headline_26_qubits_against_oracle_fixture(dtype, tol):
     f, g = _grad(fx['n_qubits'], dtype, circ, ham, params[:1])
     assert abs(f[0] - row['f']) <= tol
     assert np.max(np.abs(g[0] - np.array(row['grad']))) <= tol
+
+
+def _refbin():
+    from oracle import refbin as R
+
+    if not R.available():
+        pytest.skip("the reference simulator is not built (oracle/_ref)")
+    return R
+
+
+@pytest.mark.parametrize("dtype,tol", [(complex128, 1e-10), (complex64, 1e-5)])
+def test_cuda_path_against_the_reference_binary(dtype, tol):
+    """The default (generated-kernel) path at 20 qubits against the reference's own CPU simulator
+    (built from its sources), HEA and QAOA MaxCut."""
+    R = _refbin()
+    n = 20
+    circ, ham, params = W.hea(n, 4, 2, seed=12, encoder=True)
+    ref = R.grad(n, circ, ham, params)
+    f, g = _grad(n, dtype, circ, ham, params)
+    assert np.max(np.abs(f - ref[:, 0].real)) <= tol
+    assert np.max(np.abs(g - ref[:, 1:].real)) <= tol
+    circ, ham, pr, _ = W.qaoa_maxcut(n, 2, seed=13)
+    ref = R.grad(n, circ, ham, pr[None, :])
+    f, g = _grad(n, dtype, circ, ham, pr[None, :])
+    assert abs(f[0] - ref[0, 0].real) <= tol
+    assert np.max(np.abs(g[0] - ref[0, 1:].real)) <= tol

@@ -1,0 +1,56 @@
+"""The oracle against the reference's own CPU simulator, built from its sources (oracle/_ref).
+
+The reference (VectorState<CPUVectorPolicyAvxDouble>, its adjoint GetExpectationWithGradMultiMulti
+and ApplyCircuit) runs here on the host through oracle/refbin.py; these tests pin the oracle's
+restatement to it on the benchmark circuit families at full size where the host finishes in
+seconds: config 1 exactly (16 qubits x 8 layers), the QNN encoder/ansatz, QAOA MaxCut and random
+Pauli Hamiltonians with Y terms.  Tolerance: 1e-12 (both FP64), complex64 reference within 1e-5.
+Skipped where the reference checkout was not available to build the library.
+"""
+import numpy as np
+import pytest
+
+from mindquantum_b200 import workloads as W
+from oracle import oracle as O
+from oracle import refbin as R
+
+pytestmark = pytest.mark.skipif(not R.available(), reason="the reference simulator is not built (oracle/_ref)")
+
+
+def _oracle(n, circ, ham, params):
+    return O.get_expectation_with_grad(n, [ham], circ, params, np.zeros(0), circ.params_name, [])[:, 0]
+
+
+def test_config1_oracle_equals_reference():
+    n, layers = 16, 8
+    circ, ham, params = W.hea(n, layers, 1, seed=0, encoder=False)
+    ref = R.grad(n, circ, ham, params)
+    orc = _oracle(n, circ, ham, params)
+    assert np.max(np.abs(ref - orc)) <= 1e-12
+    qs = R.apply(n, circ, params[0])
+    oqs = O.OracleSim(n).apply_circuit(circ, dict(zip(circ.params_name, params[0].tolist()))).qs
+    assert np.max(np.abs(qs - oqs)) <= 1e-12
+    ref64 = R.grad(n, circ, ham, params, complex64=True)
+    assert np.max(np.abs(ref64 - orc)) <= 1e-5
+
+
+def test_qnn_oracle_equals_reference():
+    n = 12
+    circ, hams, enc, ans = W.qnn(n, 3, 3, n_obs=2, seed=11)
+    params = np.concatenate([enc, np.broadcast_to(ans, (enc.shape[0], ans.size))], axis=1)
+    for ham in hams:
+        assert np.max(np.abs(R.grad(n, circ, ham, params) - _oracle(n, circ, ham, params))) <= 1e-12
+
+
+def test_qaoa_oracle_equals_reference():
+    n, p = 12, 3
+    circ, ham, pr, _ = W.qaoa_maxcut(n, p, seed=5)
+    assert np.max(np.abs(R.grad(n, circ, ham, pr[None, :]) - _oracle(n, circ, ham, pr[None, :]))) <= 1e-12
+
+
+def test_random_pauli_hamiltonians_oracle_equals_reference():
+    n = 12
+    rng = np.random.default_rng(21)
+    circ, _, params = W.hea(n, 3, 2, seed=3, encoder=True)
+    ham = W.random_pauli_hamiltonian(n, 25, rng)
+    assert np.max(np.abs(R.grad(n, circ, ham, params) - _oracle(n, circ, ham, params))) <= 1e-12
