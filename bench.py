@@ -11,8 +11,9 @@ numpy.random.default_rng(0): angles first, then Hamiltonian coefficients.
 
 Under torchrun every rank runs its own batch (replicas, weak scaling, no data-path collective);
 the timed region is bracketed by a barrier and a device synchronize and the max over ranks is
-reported.  ``--impl reference`` times the reference algorithm's CPU implementation (the oracle
-port of the mqvector CPU kernels) on the host cores, one bounded sample per step.
+reported.  ``--impl reference`` times the reference's own CPU simulator (built from its sources into
+oracle/_ref; the oracle port of its kernels where that is not built) on the host cores: full
+gradient evaluations of the workload, at most three (a bounded run).
 """
 import argparse
 import ctypes
@@ -190,75 +191,65 @@ def apply_throughput(sim, circ, names, params, n, B, reps, peak):
             "bytes_model": "passes x 2 x S x B (every pass reads and writes each state once)"}
 
 
-def cpu_reference_sample(n, layers_total, threads, steps=1, warmup=0, dtype=np.complex64):
-    """Time the oracle port of the reference CPU algorithm on a bounded sample of the workload.
+def reference_full_evaluations(n, layers, batch, threads, count):
+    """Time full gradient evaluations of the workload on the host: the reference's own CPU
+    simulator (VectorState<CPUVectorPolicyAvxFloat>, built from the reference sources into
+    oracle/_ref), or the oracle port of its kernels where that library was not built.  One
+    evaluation = <H> and the full gradient of parameter set 0 (all layers, the real lambda = H psi),
+    complex64 like the benchmark.  Returns (seconds per evaluation list, kind)."""
+    from oracle import refbin as R
 
-    One sample = forward + adjoint sweep of ONE layer of the ansatz at full register size; the
-    Hamiltonian application + <psi|H psi> (same for every layer count) is timed once.  The full
-    evaluation time is t_H + layers_total * t_layer.
-    """
-    from oracle import oracle as O
-
-    O.set_num_threads(threads)
-    circ1, ham, params = build_workload(n, 1, 1)
-    prd = dict(zip(circ1.params_name, params[0].tolist()))
-    herm = [g.hermitian() for g in reversed(list(circ1))]
-    p_map = {k: i for i, k in enumerate(circ1.params_name)}
-
-    psi = O.zero_state(n, dtype)
-    for g in circ1:
-        O.apply_gate(psi, n, g, prd)
-    t0 = time.perf_counter()
-    lam = O.apply_terms(psi, n, ham)
-    O.vdot(psi, lam, n)
-    t_h = time.perf_counter() - t0
-    del lam
-
-    def one_layer():
-        s = O.zero_state(n, dtype)
-        for g in circ1:
-            O.apply_gate(s, n, g, prd)
-        lam_ = s.copy()     # stands in for H|psi>: the adjoint sweep costs the same for any lambda
-        f_g = np.zeros(1 + len(p_map), dtype=complex)
-        for g in herm:
-            O.apply_gate(s, n, g, prd)
-            if O.gate_requires_grad(g):
-                title, jac = O.jacobi(g)
-                intrin = np.array(O.expect_diff_gate(s, lam_, n, g, prd))
-                pg = intrin @ jac
-                for name, idx in title.items():
-                    f_g[1 + p_map[name]] += pg[idx]
-            O.apply_gate(lam_, n, g, prd)
-        return f_g
-
-    for _ in range(warmup):
-        one_layer()
+    circ, ham, params = build_workload(n, layers, batch)
     times = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        one_layer()
-        times.append(time.perf_counter() - t0)
-    t_layer = float(np.median(times))
-    t_eval = t_h + layers_total * t_layer
-    return {"value": 1.0 / t_eval, "t_h": t_h, "t_layer": t_layer, "t_eval": t_eval, "times": times}
+    if R.available():
+        kind = "reference"
+        for _ in range(count):
+            t0 = time.perf_counter()
+            R.grad(n, circ, ham, params[:1], threads=threads, complex64=True)
+            times.append(time.perf_counter() - t0)
+    else:
+        from oracle import oracle as O
+
+        kind = "port"
+        O.set_num_threads(threads)
+        for _ in range(count):
+            t0 = time.perf_counter()
+            O.get_expectation_with_grad(n, [ham], circ, params[:1], np.zeros(0), circ.params_name, [], np.complex64)
+            times.append(time.perf_counter() - t0)
+    return times, kind
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    r = cpu_reference_sample(args.qubits, args.layers, threads, steps=args.steps, warmup=args.warmup)
-    sample = (f"{args.qubits} qubits complex64, forward + adjoint sweep of 1 of {args.layers} layers per step plus one "
-              f"H application (51 terms); eval time = t_H + {args.layers} * t_layer")
+    # a bounded run: at most three full evaluations (each tens of seconds on the host), plus
+    # warm-up evaluations of one layer
+    from oracle import refbin as R
+
+    if R.available():
+        c1, h1, p1 = build_workload(args.qubits, 1, args.batch)
+        for _ in range(args.warmup):
+            R.grad(args.qubits, c1, h1, p1[:1], threads=threads, complex64=True)
+    count = max(1, min(args.steps, 3))
+    times, kind = reference_full_evaluations(args.qubits, args.layers, args.batch, threads, count)
+    t = float(np.mean(times))
+    value = 1.0 / t
+    sample = (f"full gradient evaluations (all {args.layers} layers, lambda = H psi, {2 * args.qubits * args.layers} "
+              f"gradients) of parameter set 0, "
+              f"{args.qubits} qubits complex64, {threads} host threads; {count} timed (of {args.steps} requested, "
+              f"bounded), {args.warmup} one-layer warm-ups")
     line = {
-        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": r["t_layer"] * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-        "config": {"workload": f"HEA {args.qubits}q x {args.layers} layers, 624 params, 51-term H, per-sample grad",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": count,
+        "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+        "config": {"workload": f"HEA {args.qubits}q x {args.layers} layers, {2 * args.qubits * args.layers} params, "
+                               f"{2 * args.qubits - 1}-term H, per-sample grad",
                    "n_qubits": args.qubits, "layers": args.layers, "batch": 1, "parallelism": "cpu"},
         "impl": "reference",
-        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
-        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
+                         "seconds": times},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -401,10 +392,10 @@ def run_b200(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         threads = os.cpu_count() or 1
-        r = cpu_reference_sample(n, layers, threads, steps=1, warmup=0)
-        cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{n} qubits complex64, forward + adjoint sweep of 1 of {layers} layers + one H "
-                         f"application; eval time = t_H + {layers} * t_layer = {r['t_eval']:.1f} s"}
+        times, kind = reference_full_evaluations(n, layers, B, threads, 1)
+        cpu = {"value": 1.0 / times[0], "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"one full gradient evaluation (all {layers} layers, lambda = H psi) of parameter set 0, "
+                         f"{n} qubits complex64: {times[0]:.1f} s"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
