@@ -28,6 +28,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+os.environ.setdefault('MQB_JIT_CACHE', os.path.join(ROOT, '_build', 'jit_cache'))
 METRIC = "grad evals/s at 26q c64-batched vs c128-plain, same B200, err≤1e-5; HBM GB/s"
 UNIT = "grad evals/s"
 

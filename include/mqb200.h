@@ -211,7 +211,7 @@ MQB_API int mqb_expectation(const mqb_hamiltonian *ham, const void *bra, const v
 MQB_API int mqb_apply_matrix1(int n_qubits, int precision, void *states, int64_t batch, int qubit,
                               uint64_t ctrl_mask, const double *matrix, void *stream);
 
-/* out[b] = <a_b|b_b> as (re, im) float64 on the device. *//* out[b] = <a_b|b_b> as (re, im) float64 on the device. */
+/* out[b] = <a_b|b_b> as (re, im) float64 on the device. */
 MQB_API int mqb_vdot(int n_qubits, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream);
 
 /* ------------------------------------------------------------------ adjoint gradient */

@@ -18,6 +18,8 @@
 #include <cstring>
 #include <functional>
 
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <atomic>
 #include <memory>
@@ -1065,6 +1067,57 @@ std::string backward_source(const Schedule &s, const Pass &p, int precision, int
     return o.str();
 }
 
+// On-disk cache of the cubins compiled here, so a new process does not compile the same pass
+// kernels again: MQB_JIT_CACHE names the directory ("0" disables it; default
+// $XDG_CACHE_HOME/mqb200 or ~/.cache/mqb200).  An entry is keyed by a 64-bit hash of everything
+// the compile reads (the source, the embedded headers, the options, the NVRTC version) and stores
+// that input next to the cubin, which is loaded only when the stored input equals the current
+// one.  The cubins are stored and loaded, never inspected.
+std::string cache_dir() {
+    const char *e = std::getenv("MQB_JIT_CACHE");
+    if (e) return std::string(e) == "0" ? std::string() : std::string(e);
+    if (const char *x = std::getenv("XDG_CACHE_HOME")) return std::string(x) + "/mqb200";
+    if (const char *h = std::getenv("HOME")) return std::string(h) + "/.cache/mqb200";
+    return std::string();
+}
+
+std::string compile_input(const Entry &e, const char *const *opts, int n_opts) {
+    int major = 0, minor = 0;
+    nvrtcVersion(&major, &minor);
+    std::string in = "nvrtc " + std::to_string(major) + "." + std::to_string(minor) + "\n";
+    for (int i = 0; i < n_opts; ++i) in += std::string(opts[i]) + "\n";
+    for (const char *h : {kJitRegmath, kJitTile, kJitAbi, kJitPipe}) in += std::string(h) + "\n";
+    return in + e.src;
+}
+
+uint64_t fnv1a(const std::string &s) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char c : s) h = (h ^ c) * 1099511628211ull;
+    return h;
+}
+
+bool read_file(const std::string &path, std::string &out) {
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    std::string buf;
+    char tmp[65536];
+    size_t k;
+    while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.append(tmp, k);
+    std::fclose(f);
+    out.swap(buf);
+    return true;
+}
+
+void write_file_atomic(const std::string &path, const char *data, size_t n) {
+    const std::string tmp = path + ".tmp" + std::to_string(std::hash<std::thread::id>()(std::this_thread::get_id()));
+    FILE *f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return;
+    const bool ok = std::fwrite(data, 1, n, f) == n;
+    std::fclose(f);
+    if (ok) std::rename(tmp.c_str(), path.c_str());
+    else std::remove(tmp.c_str());
+}
+
 void compile_entry(Entry &e) {
     // MQB_JIT_DUMP=<directory>: write every generated source there (for reading them)
     if (const char *dir = std::getenv("MQB_JIT_DUMP")) {
@@ -1082,6 +1135,21 @@ void compile_entry(Entry &e) {
         return;
     }
     const char *opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "-lineinfo"};
+    const std::string dir = cache_dir();
+    std::string input, key_path;
+    if (!dir.empty()) {
+        input = compile_input(e, opts, 3);
+        char hex[17];
+        std::snprintf(hex, sizeof(hex), "%016llx", static_cast<unsigned long long>(fnv1a(input)));
+        key_path = dir + "/" + hex;
+        std::string stored, cubin;
+        if (read_file(key_path + ".in", stored) && stored == input && read_file(key_path + ".cubin", cubin) &&
+            !cubin.empty()) {
+            e.cubin.assign(cubin.begin(), cubin.end());
+            nvrtcDestroyProgram(&prog);
+            return;
+        }
+    }
     const nvrtcResult r = nvrtcCompileProgram(prog, 3, opts);
     size_t log_n = 0;
     nvrtcGetProgramLogSize(prog, &log_n);
@@ -1092,6 +1160,13 @@ void compile_entry(Entry &e) {
         nvrtcGetCUBINSize(prog, &n);
         e.cubin.resize(n);
         nvrtcGetCUBIN(prog, e.cubin.data());
+        if (!key_path.empty()) {
+            std::string cmd = dir;   // create the directory (and parents) if needed
+            for (size_t i = 1; i <= cmd.size(); ++i)
+                if (i == cmd.size() || cmd[i] == '/') mkdir(cmd.substr(0, i).c_str(), 0755);
+            write_file_atomic(key_path + ".cubin", e.cubin.data(), e.cubin.size());
+            write_file_atomic(key_path + ".in", input.data(), input.size());
+        }
     } else {
         e.log = std::string(nvrtcGetErrorString(r)) + "\n" + log;
     }

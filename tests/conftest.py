@@ -10,6 +10,8 @@ if ROOT not in sys.path:
 HERE = os.path.dirname(os.path.abspath(__file__))
 if HERE not in sys.path:
     sys.path.insert(0, HERE)
+# compiled pass kernels are cached inside the repository's build folder
+os.environ.setdefault('MQB_JIT_CACHE', os.path.join(ROOT, '_build', 'jit_cache'))
 
 
 def pytest_configure(config):
