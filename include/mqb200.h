@@ -78,8 +78,13 @@ typedef struct mqb_gate_desc {
                                      custom parameterized gates: offset into the per-sample custom block */
     uint64_t pauli_x, pauli_y, pauli_z; /* rotation about a Pauli string (GID_RPS), global masks */
     int32_t pauli_ny;
-    int32_t reserved;
+    int32_t flags;                /* MQB_GATE_NONUNITARY: the constant matrix is not unitary (the
+                                     superoperator of a noise channel on a vectorized density matrix):
+                                     it runs in a pass of its own, never inside a fused pass, and
+                                     gradients through it need checkpoint stride 1 */
 } mqb_gate_desc;
+
+#define MQB_GATE_NONUNITARY 1
 
 typedef struct mqb_param_term {
     int32_t param;

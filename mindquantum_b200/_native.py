@@ -13,6 +13,7 @@ from .build_native import LIB, build
 MQB_OK = 0
 MQB_PREC_C64 = 0
 MQB_PREC_C128 = 1
+MQB_GATE_NONUNITARY = 1
 MQB_MAX_OBJ = 6
 MQB_MAX_ANGLES = 3
 
@@ -33,7 +34,7 @@ class GateDesc(ctypes.Structure):
         ('pauli_y', ctypes.c_uint64),
         ('pauli_z', ctypes.c_uint64),
         ('pauli_ny', ctypes.c_int32),
-        ('reserved', ctypes.c_int32),
+        ('flags', ctypes.c_int32),
     ]
 
 

@@ -194,6 +194,8 @@ struct mqb_program {
     int n_slots = 0;
     int32_t *d_csr_ptr = nullptr, *d_csr_slot = nullptr;
     double *d_csr_coeff = nullptr;
+    std::vector<char> no_fuse;   // per op: MQB_GATE_NONUNITARY
+    bool nonunitary = false;
     std::unique_ptr<SchedDev> apply_sched;
     std::map<int, std::unique_ptr<SchedDev>> grad_sched;   // by number of Hamiltonians
     ~mqb_program() {
@@ -243,7 +245,7 @@ static std::unique_ptr<SchedDev> make_sched(const mqb_program &p, int K, bool fu
     // the register kernels need 2^5..2^8 threads of 2^reg_bits amplitudes: smaller registers use
     // the per-gate kernels
     if (K < reg_bits + 5) fuse = false;
-    sd->s = build_schedule(p.n, K, contiguity_bits(p.precision), p.ops, fuse);
+    sd->s = build_schedule(p.n, K, contiguity_bits(p.precision), p.ops, fuse, &p.no_fuse);
     build_stages(sd->s, p.ops, reg_bits, p.precision, false);
     build_stages(sd->s, p.ops, fwd_reg_bits(p.precision), p.precision, true);
     sd->s.d_pass_ops = upload(sd->s.pass_ops);
@@ -471,6 +473,9 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
                       double *f, double *grad, int stride, void *ws, size_t ws_bytes, cudaStream_t st,
                       const void *lam_in = nullptr, int lam_batched = 0) {
     using V = cplx<R>;
+    if (p.nonunitary && stride != 1)
+        fail(MQB_ERR_INVALID, "programs with non-unitary operators need checkpoint stride 1 (every pass stored), got %d",
+             stride);
     SchedDev &sd = grad_schedule(p, n_hams);
     const Schedule &s = sd.s;
     const GradLayout L = grad_layout(p, s, batch, n_hams, stride);
@@ -584,6 +589,11 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
             V *psi_q;
             if (q > 0 && stored_q) {
                 psi_q = ckpt(q);
+            } else if (q == 0) {
+                // the initial state itself (applying the op in reverse would not undo a non-unitary op)
+                TimeScope ts(TK_OTHER, st);
+                ck(launch_copy_or_zero<R>(W, init_v, p.n, batch, init_stride, st), "state copy");
+                psi_q = W;
             } else {
                 V *src = loc(q + 1);
                 if (src != W) {
@@ -795,6 +805,13 @@ int mqb_program_create(int n_qubits, int precision, const mqb_gate_desc *gates, 
         p->tile_bits = options ? options->tile_bits : 0;
         p->jit = options ? options->jit : 0;
         p->descs.assign(gates, gates + n_gates);
+        p->no_fuse.assign(size_t(n_gates), 0);
+        for (int k = 0; k < n_gates; ++k)
+            if (gates[k].flags & MQB_GATE_NONUNITARY) {
+                if (gates[k].gate_id != GID_MATRIX) fail(MQB_ERR_INVALID, "gate %d: only constant matrices can be non-unitary", k);
+                p->no_fuse[size_t(k)] = 1;
+                p->nonunitary = true;
+            }
         std::vector<std::complex<double>> pool;
         std::vector<std::vector<std::pair<int32_t, double>>> csr(std::max(0, n_params));
         int64_t cursor = 0;

@@ -193,7 +193,9 @@ class JitBlock {
 };
 
 // Builders (scheduler.cpp)
-Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool fuse);
+// no_fuse (optional, one entry per op): ops that must run in a pass of their own.
+Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool fuse,
+                        const std::vector<char> *no_fuse = nullptr);
 // Split every fused pass of `s` into register stages with `reg_bits` register bits per thread:
 // the backward layout (Schedule::stages) or, with `forward`, the forward layout (f_stages).
 void build_stages(Schedule &s, const std::vector<DevOp> &ops, int reg_bits, int precision, bool forward = false);

@@ -75,7 +75,8 @@ static uint64_t touched(const DevOp &op) {
 
 static bool fusable(const DevOp &op) { return (op.kind == KIND_DENSE || op.kind == KIND_DIAG) && op.m <= kMaxFusedM; }
 
-Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool fuse) {
+Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool fuse, const std::vector<char> *no_fuse) {
+    auto fusable_at = [&](int i) { return fusable(ops[i]) && !(no_fuse && (*no_fuse)[i]); };
     Schedule s;
     if (K > n) K = n;
     // leave room for the widest fused gate next to the contiguity bits; keep at least one
@@ -91,7 +92,7 @@ Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool
     const uint64_t all = n >= 64 ? ~uint64_t(0) : ((uint64_t(1) << n) - 1);
     while (n_done < L) {
         while (first < L && done[first]) ++first;
-        if (!fuse || !fusable(ops[first])) {
+        if (!fuse || !fusable_at(first)) {
             Pass p;
             p.fused = 0;
             p.op_begin = first;
@@ -116,7 +117,7 @@ Schedule build_schedule(int n, int K, int c, const std::vector<DevOp> &ops, bool
                 if ((blocked & all) == all) break;
                 continue;
             }
-            if (!fusable(op)) {
+            if (!fusable_at(i)) {
                 blocked |= t;
                 continue;
             }

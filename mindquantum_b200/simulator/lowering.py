@@ -90,6 +90,8 @@ def lower_circuit(circuit, param_names, grad_names=None):
             d.n_obj = len(objs)
             for i, q in enumerate(objs):
                 d.obj[i] = q
+            # a channel's superoperator on a vectorized density matrix: never fused
+            d.flags = N.MQB_GATE_NONUNITARY if getattr(g, 'nonunitary', False) else 0
             d.matrix_offset = sum(x.size for x in pool)
             pool.append(m.reshape(-1))
         descs.append(d)

@@ -4,14 +4,18 @@ import numpy as np
 from ..dtype import to_mq_type
 from .backend_base import BackendBase
 
-SUPPORTED_SIMULATOR = ('mqvector_b200', 'mqvector_gpu')
+SUPPORTED_SIMULATOR = ('mqvector_b200', 'mqvector_gpu', 'mqmatrix_b200', 'mqmatrix_gpu')
 
 
 def _make_backend(name, n_qubits, seed, dtype, **kwargs):
-    from .mqvector_b200 import MQVectorB200  # pylint: disable=import-outside-toplevel
+    # pylint: disable=import-outside-toplevel
+    from .mqmatrix_b200 import MQMatrixB200
+    from .mqvector_b200 import MQVectorB200
 
     if name not in SUPPORTED_SIMULATOR:
         raise ValueError(f"backend {name} not supported, supported backends: {SUPPORTED_SIMULATOR}")
+    if name.startswith('mqmatrix'):
+        return MQMatrixB200(name, n_qubits, seed, dtype, **kwargs)
     return MQVectorB200(name, n_qubits, seed, dtype, **kwargs)
 
 
@@ -19,7 +23,8 @@ class Simulator:
     """Quantum simulator.
 
     Args:
-        backend (Union[str, BackendBase]): ``'mqvector_b200'`` (alias ``'mqvector_gpu'``) or a backend object.
+        backend (Union[str, BackendBase]): ``'mqvector_b200'`` (alias ``'mqvector_gpu'``), the density-matrix
+            ``'mqmatrix_b200'`` (alias ``'mqmatrix_gpu'``) or a backend object.
         n_qubits (int): number of qubits.
         seed (int): random seed of measurements and sampling.
         dtype: ``complex128`` (default) or ``complex64``.
@@ -91,6 +96,33 @@ class Simulator:
         return f"{self.backend.device_name()}"
 
     __repr__ = __str__
+
+    # density-matrix methods (mqsim.py:546-600); a state vector is pure
+    def purity(self):
+        fn = getattr(self.backend, 'purity', None)
+        return fn() if fn else 1.0
+
+    def entropy(self):
+        fn = getattr(self.backend, 'entropy', None)
+        return fn() if fn else 0.0
+
+    def get_partial_trace(self, obj_qubits):
+        if isinstance(obj_qubits, int):
+            obj_qubits = [obj_qubits]
+        if not hasattr(self.backend, 'get_partial_trace'):
+            raise ValueError(f"{self.backend.name} simulator not support partial trace method.")
+        return self.backend.get_partial_trace(list(obj_qubits))
+
+    def get_reduced_density_matrix(self, kept_qubits):
+        if isinstance(kept_qubits, int):
+            kept_qubits = [kept_qubits]
+        if not hasattr(self.backend, 'get_reduced_density_matrix'):
+            raise ValueError(f"{self.backend.name} simulator not support reduced density matrices.")
+        return self.backend.get_reduced_density_matrix(list(kept_qubits))
+
+    def get_pure_state_vector(self):
+        fn = getattr(self.backend, 'get_pure_state_vector', None)
+        return fn() if fn else self.get_qs()
 
 
 def inner_product(bra_simulator, ket_simulator):

@@ -982,3 +982,189 @@ def sampling_measure_ending(n, circ, prd, shots, seed, dtype=np.complex128, init
     for c, q in enumerate(m_qids):
         out[:, c] = (res >> q) & 1
     return keys, out
+
+
+# ----------------------------------------------------------------------- density matrices (mqmatrix)
+# Dense restatements of the reference's density-matrix simulator (DensityMatrixState,
+# ccsrc/include/simulator/densitymatrix/densitymatrix_state.tpp) for small registers, the way the
+# reference's own tests check it (tests/st/test_simulator/test_method_of_mqmatrix.py builds the
+# same dense products).  rho[i][j] with index bit q <-> qubit q.
+
+def dm_gate_matrix(n, g, prd):
+    """The 2^n x 2^n matrix of a unitary gate (with its controls): the oracle's own gate kernels
+    applied to every basis state."""
+    dim = 1 << n
+    U = np.zeros((dim, dim), dtype=np.complex128)
+    for j in range(dim):
+        e = np.zeros(dim, dtype=np.complex128)
+        e[j] = 1
+        apply_gate(e, n, g, prd)
+        U[:, j] = e
+    return U
+
+
+def _embed1(n, q, m):
+    """A single-qubit operator m on qubit q of n, as a 2^n x 2^n matrix."""
+    out = np.array([[1.0 + 0j]])
+    for k in reversed(range(n)):
+        out = np.kron(out, m if k == q else np.eye(2))
+    return out
+
+
+def dm_kraus_1q(g):
+    """Kraus operators of a single-qubit channel as the reference's density-matrix policy applies
+    them (cpu_densitymatrix_core_channel.cpp: ApplyPauli, ApplyAmplitudeDamping with its daggered
+    form, ApplyPhaseDamping, ApplyKraus)."""
+    if g.name in ('PC', 'BFC', 'PFC', 'BPFC'):
+        px, py, pz = g.px, g.py, g.pz
+        out = []
+        for p, m in ((px, [[0, 1], [1, 0]]), (py, [[0, -1j], [1j, 0]]), (pz, [[1, 0], [0, -1]]),
+                     (1 - px - py - pz, [[1, 0], [0, 1]])):
+            if p > 1e-8:
+                out.append(np.sqrt(p) * np.array(m, dtype=np.complex128))
+        return out
+    if g.name == 'ADC':
+        k0 = np.array([[1, 0], [0, np.sqrt(1 - g.gamma)]], dtype=np.complex128)
+        if getattr(g, 'hermitianed', False):
+            return [k0, np.array([[0, 0], [np.sqrt(g.gamma), 0]], dtype=np.complex128)]
+        return [k0, np.array([[0, np.sqrt(g.gamma)], [0, 0]], dtype=np.complex128)]
+    if g.name == 'PDC':
+        return [np.array([[1, 0], [0, np.sqrt(1 - g.gamma)]], dtype=np.complex128),
+                np.array([[0, 0], [0, np.sqrt(g.gamma)]], dtype=np.complex128)]
+    return [np.asarray(k, dtype=np.complex128) for k in g.kraus_op]
+
+
+def dm_apply_channel(rho, n, g):
+    """DensityMatrixState::ApplyChannel (densitymatrix_state.tpp:465-505): the channel's exact map."""
+    objs = list(g.obj_qubits)
+    if g.name == 'GPC':
+        for q, row in zip(objs, g.probs):
+            px, py, pz = (float(v) for v in row)
+            from types import SimpleNamespace
+
+            rho = dm_apply_channel(rho, n, SimpleNamespace(name='PC', px=px, py=py, pz=pz, obj_qubits=[q]))
+        return rho
+    if g.name == 'DC':
+        # (1 - p) rho + p (I / 2^k  (x)  Tr_objs rho)   (ApplyDepolarizing)
+        k = len(objs)
+        paulis = [np.eye(2), np.array([[0, 1], [1, 0]]), np.array([[0, -1j], [1j, 0]]), np.array([[1, 0], [0, -1]])]
+        tw = np.zeros_like(rho)
+        import itertools
+
+        for combo in itertools.product(range(4), repeat=k):
+            P = np.eye(1 << n, dtype=np.complex128)
+            for q, c in zip(objs, combo):
+                P = P @ _embed1(n, q, paulis[c])
+            tw += P @ rho @ P.conj().T
+        return (1 - g.p) * rho + g.p / 4 ** k * tw
+    if g.name == 'TRC':
+        # ApplyThermalRelaxation: rho_00 += (1 - e1) rho_11, coherences x e2, rho_11 x e1
+        e1 = np.exp(-g.gate_time / g.t1)
+        e2 = np.exp(-g.gate_time / g.t2)
+        q = objs[0]
+        dim = 1 << n
+        idx = np.arange(dim)
+        b = (idx >> q) & 1
+        out = rho.copy()
+        r1c1 = (b[:, None] == 1) & (b[None, :] == 1)
+        off = b[:, None] != b[None, :]
+        out[off] *= e2
+        out[r1c1] *= e1
+        # rho_00 block gains (1 - e1) of rho_11 block (same other bits)
+        lo = idx[b == 0]
+        out[np.ix_(lo, lo)] += (1 - e1) * rho[np.ix_(lo | (1 << q), lo | (1 << q))]
+        return out
+    out = np.zeros_like(rho)
+    for K in dm_kraus_1q(g):
+        Kf = _embed1(n, objs[0], K)
+        out += Kf @ rho @ Kf.conj().T
+    return out
+
+
+def dm_apply_circuit(n, circ, prd, rho):
+    """DensityMatrixState::ApplyCircuit (densitymatrix_state.tpp:743) for gates and channels."""
+    rho = np.array(rho, dtype=np.complex128)
+    for g in circ:
+        if is_channel(g):
+            rho = dm_apply_channel(rho, n, g)
+        elif g.name in ('BARRIER', 'I'):
+            continue
+        else:
+            U = dm_gate_matrix(n, g, prd)
+            rho = U @ rho @ U.conj().T
+    return rho
+
+
+def dm_expectation(n, ham, rho):
+    """Tr(H rho) (GetStateExpectation of the density-matrix policy)."""
+    return complex(np.trace(ham_matrix(n, ham) @ rho))
+
+
+def ham_matrix(n, ham):
+    """The 2^n x 2^n matrix of a Pauli Hamiltonian, columns by apply_terms on basis states."""
+    dim = 1 << n
+    Hm = np.zeros((dim, dim), dtype=np.complex128)
+    for j in range(dim):
+        e = np.zeros(dim, dtype=np.complex128)
+        e[j] = 1
+        Hm[:, j] = apply_terms(e, n, ham)
+    return Hm
+
+
+def dm_expectation_with_grad(n, hams, circ, params, names, rho0):
+    """f = Tr(H E(rho0)) and its gradient for every parameter row: d/dtheta of the map's output
+    (dU rho U^dag + U rho dU^dag at every gate holding the parameter, then the rest of the map),
+    which is the quantity the reference's GetExpectationWithReversibleGrad / NoiseGrad return.
+    Returns [rows][n_hams][1 + len(names)] complex."""
+    params = np.atleast_2d(np.asarray(params, dtype=np.float64))
+    gates = [g for g in circ if g.name not in ('BARRIER', 'I')]
+    Hs = [ham_matrix(n, h) for h in hams]
+    out = np.zeros((params.shape[0], len(hams), 1 + len(names)), dtype=complex)
+    for s, row in enumerate(params):
+        prd = dict(zip(names, row.tolist()))
+        states = [np.array(rho0, dtype=np.complex128)]
+        for g in gates:
+            states.append(dm_apply_circuit(n, [g], prd, states[-1]))
+        for h, Hm in enumerate(Hs):
+            out[s, h, 0] = np.trace(Hm @ states[-1])
+        for k, g in enumerate(gates):
+            if is_channel(g) or not getattr(g, 'parameterized', False):
+                continue
+            U = dm_gate_matrix(n, g, prd)
+            for name in names:
+                if not any(name in p.params_name for p in g.prs):
+                    continue
+                dU = _gate_diff_full(n, g, prd, name)
+                D = dU @ states[k] @ U.conj().T + U @ states[k] @ dU.conj().T
+                D = dm_apply_circuit(n, gates[k + 1:], prd, D)
+                for h, Hm in enumerate(Hs):
+                    out[s, h, 1 + names.index(name)] += np.trace(Hm @ D)
+    return out
+
+
+def _gate_diff_full(n, g, prd, name, eps=1e-6):
+    """d/d(name) of the gate's full matrix: sum over the gate's angles of d(angle)/d(name) times the
+    angle's derivative matrix (_diff_matrices, the reference's ExpectDiff matrices) embedded with
+    the controls (zero where the controls are not all set).  Pauli-string rotations use a central
+    difference of the exact matrices instead."""
+    dim = 1 << n
+    if g.name == 'RPS':
+        lo, hi = dict(prd), dict(prd)
+        lo[name] -= eps
+        hi[name] += eps
+        return (dm_gate_matrix(n, g, hi) - dm_gate_matrix(n, g, lo)) / (2 * eps)
+    objs, ctrls = list(g.obj_qubits), list(g.ctrl_qubits)
+    out = np.zeros((dim, dim), dtype=np.complex128)
+    for pr, dm in zip(g.prs, _diff_matrices(g, prd)):
+        if name not in pr.params_name:
+            continue
+        coeff = float(np.real(pr[name]))
+        dm = np.asarray(dm, dtype=np.complex128)
+        for j in range(dim):
+            e = np.zeros(dim, dtype=np.complex128)
+            e[j] = 1
+            e0 = e.copy()
+            apply_matrix(e, n, objs, ctrls, dm)
+            apply_matrix(e0, n, objs, ctrls, np.zeros_like(dm))
+            out[:, j] += coeff * (e - e0)
+    return out
