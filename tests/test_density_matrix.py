@@ -248,8 +248,9 @@ def test_pure_state_utilities_and_sampling():
     res = sim.sampling(mcirc, shots=4000, seed=5)
     probs = np.abs(psi) ** 2
     counts = np.zeros(8)
+    km = res.keys_map
     for row in res.samples:
-        counts[int(row[0]) | (int(row[1]) << 1) | (int(row[2]) << 2)] += 1
+        counts[int(row[km['q0']]) | (int(row[km['q1']]) << 1) | (int(row[km['q2']]) << 2)] += 1
     assert np.max(np.abs(counts / 4000 - probs)) < 0.03
 
 
