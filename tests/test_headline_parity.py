@@ -142,5 +142,6 @@ def test_cuda_path_against_the_reference_binary(dtype, tol):
     circ, ham, pr, _ = W.qaoa_maxcut(n, 2, seed=13)
     ref = R.grad(n, circ, ham, pr[None, :])
     f, g = _grad(n, dtype, circ, ham, pr[None, :])
-    assert abs(f[0] - ref[0, 0].real) <= tol
-    assert np.max(np.abs(g[0] - ref[0, 1:].real)) <= tol
+    scale = max(1.0, float(np.max(np.abs(ref))))   # QAOA values and gradients are O(10): relative bound
+    assert abs(f[0] - ref[0, 0].real) <= tol * scale
+    assert np.max(np.abs(g[0] - ref[0, 1:].real)) <= tol * scale
