@@ -579,9 +579,10 @@ def run_workload(args, rank, local_rank):
         def step():
             return batch(plist)
 
+        host_params = [x for _, _, _, x in members]
+
         def e2e_step():
-            fs, gs = batch([x for _, _, _, x in members])
-            return [f.cpu() for f in fs], [g.cpu() for g in gs]
+            return batch.evaluate(host_params)
 
         io = (sum(x.nbytes for _, _, _, x in members), sum(16 * (1 + len(c.params_name)) for _, c, _, _ in members))
         cfg = {"workload": "64 circuits of 12..24 qubits, 20 x (U3 on every qubit + brick CNOTs), own 10-term "

@@ -79,11 +79,32 @@ class CircuitBatch:
         if dtype not in (complex64, complex128):
             raise TypeError(f"dtype must be complex64 or complex128, got {dtype}")
         self.members = [_Member(n, c, h, self.precision, self.device) for n, c, h in members]
+        self._pack()
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, min(streams, len(self.members))))]
         self._plan(autotune, memory_fraction)
         self.graph = None
         if graph:
             self._capture()
+
+    def _pack(self):
+        """Every member's parameters, expectations and gradients as views into three device
+        buffers (the graph records the views' addresses), with pinned host mirrors: a call moves
+        the whole batch's inputs and outputs with one copy per buffer."""
+        n_p = [m.params.numel() for m in self.members]
+        n_f = [m.f.numel() for m in self.members]
+        n_g = [m.g.numel() for m in self.members]
+        self._p_off, self._f_off, self._g_off = (np.concatenate([[0], np.cumsum(x)]).astype(np.int64)
+                                                 for x in (n_p, n_f, n_g))
+        self.params_all = torch.zeros(int(self._p_off[-1]), dtype=torch.float64, device=self.device)
+        self.f_all = torch.zeros(int(self._f_off[-1]), dtype=torch.float64, device=self.device)
+        self.g_all = torch.zeros(int(self._g_off[-1]), dtype=torch.float64, device=self.device)
+        for i, m in enumerate(self.members):
+            m.params = self.params_all[self._p_off[i]:self._p_off[i + 1]].view(m.params.shape)
+            m.f = self.f_all[self._f_off[i]:self._f_off[i + 1]].view(m.f.shape)
+            m.g = self.g_all[self._g_off[i]:self._g_off[i + 1]].view(m.g.shape)
+        self._p_host = torch.zeros(self.params_all.numel(), dtype=torch.float64, pin_memory=True)
+        self._f_host = torch.zeros(self.f_all.numel(), dtype=torch.float64, pin_memory=True)
+        self._g_host = torch.zeros(self.g_all.numel(), dtype=torch.float64, pin_memory=True)
 
     # ------------------------------------------------------------------------------ planning
     def _plan(self, autotune, memory_fraction):
@@ -184,6 +205,36 @@ class CircuitBatch:
             f = m.f[0]
             out_f.append(torch.complex(f[:, 0], f[:, 1]))
             out_g.append(m.g[0, :, :len(m.names)])
+        return out_f, out_g
+
+    def evaluate(self, params_list):
+        """Host in, host out: every member's parameters gathered into one pinned buffer and copied
+        with one host-to-device copy, one replay, and the expectations and gradients of all members
+        read back with one device-to-host copy per buffer.  Returns (f, g): lists of numpy arrays,
+        f[i] [n_hams] complex, g[i] [n_hams][n_params]."""
+        if len(params_list) != len(self.members):
+            raise ValueError(f"expected {len(self.members)} parameter vectors, got {len(params_list)}")
+        host = self._p_host.numpy()
+        for i, (m, p) in enumerate(zip(self.members, params_list)):
+            p = np.asarray(p, dtype=np.float64).reshape(-1)
+            if p.size != len(m.names):
+                raise ValueError(f"member with {len(m.names)} parameters got {p.size} values")
+            host[self._p_off[i]:self._p_off[i] + p.size] = p
+        self.params_all.copy_(self._p_host, non_blocking=True)
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._launch_all(torch.cuda.current_stream())
+        self._f_host.copy_(self.f_all, non_blocking=True)
+        self._g_host.copy_(self.g_all, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        fh, gh = self._f_host.numpy(), self._g_host.numpy()
+        out_f, out_g = [], []
+        for i, m in enumerate(self.members):
+            f = fh[self._f_off[i]:self._f_off[i + 1]].reshape(len(m.nh), 2)
+            out_f.append(f[:, 0] + 1j * f[:, 1])
+            g = gh[self._g_off[i]:self._g_off[i + 1]].reshape(len(m.nh), -1)
+            out_g.append(g[:, :len(m.names)].copy())
         return out_f, out_g
 
     def launches_per_call(self):
