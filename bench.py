@@ -533,19 +533,25 @@ def run_workload(args, rank, local_rank):
                 for q in range(n):
                     noisy += G.DepolarizingChannel(0.01).on(q)
                     noisy += G.AmplitudeDampingChannel(0.02).on(q)
+        for q in range(n):
+            noisy += G.Measure(f'q{q}').on(q)
         names = circ.params_name
         prd = dict(zip(names, params_np[0].tolist()))
         sim_api = Simulator('mqvector_b200', n, dtype=complex64, seed=7)
-        units = 1
+        shots = 256
+        units = shots
+        seeds = iter(range(1, 1 << 30))
 
         def step():
-            return sim_api.get_expectation(ham, noisy, pr=prd)
+            return sim_api.sampling(noisy, pr=prd, shots=shots, seed=next(seeds))
 
         e2e_step = step
-        io = (params_np.nbytes, 16)
-        cfg = {"workload": f"noisy trajectories, HEA {n}q x {layers} layers with a depolarizing (p=0.01) and an "
+        io = (params_np.nbytes, shots * n * 8)
+        cfg = {"workload": f"noisy sampling, HEA {n}q x {layers} layers with a depolarizing (p=0.01) and an "
                            f"amplitude-damping (gamma=0.02) channel on every qubit after every layer "
-                           f"({2 * n * layers} channels), one trajectory + <H> per unit", "n_qubits": n, "batch": 1}
+                           f"({2 * n * layers} channels) and {n} measurements; {shots} shots per step, every "
+                           f"shot one trajectory on its own stream, run as one batch", "n_qubits": n,
+               "batch": shots}
     elif args.workload == 'pshift':
         n, layers = 16, 2
         circ, ham, params_np = build_workload(n, layers, 1, seed=rank)

@@ -216,6 +216,23 @@ MQB_API int mqb_expectation(const mqb_hamiltonian *ham, const void *bra, const v
 MQB_API int mqb_apply_matrix1(int n_qubits, int precision, void *states, int64_t batch, int qubit,
                               uint64_t ctrl_mask, const double *matrix, void *stream);
 
+/* One channel step of many noise trajectories, one launch per 256 requests.  Request i acts on
+ * state rows[i] of `states` ([batch][2^n]) with its own 2x2 matrix (matrices + 8 i: 8 doubles,
+ * row-major (re, im) pairs) on qubits[i] where every bit of ctrl_masks[i] is set.  rows, qubits,
+ * ctrl_masks and matrices are host arrays of `count` entries.
+ *   mqb_rows_apply_matrix1: every request in place; rows must be distinct.
+ *   mqb_rows_matrix1_norm:  out[i] (device float64) = || M_i psi_rows[i] ||^2, states unchanged:
+ *     the probability of a Kraus operator, and P(qubit = 1) with M = [[0, 0], [0, 1]].
+ * Batched forms of the per-trajectory sweeps of ApplyChannel (vector_state.tpp:465-709) and
+ * ApplyMeasure (vector_state.tpp:440-462): the operator ApplyPauliChannel / ApplyKraus /
+ * ApplyDampingChannel picks for each trajectory, and the norms its draws compare against. */
+MQB_API int mqb_rows_apply_matrix1(int n_qubits, int precision, void *states, int64_t batch, int64_t count,
+                                   const int64_t *rows, const int32_t *qubits, const uint64_t *ctrl_masks,
+                                   const double *matrices, void *stream);
+MQB_API int mqb_rows_matrix1_norm(int n_qubits, int precision, const void *states, int64_t batch, int64_t count,
+                                  const int64_t *rows, const int32_t *qubits, const uint64_t *ctrl_masks,
+                                  const double *matrices, double *out, void *stream);
+
 /* out[b] = <a_b|b_b> as (re, im) float64 on the device. */
 MQB_API int mqb_vdot(int n_qubits, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream);
 

@@ -95,6 +95,8 @@ SIGNATURES = {
     'mqb_expectation': [_P, _P, _P, _I64, _P, _P],
     'mqb_apply_matrix1': [_I, _I, _P, _I64, _I, ctypes.c_uint64, _P, _P],
     'mqb_vdot': [_I, _I, _P, _P, _I64, _P, _P],
+    'mqb_rows_apply_matrix1': [_I, _I, _P, _I64, _I64, _P, _P, _P, _P, _P],
+    'mqb_rows_matrix1_norm': [_I, _I, _P, _I64, _I64, _P, _P, _P, _P, _P, _P],
     'mqb_grad_workspace_size': [_P, _I64, _I, _I, _P],
     'mqb_expectation_with_grad': [_P, _P, _I, _P, _I, _I64, _P, _I64, _P, _P, _P, _I, _P, _SZ, _P],
     'mqb_sample_scratch_size': [_I, _P],

@@ -1160,6 +1160,71 @@ int mqb_apply_matrix1(int n, int precision, void *states, int64_t batch, int qub
     });
 }
 
+namespace {
+// Host checks and chunked launches shared by mqb_rows_apply_matrix1 / mqb_rows_matrix1_norm.
+void rows_matrix1(int n, int precision, void *states, int64_t batch, int64_t count, const int64_t *rows,
+                  const int32_t *qubits, const uint64_t *masks, const double *matrices, double *norm_out,
+                  cudaStream_t st) {
+    if (n < 1 || n > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
+    if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
+    if (count < 0) fail(MQB_ERR_INVALID, "count must be >= 0");
+    if (count == 0) return;
+    if (!states || !rows || !qubits || !masks || !matrices) fail(MQB_ERR_INVALID, "null argument");
+    require_aligned(states, "states");
+    for (int64_t i = 0; i < count; ++i) {
+        if (rows[i] < 0 || rows[i] >= batch) fail(MQB_ERR_INVALID, "request %lld: row %lld outside the batch",
+                                                  (long long)i, (long long)rows[i]);
+        if (qubits[i] < 0 || qubits[i] >= n) fail(MQB_ERR_INVALID, "request %lld: qubit %d outside the register",
+                                                  (long long)i, qubits[i]);
+        if (n < 64 && (masks[i] >> n)) fail(MQB_ERR_INVALID, "request %lld: control mask outside the register",
+                                            (long long)i);
+        if (masks[i] >> qubits[i] & 1) fail(MQB_ERR_INVALID, "request %lld: the target qubit cannot be a control",
+                                            (long long)i);
+    }
+    if (!norm_out) {   // in-place updates of one row from two requests would race
+        std::vector<int64_t> sorted(rows, rows + count);
+        std::sort(sorted.begin(), sorted.end());
+        if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+            fail(MQB_ERR_INVALID, "rows must be distinct");
+    }
+    const int sm = sm_count_cached();
+    TimeScope ts(TK_OTHER, st);
+    RowOps ops;
+    for (int64_t a = 0; a < count; a += kRowOpsMax) {
+        ops.count = int(std::min<int64_t>(kRowOpsMax, count - a));
+        for (int k = 0; k < ops.count; ++k) {
+            ops.row[k] = rows[a + k];
+            ops.qubit[k] = qubits[a + k];
+            ops.ctrl[k] = masks[a + k];
+            for (int v = 0; v < 8; ++v) ops.m[k][v] = matrices[8 * (a + k) + v];
+        }
+        double *o = norm_out ? norm_out + a : nullptr;
+        if (precision == MQB_PREC_C64)
+            ck(launch_row_ops<float>(static_cast<float2 *>(states), n, ops, o, sm, st), "row ops");
+        else
+            ck(launch_row_ops<double>(static_cast<double2 *>(states), n, ops, o, sm, st), "row ops");
+    }
+}
+}  // namespace
+
+int mqb_rows_apply_matrix1(int n, int precision, void *states, int64_t batch, int64_t count, const int64_t *rows,
+                           const int32_t *qubits, const uint64_t *ctrl_masks, const double *matrices, void *stream) {
+    return guarded([&] {
+        rows_matrix1(n, precision, states, batch, count, rows, qubits, ctrl_masks, matrices, nullptr,
+                     static_cast<cudaStream_t>(stream));
+    });
+}
+
+int mqb_rows_matrix1_norm(int n, int precision, const void *states, int64_t batch, int64_t count, const int64_t *rows,
+                          const int32_t *qubits, const uint64_t *ctrl_masks, const double *matrices, double *out,
+                          void *stream) {
+    return guarded([&] {
+        if (count > 0 && !out) fail(MQB_ERR_INVALID, "null argument");
+        rows_matrix1(n, precision, const_cast<void *>(states), batch, count, rows, qubits, ctrl_masks, matrices, out,
+                     static_cast<cudaStream_t>(stream));
+    });
+}
+
 int mqb_vdot(int n, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream) {
     return guarded([&] {
         if (!a || !b || !out) fail(MQB_ERR_INVALID, "null argument");

@@ -1046,6 +1046,73 @@ cudaError_t launch_matrix1(cplx<R> *st, int n, int qubit, uint64_t ctrl, int64_t
     return cudaGetLastError();
 }
 
+// Request blockIdx.y of `ops` over its pairs (amplitudes with bit q = 0 and 1), blocks in x
+// striding the pairs.  Amplitudes a matrix column does not use are not read (a projector reads
+// half the state), except where the controls are unset and the norm needs them as they are.
+template <typename R, bool NORM>
+__global__ void row_ops_kernel(cplx<R> *st, int n, const __grid_constant__ RowOps ops, double *norm_out) {
+    const int r = blockIdx.y;
+    const int q = ops.qubit[r];
+    const uint64_t ctrl = ops.ctrl[r];
+    const int64_t half = int64_t(1) << (n - 1);
+    cplx<R> *p = st + ops.row[r] * (int64_t(1) << n);
+    const double *mv = ops.m[r];
+    const R m0r = R(mv[0]), m0i = R(mv[1]), m1r = R(mv[2]), m1i = R(mv[3]);
+    const R m2r = R(mv[4]), m2i = R(mv[5]), m3r = R(mv[6]), m3i = R(mv[7]);
+    const bool use0 = mv[0] != 0 || mv[1] != 0 || mv[4] != 0 || mv[5] != 0;
+    const bool use1 = mv[2] != 0 || mv[3] != 0 || mv[6] != 0 || mv[7] != 0;
+    double acc = 0;
+    for (int64_t l = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; l < half; l += int64_t(gridDim.x) * blockDim.x) {
+        const uint64_t i = ins0_64(uint64_t(l), q), j = i | (uint64_t(1) << q);
+        if ((i & ctrl) != ctrl) {
+            if (NORM) {
+                const cplx<R> a = p[i], c = p[j];
+                acc += double(a.x) * a.x + double(a.y) * a.y + double(c.x) * c.x + double(c.y) * c.y;
+            }
+            continue;
+        }
+        const cplx<R> a = use0 ? p[i] : cplx<R>{0, 0};
+        const cplx<R> c = use1 ? p[j] : cplx<R>{0, 0};
+        const cplx<R> x{m0r * a.x - m0i * a.y + m1r * c.x - m1i * c.y, m0r * a.y + m0i * a.x + m1r * c.y + m1i * c.x};
+        const cplx<R> y{m2r * a.x - m2i * a.y + m3r * c.x - m3i * c.y, m2r * a.y + m2i * a.x + m3r * c.y + m3i * c.x};
+        if (NORM) {
+            acc += double(x.x) * x.x + double(x.y) * x.y + double(y.x) * y.x + double(y.y) * y.y;
+        } else {
+            p[i] = x;
+            p[j] = y;
+        }
+    }
+    if (NORM) {
+        __shared__ double red[32];
+        acc = warp_sum(acc);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+            v = warp_sum(v);
+            if (threadIdx.x == 0) atomicAdd(norm_out + r, v);
+        }
+    }
+}
+
+template <typename R>
+cudaError_t launch_row_ops(cplx<R> *st, int n, const RowOps &ops, double *norm_out, int sm_count, cudaStream_t s) {
+    if (ops.count <= 0) return cudaSuccess;
+    const int threads = 256;
+    const int64_t half = int64_t(1) << (n - 1);
+    const int64_t per_state = std::max<int64_t>(1, (half + threads - 1) / threads);
+    const int64_t want = std::max<int64_t>(1, (int64_t(sm_count) * 8 + ops.count - 1) / ops.count);
+    const dim3 grid(unsigned(std::min(per_state, want)), unsigned(ops.count));
+    if (norm_out) {
+        cudaError_t e = cudaMemsetAsync(norm_out, 0, sizeof(double) * ops.count, s);
+        if (e != cudaSuccess) return e;
+        row_ops_kernel<R, true><<<grid, threads, 0, s>>>(st, n, ops, norm_out);
+    } else {
+        row_ops_kernel<R, false><<<grid, threads, 0, s>>>(st, n, ops, nullptr);
+    }
+    return cudaGetLastError();
+}
+
 template <typename R>
 __global__ void copy_kernel(cplx<R> *dst, const cplx<R> *src, int n, int64_t batch, int64_t src_stride) {
     const int64_t dim = int64_t(1) << n;
@@ -1283,6 +1350,7 @@ cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale
     template cudaError_t launch_sample_search<R>(const cplx<R> *, int, int, const double *, const double *,       \
                                                  int64_t, int64_t *, cudaStream_t);                                \
     template cudaError_t launch_one_prob<R>(const cplx<R> *, int, int, double *, cudaStream_t);                    \
+    template cudaError_t launch_row_ops<R>(cplx<R> *, int, const RowOps &, double *, int, cudaStream_t);          \
     template cudaError_t launch_collapse<R>(cplx<R> *, int, int, int, double, cudaStream_t);
 
 MQB_INSTANTIATE(float)

@@ -135,6 +135,21 @@ struct Mat1 {
 template <typename R>
 cudaError_t launch_matrix1(cplx<R> *st, int n, int qubit, uint64_t ctrl, int64_t batch, const Mat1 &m, int sm_count,
                            cudaStream_t s);
+// One step of many noise trajectories in one launch: request i acts on state row[i] with its own
+// 2x2 matrix m[i] on qubit[i] where every bit of ctrl[i] is set.  Passed by value (about 21 KB of
+// kernel parameters, within the 32 KB that sm_70 and later accept).
+constexpr int kRowOpsMax = 256;
+struct RowOps {
+    int count;
+    int32_t qubit[kRowOpsMax];
+    uint64_t ctrl[kRowOpsMax];
+    int64_t row[kRowOpsMax];
+    double m[kRowOpsMax][8];
+};
+// norm_out == nullptr: apply every request in place (rows distinct); otherwise norm_out[i] =
+// || M_i psi_row[i] ||^2 and the states stay as they are.
+template <typename R>
+cudaError_t launch_row_ops(cplx<R> *st, int n, const RowOps &ops, double *norm_out, int sm_count, cudaStream_t s);
 template <typename R>
 cudaError_t launch_copy_or_zero(cplx<R> *dst, const cplx<R> *src, int n, int64_t batch, int64_t src_stride,
                                 cudaStream_t s);

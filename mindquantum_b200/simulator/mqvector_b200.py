@@ -184,31 +184,46 @@ class MQVectorB200(BackendBase):
         return torch.as_tensor(np.ascontiguousarray(blk).view(np.float64), device=self.device)
 
     def _apply_segment(self, states, circuit, pr, batch=1):
-        """Apply a measurement-free circuit in place to ``states`` ([batch][2^n])."""
+        """Apply a measurement-free circuit in place to ``states`` ([batch][2^n]); ``pr`` is one
+        ParameterResolver for every state, or ``(names, rows)`` with one row of values per state."""
         names = circuit.params_name
         prog = lowered(circuit, self.n_qubits, self.precision, names, None, self.fuse, jit=self.jit)
         if prog.n_gates == 0:
             return
-        params, params_np = self._params_tensor(prog, pr)
+        if isinstance(pr, tuple):
+            all_names, rows = pr
+            cols = [all_names.index(k) for k in prog.param_names]
+            params_np = np.ascontiguousarray(rows[:, cols] if cols else np.zeros((batch, 1)), dtype=np.float64)
+            params = torch.as_tensor(params_np, device=self.device)
+            stride = params_np.shape[1]
+        else:
+            params, params_np = self._params_tensor(prog, pr)
+            stride = 0
         custom = self._custom_tensor(prog, params_np)
+        if custom is not None and custom.shape[0] != batch:   # the custom block has one row per state
+            custom = custom.expand(batch, -1).contiguous()
         ws_bytes = ctypes.c_size_t()
         N.call('mqb_apply_workspace_size', prog.handle, batch, ctypes.byref(ws_bytes))
         ws = torch.empty(ws_bytes.value, dtype=torch.uint8, device=self.device)
-        N.call('mqb_apply', prog.handle, _ptr(states), batch, _ptr(params), 0, _ptr(custom), _ptr(ws),
+        N.call('mqb_apply', prog.handle, _ptr(states), batch, _ptr(params), stride, _ptr(custom), _ptr(ws),
                ws_bytes.value, _stream())
 
     def _measure(self, state, gate, rng):
-        """ApplyMeasure (vector_state.tpp:440-462): draw, collapse, optional reset."""
+        """ApplyMeasure (vector_state.tpp:440-462) on one state: draw, collapse, optional reset."""
+        return self._run_plans(state.view(1, -1), [self._measure_plan(gate, rng.draw)])[0]
+
+    @staticmethod
+    def _measure_plan(gate, draw):
+        """ApplyMeasure as a plan (see _run_plans): P(q = 1), a draw, the collapse (projector over
+        the square root of the outcome's probability), then X when a reset asks for it."""
         q = gate.obj_qubits[0]
-        out = torch.zeros(1, dtype=torch.float64, device=self.device)
-        N.call('mqb_qubit_one_probability', self.n_qubits, self.precision, _ptr(state), q, _ptr(out), _stream())
-        one_amp = float(out.item())
-        collapse_to_one = rng.draw() < one_amp
+        one_amp = yield ('p1', q)
+        collapse_to_one = draw() < one_amp
         prob = one_amp if collapse_to_one else 1.0 - one_amp
         scale = 1.0 / math.sqrt(prob) if prob > 0 else 0.0
-        N.call('mqb_collapse', self.n_qubits, self.precision, _ptr(state), q, int(collapse_to_one), scale, _stream())
+        yield ('apply', [[0, 0], [0, scale]] if collapse_to_one else [[scale, 0], [0, 0]], q, ())
         if gate.reset_to is not None and int(gate.reset_to) != int(collapse_to_one):
-            self._apply_segment(state, Circuit([G.X.on(q)]), ParameterResolver())
+            yield ('apply', [[0, 1], [1, 0]], q, ())
         return int(collapse_to_one)
 
     @staticmethod
@@ -238,40 +253,81 @@ class MQVectorB200(BackendBase):
     def _run(self, state, circuit, pr, rng):
         """Apply ``circuit`` in place; measurements and channels draw from ``rng``
         (VectorState::ApplyCircuit, vector_state.tpp:949-960)."""
+        return self._run_batch(state.view(1, -1), circuit, pr, [rng])[0]
+
+    def _run_batch(self, states, circuit, pr, rngs):
+        """Run len(rngs) trajectories of ``circuit`` at once on states [B][2^n], in place: the
+        unitary segments as one batched launch, every measurement and channel step with the
+        draws of each trajectory's own stream (the reference's order, trajectory by trajectory)
+        and the state-dependent probabilities of all trajectories in one reduction and one copy
+        to the host.  Returns the measurement results of every trajectory."""
+        B = states.shape[0]
+        results = [{} for _ in range(B)]
         if not circuit.has_measure_gate and not circuit.is_noise_circuit:
             if len(circuit):
-                self._apply_segment(state, circuit, pr)
-            return {}
-        results = {}
+                self._apply_segment(states, circuit, pr, B)
+            return results
         for part in self._split(circuit):
             if isinstance(part, G.Measure):
-                results[part.key] = self._measure(state, part, rng)
+                out = self._run_plans(states, [self._measure_plan(part, r.draw) for r in rngs])
+                for b in range(B):
+                    results[b][part.key] = out[b]
             elif isinstance(part, G.NoiseGate):
-                self._channel(state, part, rng)
+                self._run_plans(states, [self._channel_plan(part, r.draw) for r in rngs])
             else:
-                self._apply_segment(state, part, pr)
+                self._apply_segment(states, part, pr, B)
         return results
 
     # ------------------------------------------------------------------ noise channels
-    def _matrix_on(self, state, m, q, ctrls=()):
-        """A 2x2 matrix (unitary or not) on qubit q under ``ctrls``, in place (one device sweep)."""
-        mv = np.ascontiguousarray(np.asarray(m, dtype=np.complex128).reshape(4)).view(np.float64)
-        mask = 0
-        for c in ctrls:
-            mask |= 1 << int(c)
-        N.call('mqb_apply_matrix1', self.n_qubits, self.precision, _ptr(state), 1, int(q), mask,
-               mv.ctypes.data_as(ctypes.c_void_p), _stream())
+    _PAULI = ([[0, 1], [1, 0]], [[0, -1j], [1j, 0]], [[1, 0], [0, -1]])
+    _PROJ = {'p0': [[1, 0], [0, 0]], 'p1': [[0, 0], [0, 1]]}
 
-    _PAULI = (np.array([[0, 1], [1, 0]], dtype=complex), np.array([[0, -1j], [1j, 0]]),
-              np.array([[1, 0], [0, -1]], dtype=complex))
+    def _run_plans(self, states, plans):
+        """Drive one plan per trajectory (trajectory b on states[b]) until all are done, serving
+        their requests in rounds: every ``('apply', m, q, ctrls)`` of a round in one launch, every
+        ``('norm', m, q, ctrls)`` (||m psi||^2), ``('p0', q)`` and ``('p1', q)`` (the squared norm
+        of the part of psi with qubit q = 0 or 1, ZeroStateVdot / OneStateVdot) of a round in one
+        reduction with one copy to the host.  A plan is a generator: it yields a request, receives
+        the norm (None for an apply) and returns its result."""
+        results = [None] * len(plans)
+        pending = {}
 
-    def _pauli_on(self, state, which, q, ctrls=()):
-        self._matrix_on(state, self._PAULI[which], q, ctrls)
+        def advance(b, value):
+            try:
+                pending[b] = plans[b].send(value)
+            except StopIteration as stop:
+                results[b] = stop.value
 
-    def _one_probability(self, state, q):
-        out = torch.zeros(1, dtype=torch.float64, device=self.device)
-        N.call('mqb_qubit_one_probability', self.n_qubits, self.precision, _ptr(state), q, _ptr(out), _stream())
-        return float(out.item())
+        for b in range(len(plans)):
+            advance(b, None)
+        while pending:
+            round_, pending = pending, {}
+            applies = [(b, r) for b, r in round_.items() if r[0] == 'apply']
+            norms = [(b, ('norm', self._PROJ[r[0]], r[1], ())) if r[0] in self._PROJ else (b, r)
+                     for b, r in round_.items() if r[0] != 'apply']
+            if applies:
+                self._rows_matrix1('mqb_rows_apply_matrix1', states, applies)
+            values = self._rows_matrix1('mqb_rows_matrix1_norm', states, norms) if norms else {}
+            for b in round_:
+                advance(b, values.get(b))
+        return results
+
+    def _rows_matrix1(self, fn, states, reqs):
+        """One mqb_rows_* call for [(row, (kind, m, q, ctrls))]; the norms by row for the norm call."""
+        k = len(reqs)
+        rows = np.fromiter((b for b, _ in reqs), dtype=np.int64, count=k)
+        qubits = np.fromiter((int(r[2]) for _, r in reqs), dtype=np.int32, count=k)
+        masks = np.fromiter((sum(1 << int(c) for c in r[3]) for _, r in reqs), dtype=np.uint64, count=k)
+        mats = np.ascontiguousarray(np.array([r[1] for _, r in reqs], dtype=np.complex128).reshape(k, 4)).view(np.float64)
+        vp = ctypes.c_void_p
+        args = [self.n_qubits, self.precision, _ptr(states), states.shape[0], k, rows.ctypes.data_as(vp),
+                qubits.ctypes.data_as(vp), masks.ctypes.data_as(vp), mats.ctypes.data_as(vp)]
+        if fn == 'mqb_rows_apply_matrix1':
+            N.call(fn, *args, _stream())
+            return None
+        out = torch.empty(k, dtype=torch.float64, device=self.device)
+        N.call(fn, *args, _ptr(out), _stream())
+        return dict(zip(rows.tolist(), out.cpu().numpy().tolist()))
 
     @staticmethod
     def _pauli_index(cum, r):
@@ -281,17 +337,18 @@ class MQVectorB200(BackendBase):
         it = bisect.bisect_left(cum, r)
         return it - 1 if it > 0 else 0
 
-    def _channel(self, state, g, rng):
-        """One trajectory step of a channel (VectorState::ApplyChannel, vector_state.tpp:465-709).
-
-        The draws come from ``rng`` in the reference's order; probabilities that depend on the
-        state (damping, Kraus, thermal relaxation) are reduced on the device in FP64."""
-        objs, ctrls = list(g.obj_qubits), list(g.ctrl_qubits)
-        draw = rng.draw
+    def _channel_plan(self, g, draw):
+        """One trajectory step of a channel as a plan (see _run_plans), VectorState::ApplyChannel
+        (vector_state.tpp:465-709): the draws come from ``draw`` in the reference's order, the
+        probabilities that depend on the state (damping, Kraus, thermal relaxation) are reduced
+        on the device in FP64, and an operator followed by a renormalisation is one matrix (the
+        operator over the square root of its probability)."""
+        objs, ctrls = list(g.obj_qubits), tuple(g.ctrl_qubits)
+        pauli = self._PAULI
         if isinstance(g, G.PauliChannel):
             k = self._pauli_index(g.cumulative_probs(), draw())
             if k < 3:
-                self._pauli_on(state, k, objs[0], ctrls)
+                yield ('apply', pauli[k], objs[0], ctrls)
         elif isinstance(g, G.GroupedPauliChannel):
             picks = []
             for q, row in zip(objs, g.probs):
@@ -300,17 +357,17 @@ class MQVectorB200(BackendBase):
                 if k < 3:
                     picks.append((k, q))
             for k, q in picks:    # ApplyPauliString: no controls
-                self._pauli_on(state, k, q)
+                yield ('apply', pauli[k], q, ())
         elif isinstance(g, G.DepolarizingChannel):
             idx, p = 0, float(g.p)
             while idx < len(objs):
                 if draw() < p * 3.0 / 4.0:
                     p_i = draw()
-                    self._pauli_on(state, 0 if p_i < 1.0 / 3.0 else (1 if p_i < 2.0 / 3.0 else 2), objs[idx], ctrls)
+                    yield ('apply', pauli[0 if p_i < 1.0 / 3.0 else (1 if p_i < 2.0 / 3.0 else 2)], objs[idx], ctrls)
                     for q in objs[idx + 1:]:
                         p_i = draw()
                         if p_i < 0.75:
-                            self._pauli_on(state, 0 if p_i < 0.25 else (1 if p_i < 0.5 else 2), q, ctrls)
+                            yield ('apply', pauli[0 if p_i < 0.25 else (1 if p_i < 0.5 else 2)], q, ctrls)
                     break
                 if not 4 > 3 * p:
                     break
@@ -325,35 +382,29 @@ class MQVectorB200(BackendBase):
                     if draw() < rel:
                         if m[0, 0].imag >= 1e-6:   # identity with a phase
                             v = m[0, 0] / math.sqrt(prob)
-                            self._matrix_on(state, [[v, 0], [0, v]], 0)
+                            yield ('apply', [[v, 0], [0, v]], 0, ())
                         return
                 else:
-                    tmp = state.clone()
-                    self._matrix_on(tmp, m, objs[0], ctrls)
-                    out = torch.zeros(2, dtype=torch.float64, device=self.device)
-                    N.call('mqb_vdot', self.n_qubits, self.precision, _ptr(tmp), _ptr(tmp), 1, _ptr(out), _stream())
-                    prob = float(out[0].item())
+                    prob = yield ('norm', m, objs[0], ctrls)
                     rel = prob / total
                     total -= prob
                     if draw() < rel:
-                        v = 1 / math.sqrt(prob)
-                        self._matrix_on(tmp, [[v, 0], [0, v]], 0)
-                        state.copy_(tmp)
+                        yield ('apply', m / math.sqrt(prob), objs[0], ctrls)
                         return
         elif isinstance(g, (G.AmplitudeDampingChannel, G.PhaseDampingChannel)):
-            renorm = self._one_probability(state, objs[0])
+            renorm = yield ('p1', objs[0])
             if renorm < 1e-6:
                 return
             gamma = float(g.gamma)
             prob = gamma * renorm
             if draw() <= prob:
                 if isinstance(g, G.AmplitudeDampingChannel):
-                    self._matrix_on(state, [[0, 1 / math.sqrt(renorm)], [0, 0]], objs[0], ctrls)
+                    yield ('apply', [[0, 1 / math.sqrt(renorm)], [0, 0]], objs[0], ctrls)
                 else:
-                    self._matrix_on(state, [[0, 0], [0, 1 / math.sqrt(renorm)]], objs[0], ctrls)
+                    yield ('apply', [[0, 0], [0, 1 / math.sqrt(renorm)]], objs[0], ctrls)
             else:
                 a, b = 1 / math.sqrt(1 - prob), math.sqrt(1 - gamma) / math.sqrt(1 - prob)
-                self._matrix_on(state, [[a, 0], [0, b]], objs[0], ctrls)
+                yield ('apply', [[a, 0], [0, b]], objs[0], ctrls)
         elif isinstance(g, G.ThermalRelaxationChannel):
             t1, t2, tg = float(g.t1), float(g.t2), float(g.gate_time)
             e1, e2 = math.exp(-tg / t1), math.exp(-tg / t2)
@@ -365,29 +416,29 @@ class MQVectorB200(BackendBase):
                 if r < 1 - pz - p_reset:
                     return
                 if r < 1 - p_reset:
-                    self._pauli_on(state, 2, q, ctrls)
+                    yield ('apply', pauli[2], q, ctrls)
                 else:
-                    zero = 1.0 - self._one_probability(state, q)
+                    zero = yield ('p0', q)   # ZeroStateVdot: the state need not be normalised
                     if draw() < zero:
-                        self._matrix_on(state, [[1 / math.sqrt(zero), 0], [0, 0]], q, ctrls)
+                        yield ('apply', [[1 / math.sqrt(zero), 0], [0, 0]], q, ctrls)
                     else:
-                        self._matrix_on(state, [[0, 1 / math.sqrt(1 - zero)], [0, 0]], q, ctrls)
+                        yield ('apply', [[0, 1 / math.sqrt(1 - zero)], [0, 0]], q, ctrls)
             elif 2 * t1 > t2:
                 r = draw()
                 root = math.sqrt(p_reset * p_reset + 4 * e2 * e2)
                 ev0, ev1 = (2 - p_reset + root) / 2, (2 - p_reset - root) / 2
                 vec0, vec1 = (ev0 - e1) / e2, (ev1 - e1) / e2
-                zero = 1.0 - self._one_probability(state, q)
+                zero = yield ('p0', q)   # ZeroStateVdot: the state need not be normalised
                 one = 1 - zero
                 c0 = vec0 * vec0 * zero + one
                 p0 = c0 * ev0 / (vec0 * vec0 + 1)
                 if r < p0:
-                    self._matrix_on(state, [[vec0 / math.sqrt(c0), 0], [0, 1 / math.sqrt(c0)]], q, ctrls)
+                    yield ('apply', [[vec0 / math.sqrt(c0), 0], [0, 1 / math.sqrt(c0)]], q, ctrls)
                 elif r < 1 - p_reset * one:
                     c1 = vec1 * vec1 * zero + one
-                    self._matrix_on(state, [[vec1 / math.sqrt(c1), 0], [0, 1 / math.sqrt(c1)]], q, ctrls)
+                    yield ('apply', [[vec1 / math.sqrt(c1), 0], [0, 1 / math.sqrt(c1)]], q, ctrls)
                 else:
-                    self._matrix_on(state, [[0, 1 / math.sqrt(one)], [0, 0]], q, ctrls)
+                    yield ('apply', [[0, 1 / math.sqrt(one)], [0, 0]], q, ctrls)
         else:
             raise ValueError(f"{g.name} is not a noise channel.")
 
@@ -774,52 +825,82 @@ class MQVectorB200(BackendBase):
         o = out.cpu().numpy()
         return (o[..., 0] + 1j * o[..., 1]).T
 
+    def _trajectory_chunk(self, count):
+        """Trajectories run at once: at most 40 % of the free device memory, at most 4096."""
+        S = (1 << self.n_qubits) * (8 if self.precision == N.MQB_PREC_C64 else 16)
+        free, _ = torch.cuda.mem_get_info(self.device)
+        return int(max(1, min(count, 4096, (0.4 * free) // S)))
+
     def _noisy_shift(self, plan, P, hams, n_thread):
         """Parameter shift over stochastic channels, one trajectory per evaluation, in the
         reference's order of random draws (vector_state.tpp:1033-1230): every evaluation runs on a
         copy of the state re-seeded with int(draw * 10000) from this simulator's stream, every
         Hamiltonian copy consumes one more draw, Hamiltonians go in groups of ``n_thread`` and the
-        Hamiltonian loop sits inside the gate loop."""
+        Hamiltonian loop sits inside the gate loop.
+
+        The draws of this simulator's stream are taken first, in that order, which fixes every
+        trajectory's seed; the trajectories then run as batches (those measured with the same
+        Hamiltonian together) and f and g are summed in the reference's order."""
         rows = plan.rows(P)
         R, E = plan.rows_per_sample, plan.n_shifts
         nhs = [native_ham(h, self.n_qubits, self.precision) for h in hams]
         n_prs, n_h = P.shape[0], len(hams)
-        f = np.zeros((n_prs, n_h), dtype=np.complex128)
-        g = np.zeros((n_prs, n_h, plan.J.shape[1]), dtype=np.complex128)
-        out = torch.zeros(2, dtype=torch.float64, device=self.device)
         by_gate = {}
         for e, gi in enumerate(plan.gate_of):
             by_gate.setdefault(gi, []).append(e)
+        job_row, job_seed, job_ham = [], [], []
 
-        def trajectory(row):
-            st = self.state.clone()
-            pr = ParameterResolver(dict(zip(plan.slot_names, (float(v) for v in row))))
-            self._run(st, plan.circuit, pr, Mt19937Uniform(int(self._rng.draw() * 10000)))
-            return st
+        def job(row, ham):
+            job_row.append(row)
+            job_seed.append(int(self._rng.draw() * 10000))
+            job_ham.append(ham)
+            return len(job_row) - 1
 
-        def expect(st, j):
-            N.call('mqb_expectation', nhs[j].handle, _ptr(st), _ptr(st), 1, _ptr(out), _stream())
-            o = out.cpu().numpy()
-            return complex(o[0], o[1])
-
+        terms = []   # (s, j, base job) and (s, j, e, minus job, plus job), the reference's order
         for s in range(n_prs):
-            base = trajectory(rows[s * R])
+            base = job(s * R, -1)
             for start in range(0, n_h, n_thread):
                 group = range(start, min(start + n_thread, n_h))
                 self._rng.draw()
                 for j in group:
                     self._rng.draw()
-                    f[s, j] = expect(base, j)
+                    terms.append((s, j, base))
                 for gi in sorted(by_gate):
                     for j in group:
                         for e in by_gate[gi]:
-                            st = trajectory(rows[s * R + 1 + e])
+                            km = job(s * R + 1 + e, j)
                             self._rng.draw()
-                            f_minus = expect(st, j)
-                            st = trajectory(rows[s * R + 1 + E + e])
+                            kp = job(s * R + 1 + E + e, j)
                             self._rng.draw()
-                            f_plus = expect(st, j)
-                            g[s, j] += plan.coeff[e] * (f_plus - f_minus).real * plan.J[e]
+                            terms.append((s, j, e, km, kp))
+        values = {}
+        for ham in range(-1, n_h):
+            ids = [k for k, h in enumerate(job_ham) if h == ham]
+            chunk = self._trajectory_chunk(max(1, len(ids)))
+            for a in range(0, len(ids), chunk):
+                part = ids[a:a + chunk]
+                states = self.state.reshape(1, -1).repeat(len(part), 1)
+                self._run_batch(states, plan.circuit, (list(plan.slot_names), rows[[job_row[k] for k in part]]),
+                                [Mt19937Uniform(job_seed[k]) for k in part])
+                targets = range(n_h) if ham < 0 else (ham,)
+                res = torch.zeros((len(targets), len(part), 2), dtype=torch.float64, device=self.device)
+                for t, j in enumerate(targets):
+                    N.call('mqb_expectation', nhs[j].handle, _ptr(states), _ptr(states), len(part), _ptr(res[t]),
+                           _stream())
+                res = res.cpu().numpy()
+                for t, j in enumerate(targets):
+                    for i, k in enumerate(part):
+                        values[k, j] = complex(res[t, i, 0], res[t, i, 1])
+                del states
+        f = np.zeros((n_prs, n_h), dtype=np.complex128)
+        g = np.zeros((n_prs, n_h, plan.J.shape[1]), dtype=np.complex128)
+        for t in terms:
+            if len(t) == 3:
+                s, j, base = t
+                f[s, j] = values[base, j]
+            else:
+                s, j, e, km, kp = t
+                g[s, j] += plan.coeff[e] * (values[kp, j] - values[km, j]).real * plan.J[e]
         return f, g
 
     def _parameter_shift_grad_ops(self, hams, circ, parallel_worker):
@@ -902,11 +983,17 @@ class MQVectorB200(BackendBase):
             for g in m_gates:
                 samples[:, key_map[g.key]] = (r >> g.obj_qubits[0]) & 1
         else:
-            for s in range(shots):
-                sub = Mt19937Uniform(int(rng.draw(low=1.0, high=float(1 << 20))))
-                st = self.state.clone()
-                out = self._run(st, circuit, pr, sub)
-                for k, v in out.items():
-                    samples[s, key_map[k]] = v
+            # every shot is a trajectory on its own stream, seeded from ``rng`` in shot order; the
+            # shots run as batches of trajectories
+            seeds = [int(rng.draw(low=1.0, high=float(1 << 20))) for _ in range(shots)]
+            chunk = self._trajectory_chunk(shots)
+            for a in range(0, shots, chunk):
+                part = seeds[a:a + chunk]
+                states = self.state.reshape(1, -1).repeat(len(part), 1)
+                outs = self._run_batch(states, circuit, pr, [Mt19937Uniform(x) for x in part])
+                for i, out in enumerate(outs):
+                    for k, v in out.items():
+                        samples[a + i, key_map[k]] = v
+                del states
         res.collect_data(samples)
         return res

@@ -936,7 +936,8 @@ def apply_measure(qs, n, q, rng):
 
 
 def sampling_general(n, circ, prd, shots, seed, dtype=np.complex128, init_state=None):
-    """VectorState::Sampling (vector_state.tpp:1308-1323): re-simulate the circuit once per shot.
+    """VectorState::Sampling (vector_state.tpp:1308-1323): re-simulate the circuit once per shot;
+    the shot's measurements and noise channels draw from one stream seeded from ``seed``'s.
 
     Returns (keys in circuit order, samples[shots][n_keys]).
     """
@@ -945,10 +946,13 @@ def sampling_general(n, circ, prd, shots, seed, dtype=np.complex128, init_state=
     out = np.zeros((shots, len(keys)), dtype=np.int64)
     for s in range(shots):
         sub = _Mt19937(int(_uniform(rng, 1.0, float(1 << 20))))
+        draw = lambda: _uniform(sub, 0.0, 1.0)   # noqa: E731  pylint: disable=cell-var-from-loop
         qs = zero_state(n, dtype) if init_state is None else np.array(init_state, dtype=dtype)
         for g in circ:
             if g.name == 'M':
-                out[s, keys.index(g.key)] = apply_measure(qs, n, g.obj_qubits[0], lambda: _uniform(sub, 0.0, 1.0))
+                out[s, keys.index(g.key)] = apply_measure(qs, n, g.obj_qubits[0], draw)
+            elif is_channel(g):
+                apply_channel(qs, n, g, draw)
             else:
                 apply_gate(qs, n, g, prd or {})
     return keys, out

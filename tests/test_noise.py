@@ -124,6 +124,38 @@ def test_matrix_abi_rejects_invalid_arguments(case):
                m.ctypes.data_as(ctypes.c_void_p), None)
 
 
+@pytest.mark.parametrize("case", ['duplicate_rows', 'row', 'qubit', 'ctrl_on_target', 'ctrl_outside', 'null'])
+def test_row_matrix_abi_rejects_invalid_arguments(case):
+    """mqb_rows_apply_matrix1 / mqb_rows_matrix1_norm check every request on the host."""
+    import ctypes
+    from mindquantum_b200 import _native as N
+
+    rows = np.array([0, 2], dtype=np.int64)
+    qubits = np.array([1, 0], dtype=np.int32)
+    masks = np.zeros(2, dtype=np.uint64)
+    mats = np.tile(np.eye(2, dtype=np.complex128).reshape(4), 2).view(np.float64)
+    fn = 'mqb_rows_apply_matrix1'
+    if case == 'duplicate_rows':
+        rows[1] = 0
+    elif case == 'row':
+        rows[1] = 3
+    elif case == 'qubit':
+        qubits[0] = 3
+    elif case == 'ctrl_on_target':
+        masks[0] = 1 << 1
+    elif case == 'ctrl_outside':
+        masks[1] = 1 << 4
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)   # noqa: E731
+    args = [3, N.MQB_PREC_C128, ctypes.c_void_p(16), 3, 2, vp(rows), vp(qubits), vp(masks), vp(mats)]
+    if case == 'null':
+        args[5] = None
+    with pytest.raises(RuntimeError):
+        N.call(fn, *args, None)
+    if case not in ('duplicate_rows',):   # the norm only reads: one row may be asked twice
+        with pytest.raises(RuntimeError):
+            N.call('mqb_rows_matrix1_norm', *args, ctypes.c_void_p(64), None)
+
+
 def test_state_pointers_must_be_16_byte_aligned():
     """Misaligned state buffers are refused on the host, before any device work."""
     import ctypes
@@ -142,6 +174,66 @@ def noisy_circuit():
                  G.GroupedPauliChannel(np.array([[0.2, 0.1, 0.1], [0.0, 0.3, 0.2]])).on([1, 2]), G.H.on(1),
                  G.Rzz('c').on([0, 1])])
     return c
+
+
+def _serve_plan(plan, qs, n):
+    """Serve a channel or measurement plan's requests with numpy (the device reductions and
+    applies of the batched driver, restated) and return the plan's result."""
+    idx = np.arange(1 << n)
+
+    def on(m, q, ctrls):
+        m = np.asarray(m, dtype=complex)
+        out = qs.copy()
+        mask = sum(1 << int(c) for c in ctrls)
+        i0 = idx[(((idx >> q) & 1) == 0) & ((idx & mask) == mask)]
+        i1 = i0 | (1 << q)
+        out[i0] = m[0, 0] * qs[i0] + m[0, 1] * qs[i1]
+        out[i1] = m[1, 0] * qs[i0] + m[1, 1] * qs[i1]
+        return out
+
+    val = None
+    try:
+        while True:
+            req = plan.send(val)
+            if req[0] == 'apply':
+                qs[:] = on(*req[1:])
+                val = None
+            elif req[0] in ('p0', 'p1'):
+                val = float(np.sum(np.abs(qs[((idx >> req[1]) & 1) == int(req[0] == 'p1')]) ** 2))
+            else:
+                t = on(*req[1:])
+                val = float(np.vdot(t, t).real)
+    except StopIteration as stop:
+        return stop.value
+
+
+def test_channel_plans_follow_the_oracle_draw_for_draw():
+    """The trajectory logic the batched driver runs (one plan per channel or measurement, its
+    requests served here by numpy) equals the oracle's shots one by one: 200 shots of a circuit
+    with every channel kind and measurements in the middle.  A controlled damping channel leaves
+    the state unnormalised (the reference renormalises by the uncontrolled population), so the
+    thermal-relaxation channel after it must take P(q = 0) as the reference does, not 1 - P(q = 1)."""
+    from mindquantum_b200.simulator.mqvector_b200 import MQVectorB200 as M
+
+    circ = _measured_noisy_circuit()
+    pr = {'a': 0.7, 'b': -1.3, 'c': 2.1}
+    n, shots = 3, 200
+    keys, ref = O.sampling_general(n, circ, pr, shots, 29)
+    rng = O._Mt19937(29)   # pylint: disable=protected-access
+    host = M.__new__(M)
+    for s in range(shots):
+        sub = O._Mt19937(int(O._uniform(rng, 1.0, float(1 << 20))))   # pylint: disable=protected-access
+        draw = lambda: O._uniform(sub, 0.0, 1.0)   # noqa: E731  pylint: disable=cell-var-from-loop
+        qs = O.zero_state(n, np.complex128)
+        out = {}
+        for g in circ:
+            if isinstance(g, G.Measure):
+                out[g.key] = _serve_plan(M._measure_plan(g, draw), qs, n)   # pylint: disable=protected-access
+            elif isinstance(g, G.NoiseGate):
+                _serve_plan(host._channel_plan(g, draw), qs, n)   # pylint: disable=protected-access
+            else:
+                O.apply_gate(qs, n, g, pr)
+        assert [out[k] for k in keys] == list(ref[s]), s
 
 
 # ------------------------------------------------------------------------------------------- GPU
@@ -194,3 +286,113 @@ def test_noisy_parameter_shift_matches_the_oracle_loop(dtype):
     assert np.allclose(g, ref[:, :, 1:], atol=tol * (1 if dtype == complex128 else 10), rtol=0)
     with pytest.raises(ValueError, match="noise circuit"):
         sim.get_expectation_with_grad(hams, circ, Circuit([G.H.on(0)]))
+
+
+def _row_requests(rng, n, batch, count):
+    rows = rng.choice(batch, size=count, replace=False)
+    qubits = rng.integers(0, n, size=count)
+    masks = []
+    for q in qubits:
+        others = [c for c in range(n) if c != q]
+        picked = rng.choice(others, size=int(rng.integers(0, 3)), replace=False)
+        masks.append(sum(1 << int(c) for c in picked))
+    mats = rng.normal(size=(count, 2, 2)) + 1j * rng.normal(size=(count, 2, 2))
+    return rows, qubits, masks, mats
+
+
+def _numpy_matrix1(psi, n, m, q, mask):
+    out = psi.copy()
+    idx = np.arange(1 << n)
+    sel = ((idx >> q) & 1 == 0) & ((idx & mask) == mask)
+    i0 = idx[sel]
+    i1 = i0 | (1 << q)
+    a, c = psi[i0], psi[i1]
+    out[i0] = m[0, 0] * a + m[0, 1] * c
+    out[i1] = m[1, 0] * a + m[1, 1] * c
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,batch,count", [(6, 9, 7), (17, 3, 3), (4, 600, 300)])
+@pytest.mark.parametrize("dtype", [complex128, complex64])
+def test_row_matrix_ops_against_numpy(n, batch, count, dtype):
+    """Per-row 2x2 operators (one launch per 256 requests) and their norms against numpy."""
+    import ctypes
+    import torch
+    from mindquantum_b200 import _native as N
+
+    rng = np.random.default_rng(n * 1000 + count)
+    psi = rng.normal(size=(batch, 1 << n)) + 1j * rng.normal(size=(batch, 1 << n))
+    rows, qubits, masks, mats = _row_requests(rng, n, batch, count)
+    prec = N.MQB_PREC_C128 if dtype == complex128 else N.MQB_PREC_C64
+    tdt = torch.complex128 if dtype == complex128 else torch.complex64
+    st = torch.as_tensor(psi, dtype=tdt, device='cuda').contiguous()
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)   # noqa: E731
+    r64 = np.ascontiguousarray(rows, dtype=np.int64)
+    q32 = np.ascontiguousarray(qubits, dtype=np.int32)
+    m64 = np.ascontiguousarray(masks, dtype=np.uint64)
+    mv = np.ascontiguousarray(mats.reshape(count, 4)).view(np.float64)
+    args = [n, prec, ctypes.c_void_p(st.data_ptr()), batch, count, vp(r64), vp(q32), vp(m64), vp(mv)]
+    out = torch.empty(count, dtype=torch.float64, device='cuda')
+    N.call('mqb_rows_matrix1_norm', *args, ctypes.c_void_p(out.data_ptr()), None)
+    N.call('mqb_rows_apply_matrix1', *args, None)
+    got_norm = out.cpu().numpy()
+    got = st.cpu().numpy()
+    ref = psi.copy()
+    tol = 1e-10 if dtype == complex128 else 2e-4
+    for i in range(count):
+        ref[rows[i]] = _numpy_matrix1(psi[rows[i]], n, mats[i], qubits[i], masks[i])
+        expect = float(np.sum(np.abs(ref[rows[i]]) ** 2))
+        assert abs(got_norm[i] - expect) <= tol * expect, i
+    assert np.max(np.abs(got - ref)) <= tol * max(1.0, np.max(np.abs(ref)))
+
+
+def _measured_noisy_circuit():
+    c = noisy_circuit()
+    c += G.Measure('m0').on(0)
+    c += G.AmplitudeDampingChannel(0.2).on(0)
+    c += G.Measure('m1').on(1)
+    c += G.Measure('m2').on(2)
+    return c
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [complex128, complex64])
+def test_noisy_sampling_matches_the_oracle_shot_by_shot(dtype):
+    """Every shot of a noisy circuit with measurements in the middle is one trajectory; the shots
+    run as one batch, each on its own stream, and equal the oracle's shots one by one."""
+    circ = _measured_noisy_circuit()
+    pr = {'a': 0.7, 'b': -1.3, 'c': 2.1}
+    sim = Simulator('mqvector_b200', 3, dtype=dtype, seed=3)
+    res = sim.sampling(circ, pr, shots=80, seed=29)
+    keys, ref = O.sampling_general(3, circ, pr, 80, 29)
+    got = np.array(res.samples)
+    cols = [res.keys_map[k] for k in keys]
+    assert np.array_equal(got[:, cols], ref)
+
+
+@pytest.mark.gpu
+def test_batched_trajectories_equal_one_at_a_time(monkeypatch):
+    """12 qubits, 200 shots of a layered circuit with a channel on every qubit: the batched run
+    (all shots at once) and the run one trajectory at a time give the same outcomes."""
+    from mindquantum_b200.simulator.mqvector_b200 import MQVectorB200
+
+    n = 12
+    c = Circuit()
+    for layer in range(2):
+        for q in range(n):
+            c += G.RY(f'y{layer}_{q}').on(q)
+        for q in range(n - 1):
+            c += G.X.on(q + 1, q)
+        for q in range(n):
+            c += G.DepolarizingChannel(0.05).on(q)
+            c += G.AmplitudeDampingChannel(0.1).on(q)
+        c += G.Measure(f'mid{layer}').on(layer)
+    for q in range(n):
+        c += G.Measure(f'q{q}').on(q)
+    rng = np.random.default_rng(4)
+    pr = {k: float(v) for k, v in zip(c.params_name, rng.uniform(-2, 2, len(c.params_name)))}
+    a = Simulator('mqvector_b200', n, dtype=complex64, seed=1).sampling(c, pr, shots=200, seed=5)
+    monkeypatch.setattr(MQVectorB200, '_trajectory_chunk', lambda self, count: 1)
+    b = Simulator('mqvector_b200', n, dtype=complex64, seed=1).sampling(c, pr, shots=200, seed=5)
+    assert np.array_equal(np.array(a.samples), np.array(b.samples))
