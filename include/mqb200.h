@@ -121,7 +121,8 @@ MQB_API int mqb_version(void);
 MQB_API int mqb_device_sm_count(int *out);
 /* Per-launch timing of the engine's kernels (CUDA events on the launching stream).  Kinds:
  * 0 fused forward pass, 1 fused backward pass, 2 Hamiltonian pass, 3 matrix generation,
- * 4 per-gate apply, 5 per-gate gradient, 6 gradient scatter, 7 copies.  mqb_timing_end
+ * 4 per-gate apply, 5 per-gate gradient, 6 gradient scatter, 7 copies and single-state sweeps,
+ * 8 row-wise trajectory steps (mqb_rows_*).  mqb_timing_end
  * synchronizes, writes total milliseconds and launch counts per kind and stops timing. */
 MQB_API int mqb_timing_begin(void);
 MQB_API int mqb_timing_end(double *ms, int64_t *launches, int n_kinds);

@@ -151,7 +151,7 @@ def call(name, *args):
 
 
 TIMING_KINDS = ('fused_forward', 'fused_backward', 'hamiltonian', 'matgen', 'gate_apply', 'gate_grad', 'grad_scatter',
-                'copy')
+                'copy', 'channel_rows')
 
 
 class KernelTimer:

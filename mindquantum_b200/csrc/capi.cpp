@@ -105,7 +105,7 @@ bool is_diag_gid(int gid) { return gid == GID_RZ || gid == GID_PS || gid == GID_
 
 // Optional per-launch timing: CUDA events around every kernel launch of the engine, recorded on the
 // launching stream while enabled; mqb_timing_end synchronizes and reports the time per launch kind.
-enum TimedKind { TK_FWD = 0, TK_BWD, TK_HAM, TK_MATGEN, TK_PLAIN_APPLY, TK_PLAIN_GRAD, TK_SCATTER, TK_OTHER, TK_COUNT };
+enum TimedKind { TK_FWD = 0, TK_BWD, TK_HAM, TK_MATGEN, TK_PLAIN_APPLY, TK_PLAIN_GRAD, TK_SCATTER, TK_OTHER, TK_ROWS, TK_COUNT };
 struct TimedLaunch {
     int kind;
     cudaEvent_t a, b;
@@ -1188,7 +1188,7 @@ void rows_matrix1(int n, int precision, void *states, int64_t batch, int64_t cou
             fail(MQB_ERR_INVALID, "rows must be distinct");
     }
     const int sm = sm_count_cached();
-    TimeScope ts(TK_OTHER, st);
+    TimeScope ts(TK_ROWS, st);
     RowOps ops;
     for (int64_t a = 0; a < count; a += kRowOpsMax) {
         ops.count = int(std::min<int64_t>(kRowOpsMax, count - a));

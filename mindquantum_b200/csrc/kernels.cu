@@ -1047,10 +1047,12 @@ cudaError_t launch_matrix1(cplx<R> *st, int n, int qubit, uint64_t ctrl, int64_t
 }
 
 // Request blockIdx.y of `ops` over its pairs (amplitudes with bit q = 0 and 1), blocks in x
-// striding the pairs.  Amplitudes a matrix column does not use are not read (a projector reads
-// half the state), except where the controls are unset and the norm needs them as they are.
+// striding the pairs, four pairs per thread in flight (all loads before the first store).
+// Amplitudes a matrix column does not use are not read (a projector reads half the state), except
+// where the controls are unset and the norm needs them as they are.
 template <typename R, bool NORM>
 __global__ void row_ops_kernel(cplx<R> *st, int n, const __grid_constant__ RowOps ops, double *norm_out) {
+    constexpr int U = 4;
     const int r = blockIdx.y;
     const int q = ops.qubit[r];
     const uint64_t ctrl = ops.ctrl[r];
@@ -1061,25 +1063,41 @@ __global__ void row_ops_kernel(cplx<R> *st, int n, const __grid_constant__ RowOp
     const R m2r = R(mv[4]), m2i = R(mv[5]), m3r = R(mv[6]), m3i = R(mv[7]);
     const bool use0 = mv[0] != 0 || mv[1] != 0 || mv[4] != 0 || mv[5] != 0;
     const bool use1 = mv[2] != 0 || mv[3] != 0 || mv[6] != 0 || mv[7] != 0;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     double acc = 0;
-    for (int64_t l = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; l < half; l += int64_t(gridDim.x) * blockDim.x) {
-        const uint64_t i = ins0_64(uint64_t(l), q), j = i | (uint64_t(1) << q);
-        if ((i & ctrl) != ctrl) {
-            if (NORM) {
-                const cplx<R> a = p[i], c = p[j];
-                acc += double(a.x) * a.x + double(a.y) * a.y + double(c.x) * c.x + double(c.y) * c.y;
-            }
-            continue;
+    for (int64_t l0 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; l0 < half; l0 += stride * U) {
+        uint64_t i[U];
+        bool in[U], on[U];
+        cplx<R> a[U], c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t l = l0 + u * stride;
+            in[u] = l < half;
+            i[u] = in[u] ? ins0_64(uint64_t(l), q) : 0;
+            on[u] = in[u] && (i[u] & ctrl) == ctrl;
+            const bool raw = NORM && in[u] && !on[u];   // outside the controls the norm takes psi as it is
+            a[u] = (on[u] && use0) || raw ? p[i[u]] : cplx<R>{0, 0};
+            c[u] = (on[u] && use1) || raw ? p[i[u] | (uint64_t(1) << q)] : cplx<R>{0, 0};
         }
-        const cplx<R> a = use0 ? p[i] : cplx<R>{0, 0};
-        const cplx<R> c = use1 ? p[j] : cplx<R>{0, 0};
-        const cplx<R> x{m0r * a.x - m0i * a.y + m1r * c.x - m1i * c.y, m0r * a.y + m0i * a.x + m1r * c.y + m1i * c.x};
-        const cplx<R> y{m2r * a.x - m2i * a.y + m3r * c.x - m3i * c.y, m2r * a.y + m2i * a.x + m3r * c.y + m3i * c.x};
-        if (NORM) {
-            acc += double(x.x) * x.x + double(x.y) * x.y + double(y.x) * y.x + double(y.y) * y.y;
-        } else {
-            p[i] = x;
-            p[j] = y;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!in[u]) continue;
+            if (!on[u]) {
+                if (NORM)
+                    acc += double(a[u].x) * a[u].x + double(a[u].y) * a[u].y + double(c[u].x) * c[u].x +
+                           double(c[u].y) * c[u].y;
+                continue;
+            }
+            const cplx<R> x{m0r * a[u].x - m0i * a[u].y + m1r * c[u].x - m1i * c[u].y,
+                            m0r * a[u].y + m0i * a[u].x + m1r * c[u].y + m1i * c[u].x};
+            const cplx<R> y{m2r * a[u].x - m2i * a[u].y + m3r * c[u].x - m3i * c[u].y,
+                            m2r * a[u].y + m2i * a[u].x + m3r * c[u].y + m3i * c[u].x};
+            if (NORM) {
+                acc += double(x.x) * x.x + double(x.y) * x.y + double(y.x) * y.x + double(y.y) * y.y;
+            } else {
+                p[i[u]] = x;
+                p[i[u] | (uint64_t(1) << q)] = y;
+            }
         }
     }
     if (NORM) {
@@ -1100,7 +1118,7 @@ cudaError_t launch_row_ops(cplx<R> *st, int n, const RowOps &ops, double *norm_o
     if (ops.count <= 0) return cudaSuccess;
     const int threads = 256;
     const int64_t half = int64_t(1) << (n - 1);
-    const int64_t per_state = std::max<int64_t>(1, (half + threads - 1) / threads);
+    const int64_t per_state = std::max<int64_t>(1, (half + 4 * threads - 1) / (4 * threads));
     const int64_t want = std::max<int64_t>(1, (int64_t(sm_count) * 8 + ops.count - 1) / ops.count);
     const dim3 grid(unsigned(std::min(per_state, want)), unsigned(ops.count));
     if (norm_out) {

@@ -24,7 +24,7 @@ from .backend_base import BackendBase
 from .lowering import lowered, native_ham
 from .measure_result import MeasureResult
 from .parameter_shift import ShiftPlan
-from .rng import Mt19937Uniform
+from .rng import Mt19937Uniform, UniformBlocks, UniformStreams
 from .utils import GradOpsWrapper, _thread_balance
 
 
@@ -210,21 +210,26 @@ class MQVectorB200(BackendBase):
 
     def _measure(self, state, gate, rng):
         """ApplyMeasure (vector_state.tpp:440-462) on one state: draw, collapse, optional reset."""
-        return self._run_plans(state.view(1, -1), [self._measure_plan(gate, rng.draw)])[0]
+        return int(self._measure_rows(state.view(1, -1), gate, UniformStreams([rng]))[0])
 
-    @staticmethod
-    def _measure_plan(gate, draw):
-        """ApplyMeasure as a plan (see _run_plans): P(q = 1), a draw, the collapse (projector over
-        the square root of the outcome's probability), then X when a reset asks for it."""
+    def _measure_rows(self, states, gate, streams):
+        """ApplyMeasure on every trajectory of ``states`` at once: P(q = 1) of all of them in one
+        reduction, one draw each from its own stream, the collapse (the projector over the square
+        root of the outcome's probability) in one launch, then X where a reset asks for it."""
         q = gate.obj_qubits[0]
-        one_amp = yield ('p1', q)
-        collapse_to_one = draw() < one_amp
-        prob = one_amp if collapse_to_one else 1.0 - one_amp
-        scale = 1.0 / math.sqrt(prob) if prob > 0 else 0.0
-        yield ('apply', [[0, 0], [0, scale]] if collapse_to_one else [[scale, 0], [0, 0]], q, ())
-        if gate.reset_to is not None and int(gate.reset_to) != int(collapse_to_one):
-            yield ('apply', [[0, 1], [1, 0]], q, ())
-        return int(collapse_to_one)
+        rows = np.arange(states.shape[0])
+        one = self._rows_norm(states, rows, self._P1, q)
+        to_one = streams.take(rows) < one
+        prob = np.where(to_one, one, 1.0 - one)
+        with np.errstate(divide='ignore'):
+            scale = np.where(prob > 0, 1.0 / np.sqrt(np.where(prob > 0, prob, 1.0)), 0.0)
+        mats = np.zeros((len(rows), 2, 2), dtype=np.complex128)
+        mats[to_one, 1, 1] = scale[to_one]
+        mats[~to_one, 0, 0] = scale[~to_one]
+        self._rows_apply(states, rows, mats, q)
+        if gate.reset_to is not None:
+            self._rows_apply(states, rows[to_one.astype(int) != int(gate.reset_to)], self._PAULI[0], q)
+        return to_one.astype(np.int64)
 
     @staticmethod
     def _split(circuit):
@@ -253,158 +258,149 @@ class MQVectorB200(BackendBase):
     def _run(self, state, circuit, pr, rng):
         """Apply ``circuit`` in place; measurements and channels draw from ``rng``
         (VectorState::ApplyCircuit, vector_state.tpp:949-960)."""
-        return self._run_batch(state.view(1, -1), circuit, pr, [rng])[0]
+        res = self._run_batch(state.view(1, -1), circuit, pr, UniformStreams([rng]))
+        return {k: int(v[0]) for k, v in res.items()}
 
-    def _run_batch(self, states, circuit, pr, rngs):
-        """Run len(rngs) trajectories of ``circuit`` at once on states [B][2^n], in place: the
-        unitary segments as one batched launch, every measurement and channel step with the
-        draws of each trajectory's own stream (the reference's order, trajectory by trajectory)
-        and the state-dependent probabilities of all trajectories in one reduction and one copy
-        to the host.  Returns the measurement results of every trajectory."""
+    def _run_batch(self, states, circuit, pr, streams):
+        """Run one trajectory of ``circuit`` per row of ``states`` ([B][2^n]) in place, trajectory b
+        drawing from stream b of ``streams``: the unitary segments as one batched launch, every
+        measurement and channel with each trajectory's draws in the reference's order and the
+        state-dependent probabilities of all trajectories in one reduction and one copy to the
+        host.  Returns {measurement key: outcomes [B]}."""
         B = states.shape[0]
-        results = [{} for _ in range(B)]
+        results = {}
         if not circuit.has_measure_gate and not circuit.is_noise_circuit:
             if len(circuit):
                 self._apply_segment(states, circuit, pr, B)
             return results
         for part in self._split(circuit):
             if isinstance(part, G.Measure):
-                out = self._run_plans(states, [self._measure_plan(part, r.draw) for r in rngs])
-                for b in range(B):
-                    results[b][part.key] = out[b]
+                results[part.key] = self._measure_rows(states, part, streams)
             elif isinstance(part, G.NoiseGate):
-                self._run_plans(states, [self._channel_plan(part, r.draw) for r in rngs])
+                self._channel_rows(states, part, streams)
             else:
                 self._apply_segment(states, part, pr, B)
         return results
 
     # ------------------------------------------------------------------ noise channels
-    _PAULI = ([[0, 1], [1, 0]], [[0, -1j], [1j, 0]], [[1, 0], [0, -1]])
-    _PROJ = {'p0': [[1, 0], [0, 0]], 'p1': [[0, 0], [0, 1]]}
+    _PAULI = np.array([[[0, 1], [1, 0]], [[0, -1j], [1j, 0]], [[1, 0], [0, -1]]], dtype=np.complex128)
+    _P0 = np.array([[1, 0], [0, 0]], dtype=np.complex128)
+    _P1 = np.array([[0, 0], [0, 1]], dtype=np.complex128)
 
-    def _run_plans(self, states, plans):
-        """Drive one plan per trajectory (trajectory b on states[b]) until all are done, serving
-        their requests in rounds: every ``('apply', m, q, ctrls)`` of a round in one launch, every
-        ``('norm', m, q, ctrls)`` (||m psi||^2), ``('p0', q)`` and ``('p1', q)`` (the squared norm
-        of the part of psi with qubit q = 0 or 1, ZeroStateVdot / OneStateVdot) of a round in one
-        reduction with one copy to the host.  A plan is a generator: it yields a request, receives
-        the norm (None for an apply) and returns its result."""
-        results = [None] * len(plans)
-        pending = {}
-
-        def advance(b, value):
-            try:
-                pending[b] = plans[b].send(value)
-            except StopIteration as stop:
-                results[b] = stop.value
-
-        for b in range(len(plans)):
-            advance(b, None)
-        while pending:
-            round_, pending = pending, {}
-            applies = [(b, r) for b, r in round_.items() if r[0] == 'apply']
-            norms = [(b, ('norm', self._PROJ[r[0]], r[1], ())) if r[0] in self._PROJ else (b, r)
-                     for b, r in round_.items() if r[0] != 'apply']
-            if applies:
-                self._rows_matrix1('mqb_rows_apply_matrix1', states, applies)
-            values = self._rows_matrix1('mqb_rows_matrix1_norm', states, norms) if norms else {}
-            for b in round_:
-                advance(b, values.get(b))
-        return results
-
-    def _rows_matrix1(self, fn, states, reqs):
-        """One mqb_rows_* call for [(row, (kind, m, q, ctrls))]; the norms by row for the norm call."""
-        k = len(reqs)
-        rows = np.fromiter((b for b, _ in reqs), dtype=np.int64, count=k)
-        qubits = np.fromiter((int(r[2]) for _, r in reqs), dtype=np.int32, count=k)
-        masks = np.fromiter((sum(1 << int(c) for c in r[3]) for _, r in reqs), dtype=np.uint64, count=k)
-        mats = np.ascontiguousarray(np.array([r[1] for _, r in reqs], dtype=np.complex128).reshape(k, 4)).view(np.float64)
+    def _rows_args(self, states, rows, mats, q, mask):
+        k = len(rows)
+        self._rows_keep = (np.ascontiguousarray(rows, dtype=np.int64), np.full(k, int(q), dtype=np.int32),
+                           np.full(k, int(mask), dtype=np.uint64),
+                           np.ascontiguousarray(np.broadcast_to(mats, (k, 2, 2)), dtype=np.complex128)
+                           .reshape(k, 4).view(np.float64))
         vp = ctypes.c_void_p
-        args = [self.n_qubits, self.precision, _ptr(states), states.shape[0], k, rows.ctypes.data_as(vp),
-                qubits.ctypes.data_as(vp), masks.ctypes.data_as(vp), mats.ctypes.data_as(vp)]
-        if fn == 'mqb_rows_apply_matrix1':
-            N.call(fn, *args, _stream())
-            return None
-        out = torch.empty(k, dtype=torch.float64, device=self.device)
-        N.call(fn, *args, _ptr(out), _stream())
-        return dict(zip(rows.tolist(), out.cpu().numpy().tolist()))
+        return [self.n_qubits, self.precision, _ptr(states), states.shape[0], k] + \
+            [a.ctypes.data_as(vp) for a in self._rows_keep]
+
+    def _rows_apply(self, states, rows, mats, q, mask=0):
+        """mats[i] (or one 2x2 matrix for all) on qubit q of states[rows[i]] where every bit of
+        ``mask`` is set, in place, one launch (mqb_rows_apply_matrix1)."""
+        if len(rows):
+            N.call('mqb_rows_apply_matrix1', *self._rows_args(states, rows, mats, q, mask), _stream())
+
+    def _rows_norm(self, states, rows, mats, q, mask=0):
+        """||M_i states[rows[i]]||^2 for every row in one reduction, copied to the host
+        (mqb_rows_matrix1_norm); with M = [[1, 0], [0, 0]] or [[0, 0], [0, 1]] and no mask, the
+        reference's ZeroStateVdot / OneStateVdot."""
+        if not len(rows):
+            return np.zeros(0)
+        out = torch.empty(len(rows), dtype=torch.float64, device=self.device)
+        N.call('mqb_rows_matrix1_norm', *self._rows_args(states, rows, mats, q, mask), _ptr(out), _stream())
+        return out.cpu().numpy()
 
     @staticmethod
     def _pauli_index(cum, r):
-        """lower_bound over [0, px, px+py, px+py+pz, 1]: 0 = X, 1 = Y, 2 = Z, 3 = identity."""
-        import bisect
+        """lower_bound over [0, px, px+py, px+py+pz, 1] for every draw in ``r``: 0 = X, 1 = Y,
+        2 = Z, 3 = identity."""
+        it = np.searchsorted(np.asarray(cum, dtype=np.float64), r, side='left')
+        return np.where(it > 0, it - 1, 0)
 
-        it = bisect.bisect_left(cum, r)
-        return it - 1 if it > 0 else 0
-
-    def _channel_plan(self, g, draw):
-        """One trajectory step of a channel as a plan (see _run_plans), VectorState::ApplyChannel
-        (vector_state.tpp:465-709): the draws come from ``draw`` in the reference's order, the
-        probabilities that depend on the state (damping, Kraus, thermal relaxation) are reduced
-        on the device in FP64, and an operator followed by a renormalisation is one matrix (the
-        operator over the square root of its probability)."""
-        objs, ctrls = list(g.obj_qubits), tuple(g.ctrl_qubits)
-        pauli = self._PAULI
+    def _channel_rows(self, states, g, streams):
+        """One step of a channel on every trajectory of ``states`` at once
+        (VectorState::ApplyChannel, vector_state.tpp:465-709).  Trajectory b draws from stream b
+        in the reference's order; the probabilities that depend on the state (damping, Kraus,
+        thermal relaxation) are FP64 reductions on the device, one per step for all trajectories;
+        each trajectory's operator (the chosen Kraus operator over the square root of its
+        probability, or a Pauli) is applied to all trajectories in one launch."""
+        rows = np.arange(states.shape[0])
+        objs = [int(q) for q in g.obj_qubits]
+        mask = sum(1 << int(c) for c in g.ctrl_qubits)
+        P = self._PAULI
         if isinstance(g, G.PauliChannel):
-            k = self._pauli_index(g.cumulative_probs(), draw())
-            if k < 3:
-                yield ('apply', pauli[k], objs[0], ctrls)
+            k = self._pauli_index(g.cumulative_probs(), streams.take(rows))
+            self._rows_apply(states, rows[k < 3], P[k[k < 3]], objs[0], mask)
         elif isinstance(g, G.GroupedPauliChannel):
             picks = []
-            for q, row in zip(objs, g.probs):
-                px, py, pz = (float(v) for v in row)
-                k = self._pauli_index([0.0, px, px + py, px + py + pz, px + py + pz + (1 - px - py - pz)], draw())
-                if k < 3:
-                    picks.append((k, q))
-            for k, q in picks:    # ApplyPauliString: no controls
-                yield ('apply', pauli[k], q, ())
+            for q, prow in zip(objs, g.probs):
+                px, py, pz = (float(v) for v in prow)
+                cum = [0.0, px, px + py, px + py + pz, px + py + pz + (1 - px - py - pz)]
+                picks.append((q, self._pauli_index(cum, streams.take(rows))))
+            for q, k in picks:    # ApplyPauliString: no controls
+                self._rows_apply(states, rows[k < 3], P[k[k < 3]], q)
         elif isinstance(g, G.DepolarizingChannel):
-            idx, p = 0, float(g.p)
-            while idx < len(objs):
-                if draw() < p * 3.0 / 4.0:
-                    p_i = draw()
-                    yield ('apply', pauli[0 if p_i < 1.0 / 3.0 else (1 if p_i < 2.0 / 3.0 else 2)], objs[idx], ctrls)
+            active, idx, p = rows, 0, float(g.p)
+            while idx < len(objs) and len(active):
+                hit = streams.take(active) < p * 3.0 / 4.0
+                chosen = active[hit]
+                if len(chosen):
+                    p_i = streams.take(chosen)
+                    self._rows_apply(states, chosen, P[np.where(p_i < 1.0 / 3.0, 0, np.where(p_i < 2.0 / 3.0, 1, 2))],
+                                     objs[idx], mask)
                     for q in objs[idx + 1:]:
-                        p_i = draw()
-                        if p_i < 0.75:
-                            yield ('apply', pauli[0 if p_i < 0.25 else (1 if p_i < 0.5 else 2)], q, ctrls)
-                    break
+                        p_i = streams.take(chosen)
+                        sel = p_i < 0.75
+                        k = np.where(p_i < 0.25, 0, np.where(p_i < 0.5, 1, 2))
+                        self._rows_apply(states, chosen[sel], P[k[sel]], q, mask)
+                active = active[~hit]
                 if not 4 > 3 * p:
                     break
                 idx, p = idx + 1, p / (4 - 3 * p)
         elif isinstance(g, G.KrausChannel):
-            total = 1.0
+            active = rows
+            total = np.ones(len(rows))
             for m in np.asarray(g.kraus_op, dtype=np.complex128):
+                if not len(active):
+                    break
                 if abs(m[0, 1]) < 1e-6 and abs(m[1, 0]) < 1e-6 and abs(m[0, 0] - m[1, 1]) < 1e-6:
                     prob = float((m[0, 0] * np.conj(m[0, 0])).real)
-                    rel = prob / total
-                    total -= prob
-                    if draw() < rel:
-                        if m[0, 0].imag >= 1e-6:   # identity with a phase
-                            v = m[0, 0] / math.sqrt(prob)
-                            yield ('apply', [[v, 0], [0, v]], 0, ())
-                        return
+                    with np.errstate(divide='ignore', invalid='ignore'):
+                        rel = prob / total[active]
+                    total[active] -= prob
+                    chosen = streams.take(active) < rel
+                    if m[0, 0].imag >= 1e-6:   # identity with a phase
+                        v = m[0, 0] / math.sqrt(prob)
+                        self._rows_apply(states, active[chosen], np.array([[v, 0], [0, v]]), 0)
                 else:
-                    prob = yield ('norm', m, objs[0], ctrls)
-                    rel = prob / total
-                    total -= prob
-                    if draw() < rel:
-                        yield ('apply', m / math.sqrt(prob), objs[0], ctrls)
-                        return
+                    prob = self._rows_norm(states, active, m, objs[0], mask)
+                    with np.errstate(divide='ignore', invalid='ignore'):
+                        rel = prob / total[active]
+                    total[active] -= prob
+                    chosen = streams.take(active) < rel
+                    self._rows_apply(states, active[chosen], m[None] / np.sqrt(prob[chosen])[:, None, None], objs[0],
+                                     mask)
+                active = active[~chosen]
         elif isinstance(g, (G.AmplitudeDampingChannel, G.PhaseDampingChannel)):
-            renorm = yield ('p1', objs[0])
-            if renorm < 1e-6:
-                return
-            gamma = float(g.gamma)
-            prob = gamma * renorm
-            if draw() <= prob:
+            renorm = self._rows_norm(states, rows, self._P1, objs[0])   # OneStateVdot: controls ignored
+            live = renorm >= 1e-6
+            act, rn = rows[live], renorm[live]
+            if len(act):
+                gamma = float(g.gamma)
+                prob = gamma * rn
+                jump = streams.take(act) <= prob
+                stay = ~jump
+                mats = np.zeros((len(act), 2, 2), dtype=np.complex128)
                 if isinstance(g, G.AmplitudeDampingChannel):
-                    yield ('apply', [[0, 1 / math.sqrt(renorm)], [0, 0]], objs[0], ctrls)
+                    mats[jump, 0, 1] = 1 / np.sqrt(rn[jump])
                 else:
-                    yield ('apply', [[0, 0], [0, 1 / math.sqrt(renorm)]], objs[0], ctrls)
-            else:
-                a, b = 1 / math.sqrt(1 - prob), math.sqrt(1 - gamma) / math.sqrt(1 - prob)
-                yield ('apply', [[a, 0], [0, b]], objs[0], ctrls)
+                    mats[jump, 1, 1] = 1 / np.sqrt(rn[jump])
+                mats[stay, 0, 0] = 1 / np.sqrt(1 - prob[stay])
+                mats[stay, 1, 1] = math.sqrt(1 - gamma) / np.sqrt(1 - prob[stay])
+                self._rows_apply(states, act, mats, objs[0], mask)
         elif isinstance(g, G.ThermalRelaxationChannel):
             t1, t2, tg = float(g.t1), float(g.t2), float(g.gate_time)
             e1, e2 = math.exp(-tg / t1), math.exp(-tg / t2)
@@ -412,33 +408,35 @@ class MQVectorB200(BackendBase):
             q = objs[0]
             if t1 >= t2:
                 pz = e1 * (1 - e2 / e1) / 2
-                r = draw()
-                if r < 1 - pz - p_reset:
-                    return
-                if r < 1 - p_reset:
-                    yield ('apply', pauli[2], q, ctrls)
-                else:
-                    zero = yield ('p0', q)   # ZeroStateVdot: the state need not be normalised
-                    if draw() < zero:
-                        yield ('apply', [[1 / math.sqrt(zero), 0], [0, 0]], q, ctrls)
-                    else:
-                        yield ('apply', [[0, 1 / math.sqrt(1 - zero)], [0, 0]], q, ctrls)
+                r = streams.take(rows)
+                self._rows_apply(states, rows[(r >= 1 - pz - p_reset) & (r < 1 - p_reset)], P[2], q, mask)
+                reset = rows[r >= 1 - p_reset]
+                if len(reset):
+                    zero = self._rows_norm(states, reset, self._P0, q)   # ZeroStateVdot
+                    to_zero = streams.take(reset) < zero
+                    mats = np.zeros((len(reset), 2, 2), dtype=np.complex128)
+                    mats[to_zero, 0, 0] = 1 / np.sqrt(zero[to_zero])
+                    mats[~to_zero, 0, 1] = 1 / np.sqrt(1 - zero[~to_zero])
+                    self._rows_apply(states, reset, mats, q, mask)
             elif 2 * t1 > t2:
-                r = draw()
+                r = streams.take(rows)
                 root = math.sqrt(p_reset * p_reset + 4 * e2 * e2)
                 ev0, ev1 = (2 - p_reset + root) / 2, (2 - p_reset - root) / 2
                 vec0, vec1 = (ev0 - e1) / e2, (ev1 - e1) / e2
-                zero = yield ('p0', q)   # ZeroStateVdot: the state need not be normalised
+                zero = self._rows_norm(states, rows, self._P0, q)   # ZeroStateVdot
                 one = 1 - zero
                 c0 = vec0 * vec0 * zero + one
-                p0 = c0 * ev0 / (vec0 * vec0 + 1)
-                if r < p0:
-                    yield ('apply', [[vec0 / math.sqrt(c0), 0], [0, 1 / math.sqrt(c0)]], q, ctrls)
-                elif r < 1 - p_reset * one:
-                    c1 = vec1 * vec1 * zero + one
-                    yield ('apply', [[vec1 / math.sqrt(c1), 0], [0, 1 / math.sqrt(c1)]], q, ctrls)
-                else:
-                    yield ('apply', [[0, 1 / math.sqrt(one)], [0, 0]], q, ctrls)
+                c1 = vec1 * vec1 * zero + one
+                b0 = r < c0 * ev0 / (vec0 * vec0 + 1)
+                b1 = ~b0 & (r < 1 - p_reset * one)
+                b2 = ~b0 & ~b1
+                mats = np.zeros((len(rows), 2, 2), dtype=np.complex128)
+                mats[b0, 0, 0] = vec0 / np.sqrt(c0[b0])
+                mats[b0, 1, 1] = 1 / np.sqrt(c0[b0])
+                mats[b1, 0, 0] = vec1 / np.sqrt(c1[b1])
+                mats[b1, 1, 1] = 1 / np.sqrt(c1[b1])
+                mats[b2, 0, 1] = 1 / np.sqrt(one[b2])
+                self._rows_apply(states, rows, mats, q, mask)
         else:
             raise ValueError(f"{g.name} is not a noise channel.")
 
@@ -881,7 +879,7 @@ class MQVectorB200(BackendBase):
                 part = ids[a:a + chunk]
                 states = self.state.reshape(1, -1).repeat(len(part), 1)
                 self._run_batch(states, plan.circuit, (list(plan.slot_names), rows[[job_row[k] for k in part]]),
-                                [Mt19937Uniform(job_seed[k]) for k in part])
+                                UniformBlocks([job_seed[k] for k in part]))
                 targets = range(n_h) if ham < 0 else (ham,)
                 res = torch.zeros((len(targets), len(part), 2), dtype=torch.float64, device=self.device)
                 for t, j in enumerate(targets):
@@ -990,10 +988,9 @@ class MQVectorB200(BackendBase):
             for a in range(0, shots, chunk):
                 part = seeds[a:a + chunk]
                 states = self.state.reshape(1, -1).repeat(len(part), 1)
-                outs = self._run_batch(states, circuit, pr, [Mt19937Uniform(x) for x in part])
-                for i, out in enumerate(outs):
-                    for k, v in out.items():
-                        samples[a + i, key_map[k]] = v
+                outs = self._run_batch(states, circuit, pr, UniformBlocks(part))
+                for k, v in outs.items():
+                    samples[a:a + len(part), key_map[k]] = v
                 del states
         res.collect_data(samples)
         return res

@@ -176,64 +176,93 @@ def noisy_circuit():
     return c
 
 
-def _serve_plan(plan, qs, n):
-    """Serve a channel or measurement plan's requests with numpy (the device reductions and
-    applies of the batched driver, restated) and return the plan's result."""
+class _NumpyRows:
+    """MQVectorB200's trajectory driver with its device calls (row-wise 2x2 applies and norms,
+    unitary segments) served by numpy and the oracle, so the channel logic runs on the host."""
+
+    def __new__(cls, n):
+        from mindquantum_b200.simulator.mqvector_b200 import MQVectorB200
+
+        class Host(MQVectorB200):
+            def __init__(self):   # pylint: disable=super-init-not-called
+                self.n_qubits = n
+
+            def _rows_apply(self, states, rows, mats, q, mask=0):
+                mats = np.broadcast_to(np.asarray(mats, dtype=complex), (len(rows), 2, 2))
+                for r, m in zip(rows, mats):
+                    states[r] = _on(states[r], n, m, q, mask)
+
+            def _rows_norm(self, states, rows, mats, q, mask=0):
+                mats = np.broadcast_to(np.asarray(mats, dtype=complex), (len(rows), 2, 2))
+                return np.array([float(np.vdot(t, t).real) for t in
+                                 (_on(states[r], n, m, q, mask) for r, m in zip(rows, mats))])
+
+            def _apply_segment(self, states, circuit, pr, batch=1):
+                for r in range(batch):
+                    for g in circuit:
+                        O.apply_gate(states[r], n, g, pr)
+
+        return Host()
+
+
+def _on(psi, n, m, q, mask):
     idx = np.arange(1 << n)
-
-    def on(m, q, ctrls):
-        m = np.asarray(m, dtype=complex)
-        out = qs.copy()
-        mask = sum(1 << int(c) for c in ctrls)
-        i0 = idx[(((idx >> q) & 1) == 0) & ((idx & mask) == mask)]
-        i1 = i0 | (1 << q)
-        out[i0] = m[0, 0] * qs[i0] + m[0, 1] * qs[i1]
-        out[i1] = m[1, 0] * qs[i0] + m[1, 1] * qs[i1]
-        return out
-
-    val = None
-    try:
-        while True:
-            req = plan.send(val)
-            if req[0] == 'apply':
-                qs[:] = on(*req[1:])
-                val = None
-            elif req[0] in ('p0', 'p1'):
-                val = float(np.sum(np.abs(qs[((idx >> req[1]) & 1) == int(req[0] == 'p1')]) ** 2))
-            else:
-                t = on(*req[1:])
-                val = float(np.vdot(t, t).real)
-    except StopIteration as stop:
-        return stop.value
+    out = psi.copy()
+    i0 = idx[(((idx >> q) & 1) == 0) & ((idx & mask) == mask)]
+    i1 = i0 | (1 << q)
+    out[i0] = m[0, 0] * psi[i0] + m[0, 1] * psi[i1]
+    out[i1] = m[1, 0] * psi[i0] + m[1, 1] * psi[i1]
+    return out
 
 
-def test_channel_plans_follow_the_oracle_draw_for_draw():
-    """The trajectory logic the batched driver runs (one plan per channel or measurement, its
-    requests served here by numpy) equals the oracle's shots one by one: 200 shots of a circuit
-    with every channel kind and measurements in the middle.  A controlled damping channel leaves
-    the state unnormalised (the reference renormalises by the uncontrolled population), so the
-    thermal-relaxation channel after it must take P(q = 0) as the reference does, not 1 - P(q = 1)."""
-    from mindquantum_b200.simulator.mqvector_b200 import MQVectorB200 as M
+@pytest.mark.parametrize("batched", [True, False])
+def test_trajectory_driver_follows_the_oracle_draw_for_draw(batched):
+    """The trajectory logic of the device driver (every channel and measurement step vectorised
+    over the trajectories, its device calls served here by numpy) equals the oracle's shots one by
+    one: 200 shots of a circuit with every channel kind and measurements in the middle, all at
+    once from read-ahead streams, or one at a time from exact streams.  A controlled damping
+    channel leaves the state unnormalised (the reference renormalises by the uncontrolled
+    population), so the thermal-relaxation channel after it must take P(q = 0) as the reference
+    does, not 1 - P(q = 1)."""
+    from mindquantum_b200.simulator.rng import Mt19937Uniform, UniformBlocks, UniformStreams
 
     circ = _measured_noisy_circuit()
     pr = {'a': 0.7, 'b': -1.3, 'c': 2.1}
     n, shots = 3, 200
     keys, ref = O.sampling_general(n, circ, pr, shots, 29)
-    rng = O._Mt19937(29)   # pylint: disable=protected-access
-    host = M.__new__(M)
-    for s in range(shots):
-        sub = O._Mt19937(int(O._uniform(rng, 1.0, float(1 << 20))))   # pylint: disable=protected-access
-        draw = lambda: O._uniform(sub, 0.0, 1.0)   # noqa: E731  pylint: disable=cell-var-from-loop
-        qs = O.zero_state(n, np.complex128)
-        out = {}
-        for g in circ:
-            if isinstance(g, G.Measure):
-                out[g.key] = _serve_plan(M._measure_plan(g, draw), qs, n)   # pylint: disable=protected-access
-            elif isinstance(g, G.NoiseGate):
-                _serve_plan(host._channel_plan(g, draw), qs, n)   # pylint: disable=protected-access
-            else:
-                O.apply_gate(qs, n, g, pr)
-        assert [out[k] for k in keys] == list(ref[s]), s
+    rng = Mt19937Uniform(29)
+    seeds = [int(rng.draw(low=1.0, high=float(1 << 20))) for _ in range(shots)]
+    host = _NumpyRows(n)
+    if batched:
+        states = np.zeros((shots, 1 << n), dtype=np.complex128)
+        states[:, 0] = 1
+        out = host._run_batch(states, circ, pr, UniformBlocks(seeds, block=7))   # pylint: disable=protected-access
+        got = np.stack([out[k] for k in keys], axis=1)
+    else:
+        got = np.zeros_like(ref)
+        for s in range(shots):
+            states = np.zeros((1, 1 << n), dtype=np.complex128)
+            states[0, 0] = 1
+            out = host._run_batch(states, circ, pr, UniformStreams([Mt19937Uniform(seeds[s])]))  # pylint: disable=W0212
+            got[s] = [out[k][0] for k in keys]
+    assert np.array_equal(got, ref), np.where(np.any(got != ref, axis=1))[0]
+
+
+def test_uniform_blocks_equal_the_streams():
+    from mindquantum_b200.simulator.rng import Mt19937Uniform, UniformBlocks
+
+    seeds = [3, 99, 12345]
+    blocks = UniformBlocks(seeds, block=5)
+    ref = [Mt19937Uniform(x).draw(40) for x in seeds]
+    cur = [0, 0, 0]
+    rng = np.random.default_rng(0)
+    for _ in range(60):
+        rows = np.flatnonzero(rng.random(3) < 0.6)
+        got = blocks.take(rows)
+        for r, v in zip(rows, got):
+            if cur[r] < 40:
+                assert v == ref[r][cur[r]]
+            cur[r] += 1
 
 
 # ------------------------------------------------------------------------------------------- GPU
