@@ -9,8 +9,9 @@
 // caller can substitute the identity for threads whose controls on thread or tile bits are not
 // set (no branch, the code stays straight-line).
 //
-// Math per amplitude: dense 2x2 8 FMA-class instructions, real 2x2 and RX-like 4, diagonal 4,
-// X 0 (register renaming), dense 4x4 16.
+// Math per amplitude: dense 2x2 8 FMA-class instructions, real 2x2 and RX-like 4 (a real 2x2 in
+// complex64 on sm_100: 2 packed FP32 instructions), diagonal 4, X 0 (register renaming), dense
+// 4x4 16.
 #ifndef MQB_REGMATH_CUH_
 #define MQB_REGMATH_CUH_
 
@@ -50,6 +51,39 @@ __device__ __forceinline__ V rxl(R a, V x, R b, V y) {  // a x + i b y, a and b 
     r.y = fma(a, x.y, b * y.x);
     return r;
 }
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+// complex64 on sm_100: a real 2x2 row as two packed FP32 instructions (FMUL2, FFMA2) instead of
+// four scalar ones; per component the same rounding as the scalar form above.
+__device__ __forceinline__ float2 rlin(float a, float2 x, float b, float2 y) {
+    return __ffma2_rn(make_float2(a, a), x, __fmul2_rn(make_float2(b, b), y));
+}
+#endif
+
+// Accumulator of Re(conj(l) x) terms: complex64 keeps the (l.x x.x, l.y x.y) sums apart in one
+// packed register (one FFMA2 per term on sm_100), complex128 one FP64 sum (two FMAs per term).
+template <typename V>
+struct ReAcc;
+template <>
+struct ReAcc<float2> {
+    typedef float2 type;
+};
+template <>
+struct ReAcc<double2> {
+    typedef double type;
+};
+__device__ __forceinline__ float2 ra_zero(float2) { return make_float2(0.f, 0.f); }
+__device__ __forceinline__ double ra_zero(double) { return 0.0; }
+__device__ __forceinline__ float2 ra_add(float2 a, float2 l, float2 x) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    return __ffma2_rn(l, x, a);
+#else
+    return make_float2(fmaf(l.x, x.x, a.x), fmaf(l.y, x.y, a.y));
+#endif
+}
+__device__ __forceinline__ double ra_add(double a, double2 l, double2 x) { return fma(l.x, x.x, fma(l.y, x.y, a)); }
+__device__ __forceinline__ float ra_sum(float2 a) { return a.x + a.y; }
+__device__ __forceinline__ double ra_sum(double a) { return a; }
+
 template <typename V>
 __device__ __forceinline__ decltype(V::x) redot(V l, V y) {  // Re(conj(l) y)
     return fma(l.x, y.x, l.y * y.y);
@@ -367,9 +401,10 @@ __device__ __forceinline__ R im_acc(V l, V x, R acc) {  // acc + Im(conj(l) x)
 template <typename V, int RB, int NH, int P, unsigned CM, typename R>
 __device__ __forceinline__ void jbg_ry(V (&v)[1 << RB], V (&l)[NH][1 << RB], R a00, R a01, R a10, R a11, R gs,
                                        R (&acc)[3][NH]) {
-    R g[NH];
+    typedef typename ReAcc<V>::type A;
+    A gp[NH], gm[NH];
 #pragma unroll
-    for (int h = 0; h < NH; ++h) g[h] = 0;
+    for (int h = 0; h < NH; ++h) gp[h] = gm[h] = ra_zero(A());
 #pragma unroll
     for (int j = 0; j < (1 << RB); ++j) {
         if (!pair_on<P, CM>(j)) continue;
@@ -377,8 +412,8 @@ __device__ __forceinline__ void jbg_ry(V (&v)[1 << RB], V (&l)[NH][1 << RB], R a
         const V x0 = v[j], x1 = v[j | bit];
 #pragma unroll
         for (int h = 0; h < NH; ++h) {
-            g[h] = re_acc(l[h][j | bit], x0, g[h]);
-            g[h] = re_acc(l[h][j], cval<V>(-x1.x, -x1.y), g[h]);
+            gp[h] = ra_add(gp[h], l[h][j | bit], x0);
+            gm[h] = ra_add(gm[h], l[h][j], x1);
         }
         v[j] = rlin(a00, x0, a01, x1);
         v[j | bit] = rlin(a10, x0, a11, x1);
@@ -390,7 +425,7 @@ __device__ __forceinline__ void jbg_ry(V (&v)[1 << RB], V (&l)[NH][1 << RB], R a
         }
     }
 #pragma unroll
-    for (int h = 0; h < NH; ++h) acc[0][h] += gs * g[h];
+    for (int h = 0; h < NH; ++h) acc[0][h] += gs * (ra_sum(gp[h]) - ra_sum(gm[h]));
 }
 
 // RX-like: G = X, Re<l| -i/2 X |x> = (Im(conj(l0) x1) + Im(conj(l1) x0)) / 2; U^dag = [[a, i nb], [i nb, a]]

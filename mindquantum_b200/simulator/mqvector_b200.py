@@ -581,6 +581,9 @@ class MQVectorB200(BackendBase):
             init = init_state.to(device=self.device, dtype=self.torch_dtype).contiguous()
             init_batched = 1 if init.dim() == 2 else 0
         ham_arr = (ctypes.c_void_p * len(nh))(*[h.handle.value for h in nh])
+        # the previous call's workspace (kept for its norm checks) goes back to the allocator first,
+        # so this call can take the same memory
+        self._last_grad = None
         stride = self._choose_stride(prog, batch, len(nh)) if ckpt_stride is None else int(ckpt_stride)
         ws_bytes = ctypes.c_size_t()
         N.call('mqb_grad_workspace_size', prog.handle, batch, len(nh), stride, ctypes.byref(ws_bytes))
