@@ -6,6 +6,8 @@
 #include <cmath>
 #include <complex>
 #include <cstdarg>
+#include <cstdint>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -373,6 +375,37 @@ static void apply_impl(mqb_program &p, void *states, int64_t batch, const double
 }
 
 // Hamiltonian passes: out = H ket (if out), f += <bra|H ket> (if fout)
+// Whether a Hamiltonian group runs as the TMA-ring pass (MQB_HAM_RING=0 keeps the synchronous
+// one): 2^(K-4) threads of at least one warp and at most 256, 16-byte-aligned buffers, and three
+// buffers per operand in shared memory (two when the previous sum is staged too).  Sets rg.nb.
+template <typename R>
+static bool ham_ring_fits(const HamArgs<R> &a, HamRingGeom &rg) {
+    static const bool on = [] {
+        const char *e = std::getenv("MQB_HAM_RING");
+        return !(e && e[0] == '0');
+    }();
+    static const int stage = [] {   // MQB_HAM_RING_STAGE=0: read the previous sum instead of staging it
+        const char *e = std::getenv("MQB_HAM_RING_STAGE");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    const int threads = 1 << std::max(0, a.g.K - kHamRegBits);
+    if (!on || a.g.K < 5 + kHamRegBits || threads > 256 || a.g.qbits[0] != 0) return false;
+    if ((reinterpret_cast<uintptr_t>(a.ket) & 15) || (reinterpret_cast<uintptr_t>(a.out) & 15)) return false;
+    rg.stage_prev = stage;
+    const bool staged = a.accumulate && a.out && stage;
+    static const int nb_max = [] {   // MQB_HAM_RING_BUFFERS: buffers per operand (2..4, tuning)
+        const char *e = std::getenv("MQB_HAM_RING_BUFFERS");
+        return e ? std::max(2, std::min(4, std::atoi(e))) : 3;
+    }();
+    for (int nb = nb_max; nb >= 2; --nb) {
+        if (ham_ring_smem(a.g, int(sizeof(cplx<R>)), threads, a.n_classes, a.n_terms, staged, nb) <= 220 * 1024) {
+            rg.nb = nb;
+            return true;
+        }
+    }
+    return false;
+}
+
 template <typename R>
 static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R> *ket, cplx<R> *out, double *fout,
                      int64_t f_stride, int64_t batch, cudaStream_t st) {
@@ -419,7 +452,18 @@ static void ham_impl(const mqb_hamiltonian &h, const cplx<R> *bra, const cplx<R>
         a.out_batch_stride = dim;
         a.f_stride = f_stride;
         TimeScope ts(TK_HAM, st);
-        ck(launch_ham<R>(a, sm, st), "hamiltonian pass");
+        HamRingGeom rg{};
+        if (ham_ring_fits(a, rg)) {
+            std::vector<int> qb(g.geom.qbits, g.geom.qbits + g.geom.K);
+            alignas(64) unsigned char mk[128], mo[128];
+            tile_tma_plan(qb, h.precision, &rg.tg, rg.land);
+            tile_tma_map(mk, ket, h.n, batch, qb, h.precision);
+            tile_tma_map(mo, a.accumulate && out && rg.stage_prev ? out : nullptr, h.n, batch, qb, h.precision);
+            rg.err = jit_error_word();
+            ck(launch_ham_ring<R>(a, rg, mk, mo, sm, st), "hamiltonian pass");
+        } else {
+            ck(launch_ham<R>(a, sm, st), "hamiltonian pass");
+        }
     }
 }
 

@@ -1345,6 +1345,16 @@ cudaError_t launch_pipe(const void *kernel, void **argv, int threads, size_t sme
 
 }  // namespace
 
+void tile_tma_plan(const std::vector<int> &qbits, int precision, TmaGeom *tg, int8_t *land) {
+    const PassPlan pl = pass_plan(qbits, precision);
+    *tg = pl.tg;
+    for (size_t i = 0; i < pl.land.size(); ++i) land[i] = int8_t(pl.land[i]);
+}
+
+void tile_tma_map(void *map, const void *base, int n, long long outer, const std::vector<int> &qbits, int precision) {
+    encode_map(static_cast<CUtensorMap *>(map), base, n, outer, pass_plan(qbits, precision));
+}
+
 int *jit_error_word() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) throw std::runtime_error("jit_error_word: no device");

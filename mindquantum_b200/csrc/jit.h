@@ -23,9 +23,9 @@ std::vector<const void *> jit_backward_kernels(const Schedule &s, int precision,
 size_t jit_forward_smem(const Pass &p, int precision);
 size_t jit_backward_smem(const Pass &p, int precision, int n_hams);
 
-// Launch the generated kernel of pass p over every tile of the batch: 2^(K - RB) consumer threads
-// plus one producer warp, the TMA tensor maps of the launch's buffers encoded here, and the
-// kernel's error word filled in (jit_error_word).
+// Launch the generated kernel of pass p over every tile of the batch: G consumer groups of
+// 2^(K - RB) threads, the TMA tensor maps of the launch's buffers encoded here, and the kernel's
+// error word filled in (jit_error_word).
 template <typename V>
 cudaError_t jit_launch_forward(const void *kernel, JitFwdArgs<V> a, const Pass &p, int precision, int sm_count,
                                cudaStream_t st);
@@ -36,6 +36,12 @@ cudaError_t jit_launch_backward(const void *kernel, JitBwdArgs<V> a, const Pass 
 // The error word the generated kernels of the current device report to (MQB_DEV_ERR_*; 0: none),
 // allocated on first use.
 int *jit_error_word();
+
+// TMA movement of a tile with qubits `qbits` (ascending, qbits[0] == 0), as the generated kernels
+// do it: the tensor-map geometry and the shared-memory landing bit of every tile bit, and the
+// tensor map (a CUtensorMap, 128 bytes) of the amplitudes at `base` ([outer][2^n]).
+void tile_tma_plan(const std::vector<int> &qbits, int precision, TmaGeom *tg, int8_t *land);
+void tile_tma_map(void *map, const void *base, int n, long long outer, const std::vector<int> &qbits, int precision);
 
 // Generate and compile (without loading: no GPU needed) the kernels of every fused pass, the
 // backward ones too when n_hams > 0; returns the number of distinct kernels.

@@ -16,8 +16,10 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "kernels.cuh"
+#include "pipe.cuh"
 
 namespace mqb {
 
@@ -445,6 +447,90 @@ __global__ void __launch_bounds__(kThreads) ham_kernel(const HamArgs<R> a) {
     }
 }
 
+// The weighted partner sums of one tile for one thread: for every flip class k of the group,
+// out[r] += W_k(L_r) * ket[L_r ^ flip_k] over the thread's NR = 2^NRB amplitudes L_r = tid + T r.
+// `at(r, f)` is the shared-memory index of the amplitude L_r ^ f, sflip[k] class k's flip in the
+// same index space.  W_k comes from the terms' signs, split into the thread part popc(tid & m) and
+// the register part popc((r << hi_shift) & m): a Walsh-Hadamard transform over r of per-bin sums
+// when the class has more than two terms.
+template <typename R, int NRB, typename At>
+__device__ __forceinline__ void ham_classes(const cplx<R> *ket, At at, const HamClass *cls, const uint32_t *sflip,
+                                            int n_classes, int term_begin, const uint32_t *tmask,
+                                            const cplx<R> *tcoef, int hi_shift, R (&ar)[1 << NRB],
+                                            R (&ai)[1 << NRB]) {
+    using V = cplx<R>;
+    constexpr int NR = 1 << NRB;
+    const int tid = threadIdx.x;
+    for (int k = 0; k < n_classes; ++k) {
+        const HamClass &hc = cls[k];
+        const int tb = hc.term_begin - term_begin;
+        R wr[NR], wi[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) wr[r] = wi[r] = 0;
+        uint32_t any_mask = 0;
+        if (hc.term_count <= 2)
+            for (int q = tb; q < tb + hc.term_count; ++q) any_mask |= tmask[q];
+        if (hc.term_count <= 2 && any_mask == 0) {
+            // no sign on the tile's bits (X-type terms): one weight for every amplitude
+            R cr = 0, ci = 0;
+            for (int q = tb; q < tb + hc.term_count; ++q) {
+                cr += tcoef[q].x;
+                ci += tcoef[q].y;
+            }
+            const uint32_t f = sflip[k];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const V kv = ket[at(r, f)];
+                ar[r] = fma(cr, kv.x, fma(-ci, kv.y, ar[r]));
+                ai[r] = fma(cr, kv.y, fma(ci, kv.x, ai[r]));
+            }
+            continue;
+        }
+        if (hc.term_count <= 2) {
+            for (int q = tb; q < tb + hc.term_count; ++q) {
+                const uint32_t m = tmask[q];
+                const V cq = tcoef[q];
+                const uint32_t pt = __popc(uint32_t(tid) & m);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    const bool neg = (pt + __popc((uint32_t(r) << hi_shift) & m)) & 1;
+                    wr[r] += neg ? -cq.x : cq.x;
+                    wi[r] += neg ? -cq.y : cq.y;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int bn = 0; bn < NR; ++bn) {
+                for (int q = tb + hc.bins[bn]; q < tb + hc.bins[bn + 1]; ++q) {
+                    const V cq = tcoef[q];
+                    const bool neg = __popc(uint32_t(tid) & tmask[q]) & 1;
+                    wr[bn] += neg ? -cq.x : cq.x;
+                    wi[bn] += neg ? -cq.y : cq.y;
+                }
+            }
+#pragma unroll
+            for (int sb = 0; sb < NRB; ++sb)
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    if (r >> sb & 1) continue;
+                    const int r2 = r | (1 << sb);
+                    const R xr = wr[r], xi = wi[r];
+                    wr[r] = xr + wr[r2];
+                    wi[r] = xi + wi[r2];
+                    wr[r2] = xr - wr[r2];
+                    wi[r2] = xi - wi[r2];
+                }
+        }
+        const uint32_t f = sflip[k];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const V kv = ket[at(r, f)];
+            ar[r] = fma(wr[r], kv.x, fma(-wi[r], kv.y, ar[r]));
+            ai[r] = fma(wr[r], kv.y, fma(wi[r], kv.x, ai[r]));
+        }
+    }
+}
+
 // Register-binned Hamiltonian pass.  Every thread owns the NR = 2^NRB amplitudes L = tid + T r of
 // a tile (T = 2^(K - NRB) threads), so the sign (-1)^popc(L & m) of a Pauli term splits into a
 // per-thread part popc(tid & m) and a per-register part popc(r & m_hi).  A class's weight
@@ -473,13 +559,19 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
     V *tcoef = reinterpret_cast<V *>(smem + o);
     o = align16(o + size_t(nt) * sizeof(V));
     uint32_t *tmask = reinterpret_cast<uint32_t *>(smem + o);
+    o = align16(o + size_t(nt) * sizeof(uint32_t));
+    uint32_t *sflip = reinterpret_cast<uint32_t *>(smem + o);
+    o = align16(o + size_t(a.n_classes) * sizeof(uint32_t));
     // groups after the first add to the output: their previous sum is staged with the tile
     V *prev = nullptr;
-    if (a.accumulate && a.out) prev = reinterpret_cast<V *>(smem + align16(o + size_t(nt) * sizeof(uint32_t)));
+    if (a.accumulate && a.out) prev = reinterpret_cast<V *>(smem + o);
     const int nw = T / 32, warp = tid / 32, lane = tid % 32;
     build_table(tab, g);
     for (int i = tid; i < nw * 2; i += T) wf[i] = 0;
-    for (int i = tid; i < a.n_classes; i += T) cls[i] = a.classes[i];
+    for (int i = tid; i < a.n_classes; i += T) {
+        cls[i] = a.classes[i];
+        sflip[i] = a.classes[i].lflip;
+    }
     for (int i = tid; i < nt; i += T) tmask[i] = a.terms[a.term_begin + i].lmask;
     __syncthreads();
     const int64_t n_tiles = int64_t(1) << g.n_out;
@@ -506,54 +598,9 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
         R ar[NR], ai[NR];
 #pragma unroll
         for (int r = 0; r < NR; ++r) ar[r] = ai[r] = 0;
-        for (int k = 0; k < a.n_classes; ++k) {
-            const HamClass &hc = cls[k];
-            const int tb = hc.term_begin - a.term_begin;
-            R wr[NR], wi[NR];
-#pragma unroll
-            for (int r = 0; r < NR; ++r) wr[r] = wi[r] = 0;
-            if (hc.term_count <= 2) {
-                for (int q = tb; q < tb + hc.term_count; ++q) {
-                    const uint32_t m = tmask[q];
-                    const V cq = tcoef[q];
-                    const uint32_t pt = __popc(uint32_t(tid) & m);
-#pragma unroll
-                    for (int r = 0; r < NR; ++r) {
-                        const bool neg = (pt + __popc((uint32_t(r) << hi_shift) & m)) & 1;
-                        wr[r] += neg ? -cq.x : cq.x;
-                        wi[r] += neg ? -cq.y : cq.y;
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int bn = 0; bn < NR; ++bn) {
-                    for (int q = tb + hc.bins[bn]; q < tb + hc.bins[bn + 1]; ++q) {
-                        const V cq = tcoef[q];
-                        const bool neg = __popc(uint32_t(tid) & tmask[q]) & 1;
-                        wr[bn] += neg ? -cq.x : cq.x;
-                        wi[bn] += neg ? -cq.y : cq.y;
-                    }
-                }
-#pragma unroll
-                for (int sb = 0; sb < NRB; ++sb)
-#pragma unroll
-                    for (int r = 0; r < NR; ++r) {
-                        if (r >> sb & 1) continue;
-                        const int r2 = r | (1 << sb);
-                        const R xr = wr[r], xi = wi[r];
-                        wr[r] = xr + wr[r2];
-                        wi[r] = xi + wi[r2];
-                        wr[r2] = xr - wr[r2];
-                        wi[r2] = xi - wi[r2];
-                    }
-            }
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                const V kv = ket[uint32_t(tid + T * r) ^ hc.lflip];
-                ar[r] = fma(wr[r], kv.x, fma(-wi[r], kv.y, ar[r]));
-                ai[r] = fma(wr[r], kv.y, fma(wi[r], kv.x, ai[r]));
-            }
-        }
+        ham_classes<R, NRB>(
+            ket, [&](int r, uint32_t f) { return uint32_t(tid + T * r) ^ f; }, cls, sflip, a.n_classes, a.term_begin,
+            tmask, tcoef, hi_shift, ar, ai);
         double fr = 0, fi = 0;
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
@@ -603,7 +650,203 @@ __global__ void __launch_bounds__(sizeof(R) == 4 ? 512 : 256) ham2_kernel(const 
     }
 }
 
+// The register-binned pass with its tiles moved by the TMA.  NB shared buffers per operand (the
+// tile, and the previous groups' sum when the group adds to the output) are filled by tensor
+// copies (cp.async.bulk.tensor, no multicast) that complete on one mbarrier per buffer.  The
+// block's tiles are w = blockIdx.x + i gridDim.x; thread 0 starts tile i + NB into buffer i % NB
+// once the whole block has finished tile i, so the copies of the next tiles run under the current
+// tile's classes.  A tile lies in shared memory in the copies' landing order (tile bit j at
+// position land[j]); the index map is a bit permutation, so a flip is an XOR there too.  Every
+// wait is bounded: a timeout sets the error word and ends the block after its copies drained.
+template <typename R, int NRB>
+__global__ void __launch_bounds__(256) ham_ring_kernel(const HamArgs<R> a, const HamRingGeom rg,
+                                                       const __grid_constant__ pipe::TMap mk,
+                                                       const __grid_constant__ pipe::TMap mo) {
+    using V = cplx<R>;
+    constexpr int NR = 1 << NRB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // tile buffers on 128-byte boundaries (the launch adds 128 bytes for this)
+    unsigned char *smem = smem_raw + ((128u - (pipe::saddr(smem_raw) & 127u)) & 127u);
+    const TileGeom &g = a.g;
+    const int K = g.K, c = g.c;
+    const int TS = 1 << K;
+    const int T = blockDim.x, tid = threadIdx.x;
+    const int nt = a.n_terms, NB = rg.nb;
+    const bool staged = a.accumulate && a.out && rg.stage_prev;
+    const size_t tile_bytes = size_t(TS) * sizeof(V);
+    V *ring = reinterpret_cast<V *>(smem);
+    V *pring = reinterpret_cast<V *>(smem + size_t(NB) * tile_bytes);
+    size_t o = size_t(staged ? 2 : 1) * NB * tile_bytes;
+    pipe::u64 *full = reinterpret_cast<pipe::u64 *>(smem + o);
+    o = align16(o + size_t(NB) * sizeof(pipe::u64));
+    uint64_t *tab = reinterpret_cast<uint64_t *>(smem + o);
+    o = align16(o + (size_t(1) << (K - c)) * sizeof(uint64_t));
+    double *wf = reinterpret_cast<double *>(smem + o);
+    o = align16(o + size_t(T / 32) * 2 * sizeof(double));
+    HamClass *cls = reinterpret_cast<HamClass *>(smem + o);
+    o = align16(o + size_t(a.n_classes) * sizeof(HamClass));
+    V *tcoef = reinterpret_cast<V *>(smem + o);
+    o = align16(o + size_t(nt) * sizeof(V));
+    uint32_t *tmask = reinterpret_cast<uint32_t *>(smem + o);
+    o = align16(o + size_t(nt) * sizeof(uint32_t));
+    uint32_t *sflip = reinterpret_cast<uint32_t *>(smem + o);
+    const int nw = T / 32, warp = tid / 32, lane = tid % 32;
+    auto land = [&](uint32_t L) {
+        uint32_t x = 0;
+        for (int j = 0; j < K; ++j)
+            if (L >> j & 1) x |= 1u << rg.land[j];
+        return x;
+    };
+    if (tid == 0) {
+        for (int b = 0; b < NB; ++b) pipe::mbar_init(&full[b], 1);
+        pipe::fence_mbar_init();
+    }
+    build_table(tab, g);
+    for (int i = tid; i < nw * 2; i += T) wf[i] = 0;
+    for (int i = tid; i < a.n_classes; i += T) {
+        cls[i] = a.classes[i];
+        sflip[i] = land(a.classes[i].lflip);
+    }
+    for (int i = tid; i < nt; i += T) tmask[i] = a.terms[a.term_begin + i].lmask;
+    const int hi_shift = K - NRB;
+    const uint32_t lt = land(uint32_t(tid));
+    uint32_t lr[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) lr[r] = land(uint32_t(r) << hi_shift);
+    __syncthreads();
+    const int64_t n_tiles = int64_t(1) << g.n_out;
+    const int64_t dim = int64_t(1) << g.n;
+    const int64_t total = a.batch * n_tiles;
+    const int64_t first = blockIdx.x, step = gridDim.x;
+    const int64_t count = first < total ? (total - first + step - 1) / step : 0;
+    const uint32_t lowmask = (1u << c) - 1u;
+    const bool bra_is_ket = a.bra == a.ket;
+    const unsigned tx = unsigned(tile_bytes) * (staged ? 2u : 1u);
+    auto issue = [&](int64_t i) {   // thread 0: the copies of the block's tile i into buffer i % NB
+        const int64_t w = first + i * step;
+        const uint64_t gb = (uint64_t(w >> g.n_out) << g.n) | tile_base(g, uint64_t(w) & uint64_t(n_tiles - 1));
+        const int buf = int(i % NB);
+        pipe::mbar_expect_tx(&full[buf], tx);
+        pipe::load_tile(&mk, rg.tg, gb, reinterpret_cast<unsigned char *>(ring + size_t(buf) * TS), &full[buf]);
+        if (staged)
+            pipe::load_tile(&mo, rg.tg, gb, reinterpret_cast<unsigned char *>(pring + size_t(buf) * TS), &full[buf]);
+    };
+    if (tid == 0)
+        for (int64_t i = 0; i < NB && i < count; ++i) issue(i);
+    int64_t i = 0;
+    bool failed = false;
+    for (; i < count; ++i) {
+        const int buf = int(i % NB);
+        if (!__syncthreads_and(pipe::mbar_wait(&full[buf], unsigned(i / NB) & 1u))) {
+            failed = true;
+            break;
+        }
+        const int64_t w = first + i * step;
+        const int64_t b = w >> g.n_out;
+        const uint64_t base = tile_base(g, uint64_t(w) & uint64_t(n_tiles - 1));
+        const V *ket = ring + size_t(buf) * TS;
+        const V *prev = pring + size_t(buf) * TS;
+        for (int q = tid; q < nt; q += T) {
+            const HamTerm &ht = a.terms[a.term_begin + q];
+            const bool neg = __popcll(base & ht.omask) & 1;
+            V cq;
+            cq.x = R(neg ? -ht.cb_re : ht.cb_re);
+            cq.y = R(neg ? -ht.cb_im : ht.cb_im);
+            tcoef[q] = cq;
+        }
+        __syncthreads();
+        R ar[NR], ai[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) ar[r] = ai[r] = 0;
+        ham_classes<R, NRB>(
+            ket, [&](int r, uint32_t f) { return (lt | lr[r]) ^ f; }, cls, sflip, a.n_classes, a.term_begin, tmask,
+            tcoef, hi_shift, ar, ai);
+        double fr = 0, fi = 0;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const uint32_t L = uint32_t(tid + T * r);
+            const uint64_t gL = base + tab[L >> c] + (L & lowmask);
+            if (a.fout) {
+                const V bv = bra_is_ket ? ket[lt | lr[r]] : a.bra[b * dim + gL];
+                fr += double(bv.x) * double(ar[r]) + double(bv.y) * double(ai[r]);
+                fi += double(bv.x) * double(ai[r]) - double(bv.y) * double(ar[r]);
+            }
+            if (a.out) {
+                V v;
+                v.x = ar[r];
+                v.y = ai[r];
+                if (a.accumulate) {
+                    const V old = staged ? prev[lt | lr[r]] : a.out[b * a.out_batch_stride + gL];
+                    v.x += old.x;
+                    v.y += old.y;
+                }
+                a.out[b * a.out_batch_stride + gL] = v;
+            }
+        }
+        if (a.fout) {
+            fr = warp_sum(fr);
+            fi = warp_sum(fi);
+            if (lane == 0) {
+                wf[warp * 2] += fr;
+                wf[warp * 2 + 1] += fi;
+            }
+        }
+        const int64_t nxt = w + step;
+        const bool flush = (nxt >= total) || ((nxt >> g.n_out) != b);
+        __syncthreads();   // the block is done with buffer buf
+        if (tid == 0 && i + NB < count) issue(i + NB);
+        if (flush && a.fout) {
+            if (tid < 2) {
+                double s2 = 0;
+                for (int ww = 0; ww < nw; ++ww) {
+                    s2 += wf[ww * 2 + tid];
+                    wf[ww * 2 + tid] = 0;
+                }
+                atomicAdd(&a.fout[b * a.f_stride + tid], s2);
+            }
+            __syncthreads();
+        }
+    }
+    if (failed && tid == 0) {
+        pipe::report(rg.err, MQB_DEV_ERR_TIMEOUT);
+        // copies already started still write into this block's shared memory: let them land
+        for (int64_t j = i; j < count && j < i + NB; ++j) pipe::mbar_wait(&full[j % NB], unsigned(j / NB) & 1u);
+    }
+}
+
 static size_t align_up16(size_t x) { return (x + 15) & ~size_t(15); }
+
+size_t ham_ring_smem(const TileGeom &g, int elem_bytes, int threads, int n_classes, int n_terms, bool staged, int nb) {
+    size_t s = 128 + size_t(staged ? 2 : 1) * nb * ((size_t(1) << g.K) * elem_bytes);   // 128: base alignment
+    s = align_up16(s + size_t(nb) * sizeof(uint64_t));
+    s = align_up16(s + (size_t(1) << (g.K - g.c)) * sizeof(uint64_t));
+    s = align_up16(s + size_t(threads / 32) * 2 * sizeof(double));
+    s = align_up16(s + size_t(n_classes) * sizeof(HamClass));
+    s = align_up16(s + size_t(n_terms) * elem_bytes);
+    s = align_up16(s + size_t(n_terms) * sizeof(uint32_t));
+    return s + size_t(n_classes) * sizeof(uint32_t);
+}
+
+template <typename R>
+cudaError_t launch_ham_ring(const HamArgs<R> &a, const HamRingGeom &rg, const void *map_ket, const void *map_prev,
+                            int sm_count, cudaStream_t s) {
+    const int threads = 1 << (a.g.K - kHamRegBits);
+    const size_t smem = ham_ring_smem(a.g, int(sizeof(cplx<R>)), threads, a.n_classes, a.n_terms,
+                                      a.accumulate && a.out && rg.stage_prev, rg.nb);
+    auto kern = ham_ring_kernel<R, kHamRegBits>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int64_t work = a.batch << a.g.n_out;
+    const int blocks = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(sm_count) * per_sm, work)));
+    pipe::TMap mk, mo;
+    std::memcpy(&mk, map_ket, sizeof(mk));
+    std::memcpy(&mo, map_prev, sizeof(mo));
+    kern<<<blocks, threads, smem, s>>>(a, rg, mk, mo);
+    return cudaGetLastError();
+}
 
 static size_t ham2_smem(const TileGeom &g, int elem_bytes, int threads, int n_classes, int n_terms, bool staged_out) {
     size_t s = align_up16((size_t(1) << g.K) * elem_bytes);
@@ -611,8 +854,9 @@ static size_t ham2_smem(const TileGeom &g, int elem_bytes, int threads, int n_cl
     s = align_up16(s + size_t(threads / 32) * 2 * sizeof(double));
     s = align_up16(s + size_t(n_classes) * sizeof(HamClass));
     s = align_up16(s + size_t(n_terms) * elem_bytes);
-    s += size_t(n_terms) * sizeof(uint32_t);
-    if (staged_out) s = align_up16(s) + (size_t(1) << g.K) * elem_bytes;   // the previous groups' sum
+    s = align_up16(s + size_t(n_terms) * sizeof(uint32_t));
+    s = align_up16(s + size_t(n_classes) * sizeof(uint32_t));
+    if (staged_out) s += (size_t(1) << g.K) * elem_bytes;   // the previous groups' sum
     return s;
 }
 
@@ -1355,6 +1599,8 @@ cudaError_t launch_collapse(cplx<R> *st, int n, int q, int outcome, double scale
 #define MQB_INSTANTIATE(R)                                                                                         \
     template cudaError_t launch_matgen<R>(const MatgenArgs &, cudaStream_t);                                       \
     template cudaError_t launch_ham<R>(const HamArgs<R> &, int, cudaStream_t);                                     \
+    template cudaError_t launch_ham_ring<R>(const HamArgs<R> &, const HamRingGeom &, const void *, const void *,   \
+                                            int, cudaStream_t);                                                    \
     template cudaError_t launch_plain_apply<R>(cplx<R> *, int, int64_t, const DevOp &, const cplx<R> *, int64_t,   \
                                                const cplx<R> *, bool, int, cudaStream_t);                          \
     template cudaError_t launch_plain_grad<R>(const cplx<R> *, const cplx<R> *, int, int64_t, int, const DevOp &,  \

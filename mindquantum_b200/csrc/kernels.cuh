@@ -100,6 +100,22 @@ template <typename R>
 cudaError_t launch_fused_bwd2(const Bwd2Args<R> &a, int sm_count, cudaStream_t s);
 template <typename R>
 cudaError_t launch_ham(const HamArgs<R> &a, int sm_count, cudaStream_t s);
+// The tile movement of the TMA-ring Hamiltonian pass: how the copies cut a group's tile
+// (tensor-map geometry), where tile bit j lands in shared memory, the buffers per operand and the
+// error word a bounded wait reports to.
+struct HamRingGeom {
+    TmaGeom tg;
+    int8_t land[kMaxTileBits];
+    int nb;
+    int stage_prev;   // a group that adds to the output stages the previous sum by TMA too (else reads it)
+    int *err;
+};
+size_t ham_ring_smem(const TileGeom &g, int elem_bytes, int threads, int n_classes, int n_terms, bool staged, int nb);
+// map_ket / map_prev: CUtensorMap (128 bytes) of a.ket and of a.out ([batch][2^n] each, the same
+// tile geometry); map_prev is used only when the group adds to the output and stages it.
+template <typename R>
+cudaError_t launch_ham_ring(const HamArgs<R> &a, const HamRingGeom &rg, const void *map_ket, const void *map_prev,
+                            int sm_count, cudaStream_t s);
 template <typename R>
 cudaError_t launch_plain_apply(cplx<R> *st, int n, int64_t batch, const DevOp &op, const cplx<R> *mats,
                                int64_t mats_stride, const cplx<R> *cpool, bool adjoint, int sm_count, cudaStream_t s);
