@@ -223,7 +223,7 @@ def reference_full_evaluations(n, layers, batch, threads, count):
 def run_reference(args, rank):
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
+    threads = args.threads or os.cpu_count() or 1
     # a bounded run: at most three full evaluations (each tens of seconds on the host), plus
     # warm-up evaluations of one layer
     from oracle import refbin as R
@@ -649,6 +649,8 @@ def main():
     ap.add_argument('--layers', type=int, default=12)
     ap.add_argument('--batch', type=int, default=8)
     ap.add_argument('--skip-extras', action='store_true')
+    ap.add_argument('--threads', type=int, default=0,
+                    help='host threads of the reference arm (default: every core)')
     ap.add_argument('--skip-plain', action='store_true')
     ap.add_argument('--skip-cpu', action='store_true')
     ap.add_argument('--workload', default='hea', choices=['hea', 'qnn', 'qaoa', 'uneven', 'csr', 'pshift', 'noise'],
