@@ -287,9 +287,10 @@ static TileGeom pass_geom(int n, const Pass &ps) {
 
 // ---------------------------------------------------------------------------------------------- execution
 template <typename R>
-static void run_forward_pass(const mqb_program &p, const SchedDev &sd, size_t pi, const void *jk,
+static bool run_forward_pass(const mqb_program &p, const SchedDev &sd, size_t pi, const void *jk,
                              const cplx<R> *mats, const cplx<R> *src, int64_t src_stride, cplx<R> *dst, int64_t batch,
-                             cudaStream_t st) {
+                             cudaStream_t st, double *norm = nullptr) {
+    // returns whether the pass also added <psi|psi> of its output to norm[b][0] (generated passes)
     const Schedule &s = sd.s;
     const Pass &ps = s.passes[pi];
     const int sm = sm_count_cached();
@@ -307,9 +308,10 @@ static void run_forward_pass(const mqb_program &p, const SchedDev &sd, size_t pi
         a.dst = dst;
         a.batch = batch;
         a.src_batch_stride = src_stride;
+        a.norm = norm;
         TimeScope ts(TK_FWD, st);
         ck(jit_launch_forward<cplx<R>>(jk, a, ps, p.precision, sm, st), "generated forward pass");
-        return;
+        return norm != nullptr;
     }
     if (ps.fused) {
         Fwd2Args<R> a{};
@@ -329,7 +331,7 @@ static void run_forward_pass(const mqb_program &p, const SchedDev &sd, size_t pi
         a.src_batch_stride = src_stride;
         TimeScope ts(TK_FWD, st);
         ck(launch_fused_fwd2<R>(a, sm, st), "fused forward pass");
-        return;
+        return false;
     }
     if (src != dst) {
         TimeScope ts(TK_OTHER, st);
@@ -338,6 +340,7 @@ static void run_forward_pass(const mqb_program &p, const SchedDev &sd, size_t pi
     TimeScope ts(TK_PLAIN_APPLY, st);
     ck(launch_plain_apply<R>(dst, p.n, batch, p.ops[ps.op_begin], mats, p.per_sample, cpool, false, sm, st),
        "gate kernel");
+    return false;
 }
 
 template <typename R>
@@ -560,11 +563,14 @@ static void grad_impl(mqb_program &p, const mqb_hamiltonian *const *hams, int n_
     for (int q = 0; q < P; ++q) {
         const V *src = (q == 0) ? init_v : loc(q);
         const int64_t sstr = (q == 0) ? init_stride : dim;
-        run_forward_pass<R>(p, sd, q, jf ? (*jf)[q] : nullptr, mats, src, sstr, loc(q + 1), batch, st);
-        if (next_fwd < L.norm_fwd.size() && L.norm_fwd[next_fwd] == q + 1) {
+        const bool check = next_fwd < L.norm_fwd.size() && L.norm_fwd[next_fwd] == q + 1;
+        // a generated pass adds the norm of its output itself; other passes get a separate reduction
+        if (run_forward_pass<R>(p, sd, q, jf ? (*jf)[q] : nullptr, mats, src, sstr, loc(q + 1), batch, st,
+                                check ? norms + 2 * batch * n_checked : nullptr))
+            ++n_checked;
+        else if (check)
             norm_check(loc(q + 1));
-            ++next_fwd;
-        }
+        if (check) ++next_fwd;
     }
     V *psiP = W;
     if (P > 0) {

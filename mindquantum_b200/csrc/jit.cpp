@@ -953,6 +953,10 @@ std::string forward_source(const Schedule &s, const Pass &p, int precision) {
                 ++k;
             }
         }
+        if (last)   // the FP64 norm check of the output, when the launch asks for it
+            o << "    if (a.norm) {\n     double ns = 0;\n"
+              << "     for (int j = 0; j < NR; ++j) ns += double(v[j].x) * double(v[j].x) + double(v[j].y) * double(v[j].y);\n"
+              << "     ns = warp_sum(ns);\n     if ((threadIdx.x & 31u) == 0u) atomicAdd(a.norm + 2 * b, ns);\n    }\n";
         emit_stage_store(o, pl, sd, RB, TB, 0, lp.in[si], lp.out[si], !last || lp.relayout_out);
     }
     if (lp.relayout_out) {

@@ -57,6 +57,7 @@ struct JitFwdArgs {
     long long src_batch_stride;
     TmaGeom tg;
     int *err;               // error word (MQB_DEV_ERR_*), set once
+    double *norm;           // nullptr, or [batch][2]: += <psi|psi> of the pass's output in FP64 (re)
 };
 
 template <typename V>
