@@ -198,8 +198,18 @@ void emit_backward_op(std::ostringstream &o, const StageOp &so, int NH, int gid)
     const bool gen_ry = G == 1 && gid == GID_RY && so.kind == SK_REAL1;
     const bool gen_rx = G == 1 && gid == GID_RX && so.kind == SK_RXL1;
     const bool gen_diag = !pw.empty() && (so.kind == SK_DIAG1 || so.kind == SK_DIAG2);
+    const bool gen_u3 = G != 0 && gid == GID_U3 && so.kind == SK_DENSE1;
     auto wsel = [&](const std::string &w) { return cond ? "(on ? " + w + " : R(0))" : w; };
-    if (gen_ry) {
+    if (gen_u3) {
+        // e^{i lam} comes from the theta derivative, which is in the table only when theta has a gradient
+        o << "      const V el = " << ((G & 1) ? "u3_phase(" + mt(M) + ", " + mt(M + 1) + ", " + dm(0, 0) + ", " + dm(0, 1) + ")"
+                                           : std::string("cval<V>(1, 0)"))
+          << ";\n";
+        o << "      jbg_u3<V, RB, NH, " << so.p0 << ", " << CM << ", " << G << ">(v, l, "
+          << sel("cconj(" + mt(M) + ")", one) << ", " << sel("cconj(" + mt(M + 2) + ")", zero) << ", "
+          << sel("cconj(" + mt(M + 1) + ")", zero) << ", " << sel("cconj(" + mt(M + 3) + ")", one) << ", el, "
+          << wsel("R(1)") << ", acc);\n";
+    } else if (gen_ry) {
         o << "      jbg_ry<V, RB, NH, " << so.p0 << ", " << CM << ">(v, l, " << sel(mt(M) + ".x", "R(1)") << ", "
           << sel(mt(M + 2) + ".x", "R(0)") << ", " << sel(mt(M + 1) + ".x", "R(0)") << ", "
           << sel(mt(M + 3) + ".x", "R(1)") << ", " << wsel("R(0.5)") << ", acc);\n";

@@ -428,6 +428,70 @@ __device__ __forceinline__ void jbg_ry(V (&v)[1 << RB], V (&l)[NH][1 << RB], R a
     for (int h = 0; h < NH; ++h) acc[0][h] += gs * (ra_sum(gp[h]) - ra_sum(gm[h]));
 }
 
+// U3(theta, phi, lam) = P(phi) RY'(theta) P(lam), P(x) = diag(1, e^{ix}), with its three gradients
+// in generator form (z = U^dag l is lambda on the gate's input side, w = U^dag v psi there):
+//   d/dphi = diag(0, i) U:  Re<l|diag(0,i)|v> = -Im(conj(l1) v1)
+//   d/dlam = U diag(0, i):  Re<z|diag(0,i)|w> = -Im(conj(z1) w1)
+//   d/dtheta = U G, G = [[0, -e^{i lam}], [e^{-i lam}, 0]] / 2:
+//                            Re(-e^{i lam} A + e^{-i lam} B) / 2, A = sum conj(z0) w1, B = sum conj(z1) w0
+// 12 FMAs per pair for all three instead of a derivative matrix applied per angle; `el` = e^{i lam},
+// gw = 1 (0 for a thread whose controls are off).
+template <typename V, int RB, int NH, int P, unsigned CM, int G, typename R>
+__device__ __forceinline__ void jbg_u3(V (&v)[1 << RB], V (&l)[NH][1 << RB], V a00, V a01, V a10, V a11, V el, R gw,
+                                       R (&acc)[3][NH]) {
+    R gphi[NH], glam[NH], ar[NH], ai[NH], br[NH], bi[NH];
+#pragma unroll
+    for (int h = 0; h < NH; ++h) gphi[h] = glam[h] = ar[h] = ai[h] = br[h] = bi[h] = 0;
+#pragma unroll
+    for (int j = 0; j < (1 << RB); ++j) {
+        if (!pair_on<P, CM>(j)) continue;
+        constexpr int bit = 1 << P;
+        const V x0 = v[j], x1 = v[j | bit];
+        const V w0 = cmadd(a00, x0, cmul(a01, x1)), w1 = cmadd(a10, x0, cmul(a11, x1));
+        v[j] = w0;
+        v[j | bit] = w1;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+            const V l0 = l[h][j], l1 = l[h][j | bit];
+            if (G & 2) gphi[h] = im_acc(l1, x1, gphi[h]);
+            const V z0 = cmadd(a00, l0, cmul(a01, l1)), z1 = cmadd(a10, l0, cmul(a11, l1));
+            if (G & 4) glam[h] = im_acc(z1, w1, glam[h]);
+            if (G & 1) {
+                ar[h] = re_acc(z0, w1, ar[h]);
+                ai[h] = im_acc(z0, w1, ai[h]);
+                br[h] = re_acc(z1, w0, br[h]);
+                bi[h] = im_acc(z1, w0, bi[h]);
+            }
+            l[h][j] = z0;
+            l[h][j | bit] = z1;
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < NH; ++h) {
+        // Re(-el A + conj(el) B) / 2
+        if (G & 1) acc[0][h] += gw * R(0.5) * (-(el.x * ar[h] - el.y * ai[h]) + (el.x * br[h] + el.y * bi[h]));
+        if (G & 2) acc[1][h] -= gw * gphi[h];
+        if (G & 4) acc[2][h] -= gw * glam[h];
+    }
+}
+
+// e^{i lam} of a U3 from its matrix m (row-major) and its theta derivative d: -m01 / s with
+// s = sin(theta/2) = -2 Re d00 when |s| >= |c|, else -2 d01 / c with c = cos(theta/2) = Re m00.
+template <typename V>
+__device__ __forceinline__ V u3_phase(V m00, V m01, V d00, V d01) {
+    typedef decltype(V::x) R;
+    const R s = R(-2) * d00.x, c = m00.x;
+    V e;
+    if (fabs(s) >= fabs(c)) {
+        e.x = -m01.x / s;
+        e.y = -m01.y / s;
+    } else {
+        e.x = R(-2) * d01.x / c;
+        e.y = R(-2) * d01.y / c;
+    }
+    return e;
+}
+
 // RX-like: G = X, Re<l| -i/2 X |x> = (Im(conj(l0) x1) + Im(conj(l1) x0)) / 2; U^dag = [[a, i nb], [i nb, a]]
 template <typename V, int RB, int NH, int P, unsigned CM, typename R>
 __device__ __forceinline__ void jbg_rx(V (&v)[1 << RB], V (&l)[NH][1 << RB], R a, R nb, R gs, R (&acc)[3][NH]) {
