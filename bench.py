@@ -538,7 +538,7 @@ def run_workload(args, rank, local_rank):
         names = circ.params_name
         prd = dict(zip(names, params_np[0].tolist()))
         sim_api = Simulator('mqvector_b200', n, dtype=complex64, seed=7)
-        shots = 256
+        shots = 1024
         units = shots
         seeds = iter(range(1, 1 << 30))
 

@@ -379,8 +379,8 @@ static void apply_impl(mqb_program &p, void *states, int64_t batch, const double
 
 // Hamiltonian passes: out = H ket (if out), f += <bra|H ket> (if fout)
 // Whether a Hamiltonian group runs as the TMA-ring pass (MQB_HAM_RING=0 keeps the synchronous
-// one): 2^(K-4) threads of at least one warp and at most 256, 16-byte-aligned buffers, and three
-// buffers per operand in shared memory (two when the previous sum is staged too).  Sets rg.nb.
+// one): 2^(K-4) threads of at least one warp and at most 256, 16-byte-aligned buffers, and at
+// least two buffers per operand in shared memory.  Sets rg.nb.
 template <typename R>
 static bool ham_ring_fits(const HamArgs<R> &a, HamRingGeom &rg) {
     static const bool on = [] {
@@ -396,9 +396,12 @@ static bool ham_ring_fits(const HamArgs<R> &a, HamRingGeom &rg) {
     if ((reinterpret_cast<uintptr_t>(a.ket) & 15) || (reinterpret_cast<uintptr_t>(a.out) & 15)) return false;
     rg.stage_prev = stage;
     const bool staged = a.accumulate && a.out && stage;
-    static const int nb_max = [] {   // MQB_HAM_RING_BUFFERS: buffers per operand (2..4, tuning)
+    // MQB_HAM_RING_BUFFERS: buffers per operand (2..4, tuning).  Two by default: the 26-qubit
+    // ZZ + X pass took 22.0 ms with two, 22.7 with three (an unstaged group then fits three blocks
+    // per SM instead of two)
+    static const int nb_max = [] {
         const char *e = std::getenv("MQB_HAM_RING_BUFFERS");
-        return e ? std::max(2, std::min(4, std::atoi(e))) : 3;
+        return e ? std::max(2, std::min(4, std::atoi(e))) : 2;
     }();
     for (int nb = nb_max; nb >= 2; --nb) {
         if (ham_ring_smem(a.g, int(sizeof(cplx<R>)), threads, a.n_classes, a.n_terms, staged, nb) <= 220 * 1024) {
