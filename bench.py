@@ -220,8 +220,59 @@ def reference_full_evaluations(n, layers, batch, threads, count):
     return times, kind
 
 
+def run_reference_gpu(args):
+    """The reference's own thrust GPU simulator (`mqvector_gpu`, built from its sources for sm_100a
+    into oracle/_ref/libmqref_gpu.so) on this GPU: full gradient evaluations of parameter set 0, one
+    at a time as the reference runs them, complex64 (the line's value) and complex128 (the plain
+    per-gate path of the reference).  Its API is synchronous and returns host values, so each
+    evaluation is timed on the host clock between device synchronizations."""
+    import torch
+
+    from oracle import refbin as R
+
+    if not R.available('gpu'):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference GPU simulator was not built "
+                                                              "(make -C oracle refgpu, with the reference checkout)"}))
+        return
+    circ, ham, params = build_workload(args.qubits, args.layers, args.batch)
+    c1, h1, p1 = build_workload(args.qubits, 1, args.batch)
+    count = max(1, min(args.steps, 3))
+    out = {}
+    for prec, c64 in (("c64", True), ("c128", False)):
+        for _ in range(args.warmup):
+            R.grad(args.qubits, c1, h1, p1[:1], complex64=c64, device='gpu')
+        times = []
+        for _ in range(count):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            R.grad(args.qubits, circ, ham, params[:1], complex64=c64, device='gpu')
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        out[prec] = times
+    t = float(np.mean(out["c64"]))
+    value = 1.0 / t
+    sample = (f"full gradient evaluations (all {args.layers} layers, lambda = H psi) of parameter set 0, "
+              f"{args.qubits} qubits, {count} timed per precision after {args.warmup} one-layer warm-ups")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": count, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic",
+        "config": {"workload": f"HEA {args.qubits}q x {args.layers} layers, {2 * args.qubits * args.layers} params, "
+                               f"{2 * args.qubits - 1}-term H, per-sample grad",
+                   "n_qubits": args.qubits, "layers": args.layers, "batch": 1, "parallelism": "gpu x1"},
+        "impl": "reference", "ref_device": "gpu: the reference's thrust mqvector_gpu built for sm_100a",
+        "sample": sample, "seconds": out,
+        "c128": {"value": 1.0 / float(np.mean(out["c128"])), "unit": UNIT},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank):
     if rank != 0:
+        return
+    if args.ref_device == 'gpu':
+        run_reference_gpu(args)
         return
     threads = args.threads or os.cpu_count() or 1
     # a bounded run: at most three full evaluations (each tens of seconds on the host), plus
@@ -651,6 +702,8 @@ def main():
     ap.add_argument('--skip-extras', action='store_true')
     ap.add_argument('--threads', type=int, default=0,
                     help='host threads of the reference arm (default: every core)')
+    ap.add_argument('--ref-device', default='cpu', choices=['cpu', 'gpu'],
+                    help="reference arm: the reference's CPU simulator (default) or its thrust GPU simulator")
     ap.add_argument('--skip-plain', action='store_true')
     ap.add_argument('--skip-cpu', action='store_true')
     ap.add_argument('--workload', default='hea', choices=['hea', 'qnn', 'qaoa', 'uneven', 'csr', 'pshift', 'noise'],

@@ -3,179 +3,32 @@
 // Built by oracle/Makefile (target _ref/libmqref.so) together with the reference's C++ sources,
 // compiled in place from the reference tree: VectorState<CPUVectorPolicyAvxDouble> and its CPU
 // policy (ccsrc/include/simulator/vector/vector_state.h/.tpp, ccsrc/lib/simulator/vector/detail/
-// cpu_common, cpu_avx_double), the gates and parameter resolvers it uses.  This file only builds
-// circuits and Hamiltonians with the reference's classes and calls its entry points:
+// cpu_common, cpu_avx_double), the gates and parameter resolvers it uses.  The circuits and
+// Hamiltonians are built by ref_harness_common.h with the reference's classes:
 //
 //   mqref_apply: VectorState::ApplyCircuit + GetQS (vector_state.tpp:949-960);
 //   mqref_grad:  VectorState::GetExpectationWithGradMultiMulti (the adjoint gradient,
-//                ccsrc/include/simulator/vector/gradient.h:100-197), with the Hermitian circuit
-//                built the way the reference's Python builds it (mindquantum/core/circuit/
-//                circuit.py hermitian(): the daggers in reverse order, parameter expressions
-//                negated).
+//                ccsrc/include/simulator/vector/gradient.h:100-197).
 //
 // Only tests/ and bench.py's CPU legs load it, to pin the oracle to the reference itself and to
 // time the reference on the host; the product never does.
-#include <omp.h>
-
-#include <complex>
-#include <cstring>
-#include <map>
-#include <memory>
-#include <string>
-#include <vector>
-
-#include "ops/basic_gate.h"
-#include "ops/hamiltonian.h"
+#include "ref_harness_common.h"
 #include "simulator/vector/detail/cpu_vector_avx_double_policy.h"
 #include "simulator/vector/detail/cpu_vector_avx_float_policy.h"
-#include "simulator/vector/vector_state.h"
 
 namespace {
-
-using mindquantum::Index;
-using mindquantum::qbits_t;
-using parameter::ParameterResolver;
 using sim_d = mindquantum::sim::vector::detail::VectorState<mindquantum::sim::vector::detail::CPUVectorPolicyAvxDouble>;
 using sim_f = mindquantum::sim::vector::detail::VectorState<mindquantum::sim::vector::detail::CPUVectorPolicyAvxFloat>;
-using circuit_t = std::vector<std::shared_ptr<mindquantum::BasicGate>>;
-
-// Gate kinds of the harness's gate table.
-enum Kind { K_X = 0, K_H = 1, K_RX = 2, K_RY = 3, K_RZ = 4, K_Z = 5, K_RZZ = 6, K_Y = 7, K_PS = 8 };
-
-ParameterResolver angle(int param, double coeff, double cst, const std::vector<std::string> &names, double sign) {
-    if (param < 0) return ParameterResolver(sign * cst);
-    return ParameterResolver(sign * cst, std::map<std::string, double>{{names[param], sign * coeff}});
-}
-
-// The circuit of the table, or its Hermitian conjugate (reversed, parameter expressions negated).
-circuit_t build(int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl, const int *param,
-                const double *coeff, const double *cst, const std::vector<std::string> &names, bool herm) {
-    circuit_t c;
-    for (int i = 0; i < n_gates; ++i) {
-        const int k = herm ? n_gates - 1 - i : i;
-        const double sign = herm ? -1.0 : 1.0;
-        const qbits_t ctrls = ctrl[k] >= 0 ? qbits_t{Index(ctrl[k])} : qbits_t{};
-        const qbits_t obj1q = obj1[k] >= 0 ? qbits_t{Index(obj0[k]), Index(obj1[k])} : qbits_t{Index(obj0[k])};
-        switch (kind[k]) {
-            case K_X: c.push_back(std::make_shared<mindquantum::XGate>(obj1q, ctrls)); break;
-            case K_Y: c.push_back(std::make_shared<mindquantum::YGate>(obj1q, ctrls)); break;
-            case K_Z: c.push_back(std::make_shared<mindquantum::ZGate>(obj1q, ctrls)); break;
-            case K_H: c.push_back(std::make_shared<mindquantum::HGate>(obj1q, ctrls)); break;
-            case K_RX:
-                c.push_back(std::make_shared<mindquantum::RXGate>(angle(param[k], coeff[k], cst[k], names, sign), obj1q, ctrls));
-                break;
-            case K_RY:
-                c.push_back(std::make_shared<mindquantum::RYGate>(angle(param[k], coeff[k], cst[k], names, sign), obj1q, ctrls));
-                break;
-            case K_RZ:
-                c.push_back(std::make_shared<mindquantum::RZGate>(angle(param[k], coeff[k], cst[k], names, sign), obj1q, ctrls));
-                break;
-            case K_RZZ:
-                c.push_back(std::make_shared<mindquantum::RzzGate>(angle(param[k], coeff[k], cst[k], names, sign), obj1q, ctrls));
-                break;
-            case K_PS:
-                c.push_back(std::make_shared<mindquantum::PSGate>(angle(param[k], coeff[k], cst[k], names, sign), obj1q, ctrls));
-                break;
-            default:
-                return {};
-        }
-    }
-    return c;
-}
-
-std::vector<std::string> param_names(int n_params) {
-    std::vector<std::string> v;
-    for (int i = 0; i < n_params; ++i) v.push_back("p" + std::to_string(i));
-    return v;
-}
-
 }  // namespace
 
 extern "C" {
 
-// Apply the circuit to |0...0> with parameter values params[n_params]; out: 2^n complex128 (re, im).
-int mqref_apply(int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl, const int *param,
-                const double *coeff, const double *cst, int n_params, const double *params, int threads, double *out) {
-    try {
-        if (threads > 0) omp_set_num_threads(threads);
-        const auto names = param_names(n_params);
-        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false);
-        if (int(c.size()) != n_gates) return -1;
-        ParameterResolver pr;
-        for (int i = 0; i < n_params; ++i) pr.SetItem(names[i], params[i]);
-        sim_d sim{static_cast<Index>(n)};
-        sim.ApplyCircuit(c, pr);
-        const auto qs = sim.GetQS();
-        for (size_t i = 0; i < qs.size(); ++i) {
-            out[2 * i] = qs[i].real();
-            out[2 * i + 1] = qs[i].imag();
-        }
-        return 0;
-    } catch (...) {
-        return -2;
-    }
-}
+int mqref_apply(MQREF_APPLY_ARGS) { return mqref::apply_impl<sim_d>(MQREF_APPLY_PASS); }
 
-// <H> and its gradient for n_samples parameter rows (all parameters treated as encoder inputs, as
-// get_expectation_with_grad does for an encoder circuit).  Hamiltonian: n_terms Pauli strings,
-// term t has term_len[t] (qubit, 'X'|'Y'|'Z') pairs from term_q / term_p and coefficient term_c[t].
-// out: [n_samples][1 + n_params] complex128 (re, im): f, then the gradient.
-#define MQREF_GRAD_ARGS                                                                                             \
-    int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl, const int *param,      \
-        const double *coeff, const double *cst, int n_terms, const int *term_len, const int *term_q,               \
-        const char *term_p, const double *term_c, int n_params, int n_samples, const double *params, int threads, \
-        double *out
-int mqref_grad(MQREF_GRAD_ARGS);      // complex128 (CPUVectorPolicyAvxDouble)
-int mqref_grad_c64(MQREF_GRAD_ARGS);  // complex64 (CPUVectorPolicyAvxFloat)
+// complex128 (CPUVectorPolicyAvxDouble)
+int mqref_grad(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_d, double>(MQREF_GRAD_PASS); }
 
-}  // extern "C"
-
-namespace {
-
-template <typename sim_t, typename calc_t>
-int grad_impl(MQREF_GRAD_ARGS) {
-    try {
-        if (threads > 0) omp_set_num_threads(threads);
-        const auto names = param_names(n_params);
-        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false);
-        const circuit_t h = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, true);
-        if (int(c.size()) != n_gates || int(h.size()) != n_gates) return -1;
-        std::vector<mindquantum::PauliTerm<calc_t>> terms;
-        for (int t = 0, o = 0; t < n_terms; ++t) {
-            std::vector<mindquantum::PauliWord> w;
-            for (int k = 0; k < term_len[t]; ++k, ++o) w.emplace_back(Index(term_q[o]), term_p[o]);
-            terms.emplace_back(w, calc_t(term_c[t]));
-        }
-        std::vector<std::shared_ptr<mindquantum::Hamiltonian<calc_t>>> hams{
-            std::make_shared<mindquantum::Hamiltonian<calc_t>>(terms)};
-        std::vector<std::vector<calc_t>> enc(n_samples, std::vector<calc_t>(n_params));
-        for (int s = 0; s < n_samples; ++s)
-            for (int i = 0; i < n_params; ++i) enc[s][i] = calc_t(params[s * n_params + i]);
-        sim_t sim{static_cast<Index>(n)};
-        const auto res = sim.GetExpectationWithGradMultiMulti(hams, c, h, enc, {}, names, {}, 1, 1);
-        for (int s = 0; s < n_samples; ++s)
-            for (int i = 0; i <= n_params; ++i) {
-                out[2 * (s * (n_params + 1) + i)] = double(res[s][0][i].real());
-                out[2 * (s * (n_params + 1) + i) + 1] = double(res[s][0][i].imag());
-            }
-        return 0;
-    } catch (...) {
-        return -2;
-    }
-}
-
-}  // namespace
-
-extern "C" {
-
-int mqref_grad(MQREF_GRAD_ARGS) {
-    return grad_impl<sim_d, double>(n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, n_terms, term_len, term_q,
-                                    term_p, term_c, n_params, n_samples, params, threads, out);
-}
-
-int mqref_grad_c64(MQREF_GRAD_ARGS) {
-    return grad_impl<sim_f, float>(n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, n_terms, term_len, term_q,
-                                   term_p, term_c, n_params, n_samples, params, threads, out);
-}
+// complex64 (CPUVectorPolicyAvxFloat)
+int mqref_grad_c64(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_f, float>(MQREF_GRAD_PASS); }
 
 }  // extern "C"

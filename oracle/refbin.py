@@ -1,6 +1,8 @@
-"""The reference's own CPU simulator (built from its sources by oracle/Makefile into
-oracle/_ref/libmqref.so).  TEST INFRASTRUCTURE ONLY: tests/ use it to pin the oracle (and the CUDA
-path) to the reference itself, and bench.py times it as the CPU baseline; the product never does.
+"""The reference's own simulators, built from its sources by oracle/Makefile: the CPU simulator
+(oracle/_ref/libmqref.so) and its thrust GPU simulator `mqvector_gpu` built for sm_100a
+(oracle/_ref/libmqref_gpu.so).  TEST INFRASTRUCTURE ONLY: tests/ use them to pin the oracle (and
+the CUDA path) to the reference itself, and bench.py's reference arm times them; the product never
+does.
 
 Supported gates: X, Y, Z, H (at most one control), RX, RY, RZ, Rzz and PhaseShift whose angle is
 ``coeff * p + const`` of at most one parameter.  Hamiltonians: Pauli strings with real coefficients.
@@ -12,27 +14,32 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref.so')
+GPU_LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref_gpu.so')
 _KINDS = {'X': 0, 'H': 1, 'RX': 2, 'RY': 3, 'RZ': 4, 'Z': 5, 'Rzz': 6, 'Y': 7, 'PS': 8}
-_lib = None
+_libs = {}
 
 
-def available():
-    return os.path.exists(LIB_PATH)
+def available(device='cpu'):
+    return os.path.exists(GPU_LIB_PATH if device == 'gpu' else LIB_PATH)
 
 
-def lib():
-    global _lib  # pylint: disable=global-statement
-    if _lib is None:
-        if not available():
-            raise FileNotFoundError(f"{LIB_PATH} is not built (make -C oracle ref, with the reference checkout)")
-        L = ctypes.CDLL(LIB_PATH)
+def lib(device='cpu'):
+    """The CPU (``device='cpu'``) or thrust GPU (``device='gpu'``) build; entry points are named
+    mqref_* and mqref_gpu_* respectively and take the same arguments."""
+    if device not in _libs:
+        path, target = (GPU_LIB_PATH, 'refgpu') if device == 'gpu' else (LIB_PATH, 'ref')
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (make -C oracle {target}, with the reference checkout)")
+        L = ctypes.CDLL(path)
         P = ctypes.c_void_p
-        L.mqref_apply.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, ctypes.c_int, P]
-        for fn in (L.mqref_grad, L.mqref_grad_c64):
+        pre = 'mqref_gpu_' if device == 'gpu' else 'mqref_'
+        getattr(L, pre + 'apply').argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, ctypes.c_int,
+                                                                                      P]
+        for fn in (getattr(L, pre + 'grad'), getattr(L, pre + 'grad_c64')):
             fn.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, P, P, P, ctypes.c_int,
                                                                     ctypes.c_int, P, ctypes.c_int, P]
-        _lib = L
-    return _lib
+        _libs[device] = (L, pre)
+    return _libs[device]
 
 
 def _gate_table(circ, names):
@@ -67,22 +74,25 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
-def apply(n, circ, params, threads=0):
-    """VectorState::ApplyCircuit from |0...0> with parameter values ``params`` (circ.params_name order)."""
+def apply(n, circ, params, threads=0, device='cpu'):
+    """VectorState::ApplyCircuit from |0...0> with parameter values ``params`` (circ.params_name order),
+    complex128, on the reference's CPU or thrust GPU policy."""
     names = list(circ.params_name)
     ints, dbls = _gate_table(circ, names)
     out = np.zeros(2 << n, dtype=np.float64)
     p = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
-    st = lib().mqref_apply(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
+    L, pre = lib(device)
+    st = getattr(L, pre + 'apply')(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
                            _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), len(names), _p(p), threads, _p(out))
     if st != 0:
         raise RuntimeError(f"mqref_apply failed ({st})")
     return out[0::2] + 1j * out[1::2]
 
 
-def grad(n, circ, ham, params, threads=0, complex64=False):
+def grad(n, circ, ham, params, threads=0, complex64=False, device='cpu'):
     """VectorState::GetExpectationWithGradMultiMulti for one Hamiltonian, every parameter an encoder
-    input: params [samples][n_params] -> [samples][1 + n_params] complex (f, then the gradient)."""
+    input: params [samples][n_params] -> [samples][1 + n_params] complex (f, then the gradient), on
+    the reference's CPU (``device='cpu'``) or thrust GPU (``device='gpu'``) policy."""
     names = list(circ.params_name)
     ints, dbls = _gate_table(circ, names)
     tl, tq, tp, tc = [], [], [], []
@@ -99,7 +109,8 @@ def grad(n, circ, ham, params, threads=0, complex64=False):
     params = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
     S = params.shape[0]
     out = np.zeros(S * (1 + len(names)) * 2, dtype=np.float64)
-    fn = lib().mqref_grad_c64 if complex64 else lib().mqref_grad
+    L, pre = lib(device)
+    fn = getattr(L, pre + ('grad_c64' if complex64 else 'grad'))
     st = fn(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']), _p(ints['param']),
             _p(dbls['coeff']), _p(dbls['cst']), len(tl), _p(tl), _p(tq), ctypes.cast(tpb, ctypes.c_void_p), _p(tc),
             len(names), S, _p(params), threads, _p(out))

@@ -6,6 +6,10 @@ restatement to it on the benchmark circuit families at full size where the host 
 seconds: config 1 exactly (16 qubits x 8 layers), the QNN encoder/ansatz, QAOA MaxCut and random
 Pauli Hamiltonians with Y terms.  Tolerance: 1e-12 (both FP64), complex64 reference within 1e-5.
 Skipped where the reference checkout was not available to build the library.
+
+The reference's thrust GPU simulator (`mqvector_gpu`, VectorState<GPUVectorPolicyDouble/Float>,
+built from its sources for sm_100a into oracle/_ref/libmqref_gpu.so) is pinned the same way on a
+B200 (marked gpu): FP64 within 1e-10 (its reductions run in another order), complex64 within 1e-5.
 """
 import numpy as np
 import pytest
@@ -54,3 +58,23 @@ def test_random_pauli_hamiltonians_oracle_equals_reference():
     circ, _, params = W.hea(n, 3, 2, seed=3, encoder=True)
     ham = W.random_pauli_hamiltonian(n, 25, rng)
     assert np.max(np.abs(R.grad(n, circ, ham, params) - _oracle(n, circ, ham, params))) <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not R.available('gpu'), reason="the reference GPU simulator is not built (oracle/_ref)")
+def test_reference_gpu_simulator_equals_oracle():
+    """Config 1 exactly (16 qubits x 8 layers, T = 31) and a random Pauli Hamiltonian with Y terms on
+    the reference's own thrust GPU simulator, against the oracle."""
+    n, layers = 16, 8
+    circ, ham, params = W.hea(n, layers, 1, seed=0, encoder=False)
+    orc = _oracle(n, circ, ham, params)
+    assert np.max(np.abs(R.grad(n, circ, ham, params, device='gpu') - orc)) <= 1e-10
+    assert np.max(np.abs(R.grad(n, circ, ham, params, complex64=True, device='gpu') - orc)) <= 1e-5
+    qs = R.apply(n, circ, params[0], device='gpu')
+    oqs = O.OracleSim(n).apply_circuit(circ, dict(zip(circ.params_name, params[0].tolist()))).qs
+    assert np.max(np.abs(qs - oqs)) <= 1e-12
+    n = 12
+    rng = np.random.default_rng(21)
+    circ, _, params = W.hea(n, 3, 2, seed=3, encoder=True)
+    ham = W.random_pauli_hamiltonian(n, 25, rng)
+    assert np.max(np.abs(R.grad(n, circ, ham, params, device='gpu') - _oracle(n, circ, ham, params))) <= 1e-10
