@@ -37,7 +37,7 @@ from .lowering import lowered, native_ham
 from .measure_result import MeasureResult
 from .mqvector_b200 import MQVectorB200, _ptr, _split_inputs, _stream
 from .rng import Mt19937Uniform
-from .utils import GradOpsWrapper
+from .utils import GradOpsWrapper, check_kept_qubits, qs_of_qubits
 
 _CHANNEL_NAMES = ('PC', 'BFC', 'PFC', 'BPFC', 'GPC', 'DC', 'ADC', 'PDC', 'TRC')
 # conj(exp(-i t/2 G)) = exp(-i (-t)/2 G) when the generator G is real, itself when G is imaginary
@@ -470,8 +470,13 @@ class MQMatrixB200(BackendBase):
         return t.reshape(d, d)
 
     def get_reduced_density_matrix(self, kept_qubits):
-        drop = [q for q in range(self.n_qubits) if q not in kept_qubits]
+        kept = check_kept_qubits(kept_qubits, self.n_qubits)
+        drop = [q for q in range(self.n_qubits) if q not in kept]
         return self.get_partial_trace(drop)
+
+    def get_qs_of_qubits(self, qubits, ket=False):
+        """Reduced state of ``qubits`` (mqsim.py:598-626)."""
+        return qs_of_qubits(self, qubits, ket)
 
     def entropy(self):
         ev = np.real(np.linalg.eigvals(self.get_qs()))

@@ -25,7 +25,7 @@ from .lowering import lowered, native_ham
 from .measure_result import MeasureResult
 from .parameter_shift import ShiftPlan
 from .rng import Mt19937Uniform, UniformBlocks, UniformStreams
-from .utils import GradOpsWrapper, _thread_balance
+from .utils import GradOpsWrapper, _thread_balance, check_kept_qubits, qs_of_qubits, reduced_density_matrix
 
 
 def _stream():
@@ -147,6 +147,17 @@ class MQVectorB200(BackendBase):
         if ket:
             return '\n'.join(f"{v}¦{format(i, f'0{self.n_qubits}b')}⟩" for i, v in enumerate(qs) if abs(v) > 1e-12)
         return qs
+
+    def get_reduced_density_matrix(self, kept_qubits):
+        """Density matrix of ``kept_qubits`` with the other qubits traced out (mqsim.py:559-570,
+        VectorState::GetReducedDensityMatrix): computed on the device from the state."""
+        kept = check_kept_qubits(kept_qubits, self.n_qubits)
+        return reduced_density_matrix(self.state.detach(), self.n_qubits, kept)
+
+    def get_qs_of_qubits(self, qubits, ket=False):
+        """Reduced state of ``qubits``: a vector when it is pure, else its density matrix
+        (mqsim.py:598-626)."""
+        return qs_of_qubits(self, qubits, ket)
 
     def set_qs(self, quantum_state):
         """Set the state; the vector is normalised first (mqsim.py:538-544)."""

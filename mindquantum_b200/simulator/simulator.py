@@ -124,6 +124,15 @@ class Simulator:
         fn = getattr(self.backend, 'get_pure_state_vector', None)
         return fn() if fn else self.get_qs()
 
+    def get_qs_of_qubits(self, qubits, ket=False):
+        """Reduced state of ``qubits``: a vector when pure, else a density matrix (simulator.py:641)."""
+        return self.backend.get_qs_of_qubits(qubits, ket)
+
+    def set_threads_number(self, number):
+        """Forwarded to the backend (simulator.py:507); the B200 backends, like the reference's
+        MQSim, do not implement it (BackendBase raises NotImplementedError)."""
+        return self.backend.set_threads_number(number)
+
 
 def inner_product(bra_simulator, ket_simulator):
     """<bra|ket> of two simulators (mindquantum/simulator/simulator.py inner_product; Vdot)."""

@@ -483,6 +483,24 @@ def hermitian_gate(g):
 
 
 # ----------------------------------------------------------------------------- drivers
+def reduced_density_matrix(qs, n, kept_qubits):
+    """GetReducedDensityMatrix, ccsrc/lib/simulator/vector/detail/cpu_common/cpu_vector_core_policy.cpp:335-383:
+    for every pair (i, j) of basis states whose traced bits agree, rho[i_kept][j_kept] +=
+    qs[i] conj(qs[j]), bit k of i_kept being bit sorted(kept)[k] of i.  Pure-Python loops: small n."""
+    kept = sorted(kept_qubits)
+    traced = [q for q in range(n) if q not in kept]
+    rho = np.zeros((1 << len(kept), 1 << len(kept)), dtype=np.complex128)
+
+    def sub(i, qubits):
+        return sum(((i >> q) & 1) << k for k, q in enumerate(qubits))
+
+    for i in range(1 << n):
+        for j in range(1 << n):
+            if sub(i, traced) == sub(j, traced):
+                rho[sub(i, kept), sub(j, kept)] += qs[i] * np.conj(qs[j])
+    return rho
+
+
 class OracleSim:
     """A VectorState restatement: holds a numpy state and applies circuits with the C kernels."""
 
