@@ -74,6 +74,12 @@ void require_aligned(const void *ptr, const char *what) {
     if (ptr && (reinterpret_cast<uintptr_t>(ptr) & 15u)) fail(MQB_ERR_INVALID, "%s must be 16-byte aligned", what);
 }
 
+// The register arguments of the entry points that take a bare state: 1..40 qubits, a known precision.
+void require_register(int n, int precision) {
+    if (n < 1 || n > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40], got %d", n);
+    if (precision != MQB_PREC_C64 && precision != MQB_PREC_C128) fail(MQB_ERR_INVALID, "bad precision %d", precision);
+}
+
 // Device allocations of the library (program and Hamiltonian tables): an out-of-memory error is
 // MQB_ERR_ALLOC.  mqb_inject_alloc_failure arms a countdown on the calling thread: after that many
 // successful allocations the next one fails as if the device were out of memory (host-side fault
@@ -1024,6 +1030,8 @@ int mqb_program_get_info(const mqb_program *p, mqb_program_info *info) {
 
 int mqb_program_grad_passes(mqb_program *p, int n_hams, int *n_passes, int *tile_bits) {
     return guarded([&] {
+        if (!p || !n_passes || !tile_bits) fail(MQB_ERR_INVALID, "null argument");
+        if (n_hams < 1) fail(MQB_ERR_INVALID, "need at least one Hamiltonian");
         SchedDev &sd = grad_schedule(*p, n_hams);
         *n_passes = int(sd.s.passes.size());
         *tile_bits = sd.s.K;
@@ -1031,7 +1039,11 @@ int mqb_program_grad_passes(mqb_program *p, int n_hams, int *n_passes, int *tile
 }
 
 int mqb_apply_workspace_size(const mqb_program *p, int64_t batch, size_t *bytes) {
-    return guarded([&] { *bytes = std::max<size_t>(256, align_up(size_t(batch) * p->per_sample * p->elem())); });
+    return guarded([&] {
+        if (!p || !bytes) fail(MQB_ERR_INVALID, "null argument");
+        if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
+        *bytes = std::max<size_t>(256, align_up(size_t(batch) * p->per_sample * p->elem()));
+    });
 }
 
 int mqb_apply(mqb_program *p, void *states, int64_t batch, const double *params, int64_t param_stride,
@@ -1168,6 +1180,7 @@ int mqb_apply_hamiltonian(const mqb_hamiltonian *h, const void *in, void *out, i
         require_aligned(in, "in");
         require_aligned(out, "out");
         if (in == out) fail(MQB_ERR_INVALID, "in and out must be different buffers");
+        if (batch < 0) fail(MQB_ERR_INVALID, "batch must be >= 0");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         if (h->precision == MQB_PREC_C64)
             ham_impl<float>(*h, nullptr, static_cast<const float2 *>(in), static_cast<float2 *>(out), nullptr, 2, batch, st);
@@ -1180,6 +1193,7 @@ int mqb_apply_hamiltonian(const mqb_hamiltonian *h, const void *in, void *out, i
 int mqb_expectation(const mqb_hamiltonian *h, const void *bra, const void *ket, int64_t batch, double *out, void *stream) {
     return guarded([&] {
         if (!h || !bra || !ket || !out) fail(MQB_ERR_INVALID, "null argument");
+        if (batch < 0) fail(MQB_ERR_INVALID, "batch must be >= 0");
         require_aligned(bra, "bra");
         require_aligned(ket, "ket");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1281,6 +1295,8 @@ int mqb_rows_matrix1_norm(int n, int precision, const void *states, int64_t batc
 int mqb_vdot(int n, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream) {
     return guarded([&] {
         if (!a || !b || !out) fail(MQB_ERR_INVALID, "null argument");
+        require_register(n, precision);
+        if (batch < 0) fail(MQB_ERR_INVALID, "batch must be >= 0");
         require_aligned(a, "a");
         require_aligned(b, "b");
         const int sm = sm_count_cached();
@@ -1295,7 +1311,9 @@ int mqb_vdot(int n, int precision, const void *a, const void *b, int64_t batch, 
 
 int mqb_grad_workspace_size(const mqb_program *p, int64_t batch, int n_hams, int stride, size_t *bytes) {
     return guarded([&] {
+        if (!p || !bytes) fail(MQB_ERR_INVALID, "null argument");
         if (n_hams < 1) fail(MQB_ERR_INVALID, "need at least one Hamiltonian");
+        if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
         SchedDev &sd = grad_schedule(const_cast<mqb_program &>(*p), n_hams);
         *bytes = grad_layout(*p, sd.s, batch, n_hams, stride).total;
     });
@@ -1372,6 +1390,8 @@ int mqb_adjoint_with_lambda(mqb_program *p, const void *lam, int lam_batched, co
 
 int mqb_sample_scratch_size(int n, size_t *bytes) {
     return guarded([&] {
+        if (!bytes) fail(MQB_ERR_INVALID, "null argument");
+        if (n < 1 || n > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40], got %d", n);
         const int cb = std::min(n, 12);
         *bytes = sizeof(double) * ((size_t(1) << (n - cb)) + 1);
     });
@@ -1380,6 +1400,9 @@ int mqb_sample_scratch_size(int n, size_t *bytes) {
 int mqb_sample_indices(int n, int precision, const void *state, const double *u, int64_t shots, int64_t *out,
                        void *scratch, size_t scratch_bytes, void *stream) {
     return guarded([&] {
+        require_register(n, precision);
+        if (shots < 0) fail(MQB_ERR_INVALID, "shots must be >= 0");
+        if (!state || (shots > 0 && (!u || !out))) fail(MQB_ERR_INVALID, "null argument");
         const int cb = std::min(n, 12);
         const size_t need = sizeof(double) * ((size_t(1) << (n - cb)) + 1);
         if (!scratch || scratch_bytes < need) fail(MQB_ERR_WORKSPACE, "scratch too small");
@@ -1400,6 +1423,8 @@ int mqb_sample_indices(int n, int precision, const void *state, const double *u,
 
 int mqb_qubit_one_probability(int n, int precision, const void *state, int q, double *out, void *stream) {
     return guarded([&] {
+        require_register(n, precision);
+        if (!state || !out) fail(MQB_ERR_INVALID, "null argument");
         if (q < 0 || q >= n) fail(MQB_ERR_INVALID, "qubit out of range");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         if (precision == MQB_PREC_C64)
@@ -1411,7 +1436,10 @@ int mqb_qubit_one_probability(int n, int precision, const void *state, int q, do
 
 int mqb_collapse(int n, int precision, void *state, int q, int outcome, double scale, void *stream) {
     return guarded([&] {
+        require_register(n, precision);
+        if (!state) fail(MQB_ERR_INVALID, "null argument");
         if (q < 0 || q >= n) fail(MQB_ERR_INVALID, "qubit out of range");
+        if (outcome != 0 && outcome != 1) fail(MQB_ERR_INVALID, "outcome must be 0 or 1, got %d", outcome);
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         if (precision == MQB_PREC_C64)
             ck(launch_collapse<float>(static_cast<float2 *>(state), n, q, outcome, scale, st), "collapse");

@@ -1,7 +1,8 @@
 """Precision checks and failure handling of the engine.
 
-Host (no GPU): invalid Hamiltonian tables are refused with MQB_ERR_INVALID before any device
-work, and an injected allocation failure surfaces as MQB_ERR_ALLOC with its message.
+Host (no GPU): invalid Hamiltonian tables and invalid arguments of the entry points that take a
+bare state are refused with MQB_ERR_INVALID before any device work, and an injected allocation
+failure surfaces as MQB_ERR_ALLOC with its message.
 
 GPU:
 * the periodic FP64 norm check of the complex64 state (every ceil(sqrt(P)) passes): present for
@@ -46,6 +47,38 @@ def test_ham_create_rejects_bad_tables_on_the_host():
     assert st == MQB_ERR_INVALID and 'overlapping' in msg
     st, _, msg = _ham_call(4, N.MQB_PREC_C64, [1 << 5], [0], [0], [0], [1.0], 1)
     assert st == MQB_ERR_INVALID and 'outside' in msg
+
+
+def test_state_entry_points_reject_bad_arguments_on_the_host():
+    """The entry points that take a bare state check their arguments before any device work: the
+    register (1..40 qubits, a known precision), null pointers, batch and shot counts, qubit and
+    outcome ranges.  The pointers below are never dereferenced."""
+    L = N.lib()
+    p = ctypes.c_void_p(4096)
+    sz = ctypes.c_size_t()
+    i1, i2 = ctypes.c_int(), ctypes.c_int()
+    C64 = N.MQB_PREC_C64
+
+    def err(st, what):
+        msg = L.mqb_last_error().decode()
+        assert st == MQB_ERR_INVALID and what in msg, (st, msg)
+
+    err(L.mqb_vdot(0, C64, p, p, 1, p, None), 'n_qubits')
+    err(L.mqb_vdot(41, C64, p, p, 1, p, None), 'n_qubits')
+    err(L.mqb_vdot(3, 7, p, p, 1, p, None), 'precision')
+    err(L.mqb_vdot(3, C64, p, p, -1, p, None), 'batch')
+    err(L.mqb_sample_scratch_size(0, ctypes.byref(sz)), 'n_qubits')
+    err(L.mqb_sample_scratch_size(3, None), 'null')
+    err(L.mqb_sample_indices(3, C64, None, p, 1, p, p, 1 << 20, None), 'null')
+    err(L.mqb_sample_indices(3, C64, p, p, -1, p, p, 1 << 20, None), 'shots')
+    err(L.mqb_sample_indices(3, 9, p, p, 1, p, p, 1 << 20, None), 'precision')
+    err(L.mqb_qubit_one_probability(3, C64, p, 3, p, None), 'qubit')
+    err(L.mqb_qubit_one_probability(3, C64, None, 0, p, None), 'null')
+    err(L.mqb_collapse(3, C64, p, 0, 2, 1.0, None), 'outcome')
+    err(L.mqb_collapse(3, C64, None, 0, 1, 1.0, None), 'null')
+    err(L.mqb_apply_workspace_size(None, 1, ctypes.byref(sz)), 'null')
+    err(L.mqb_grad_workspace_size(None, 1, 1, 1, ctypes.byref(sz)), 'null')
+    err(L.mqb_program_grad_passes(None, 1, ctypes.byref(i1), ctypes.byref(i2)), 'null')
 
 
 def test_injected_allocation_failure_is_reported():
