@@ -6,7 +6,8 @@
 // cpu_common, cpu_avx_double), the gates and parameter resolvers it uses.  The circuits and
 // Hamiltonians are built by ref_harness_common.h with the reference's classes:
 //
-//   mqref_apply: VectorState::ApplyCircuit + GetQS (vector_state.tpp:949-960);
+//   mqref_apply:  VectorState::ApplyCircuit + GetQS (vector_state.tpp:949-960);
+//   mqref_sample: SamplingMeasurementEndingWithoutNoise / Sampling (vector_state.tpp:1308-1373);
 //   mqref_grad:  VectorState::GetExpectationWithGradMultiMulti (the adjoint gradient,
 //                ccsrc/include/simulator/vector/gradient.h:100-197).
 //
@@ -24,6 +25,9 @@ using sim_f = mindquantum::sim::vector::detail::VectorState<mindquantum::sim::ve
 extern "C" {
 
 int mqref_apply(MQREF_APPLY_ARGS) { return mqref::apply_impl<sim_d>(MQREF_APPLY_PASS); }
+
+// complex128 (CPUVectorPolicyAvxDouble)
+int mqref_sample(MQREF_SAMPLE_ARGS) { return mqref::sample_impl<sim_d>(MQREF_SAMPLE_PASS); }
 
 // complex128 (CPUVectorPolicyAvxDouble)
 int mqref_grad(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_d, double>(MQREF_GRAD_PASS); }

@@ -5,6 +5,8 @@
 // with the reference's classes and calls its VectorState entry points:
 //
 //   apply_impl: VectorState::ApplyCircuit + GetQS (ccsrc/include/simulator/vector/vector_state.tpp:949-960);
+//   sample_impl: VectorState::SamplingMeasurementEndingWithoutNoise / Sampling (vector_state.tpp:1308-1373),
+//                the reference's seeded shot streams;
 //   grad_impl:  VectorState::GetExpectationWithGradMultiMulti (the adjoint gradient,
 //               ccsrc/include/simulator/vector/gradient.h:100-197), with the Hermitian circuit
 //               built the way the reference's Python builds it (mindquantum/core/circuit/
@@ -32,8 +34,9 @@ using mindquantum::qbits_t;
 using parameter::ParameterResolver;
 using circuit_t = std::vector<std::shared_ptr<mindquantum::BasicGate>>;
 
-// Gate kinds of the harness's gate table.
-enum Kind { K_X = 0, K_H = 1, K_RX = 2, K_RY = 3, K_RZ = 4, K_Z = 5, K_RZZ = 6, K_Y = 7, K_PS = 8 };
+// Gate kinds of the harness's gate table.  A measurement (K_M) takes its key from the param column:
+// key "k<param>".
+enum Kind { K_X = 0, K_H = 1, K_RX = 2, K_RY = 3, K_RZ = 4, K_Z = 5, K_RZZ = 6, K_Y = 7, K_PS = 8, K_M = 9 };
 
 inline ParameterResolver angle(int param, double coeff, double cst, const std::vector<std::string> &names,
                                double sign) {
@@ -73,6 +76,9 @@ inline circuit_t build(int n_gates, const int *kind, const int *obj0, const int 
             case K_PS:
                 c.push_back(std::make_shared<mindquantum::PSGate>(angle(param[k], coeff[k], cst[k], names, sign), obj1q, ctrls));
                 break;
+            case K_M:
+                c.push_back(std::make_shared<mindquantum::MeasureGate>("k" + std::to_string(param[k]), obj1q));
+                break;
             default:
                 return {};
         }
@@ -108,6 +114,37 @@ int apply_impl(MQREF_APPLY_ARGS) {
             out[2 * i] = double(qs[i].real());
             out[2 * i + 1] = double(qs[i].imag());
         }
+        return 0;
+    } catch (...) {
+        return -2;
+    }
+}
+
+// Shots of a circuit with measurements from |0...0>: measurement-ending circuits by
+// SamplingMeasurementEndingWithoutNoise (ending != 0), others by Sampling (one re-simulation per
+// shot).  Measurement keys are "k<i>" for the M gates' param column i; out: [shots][n_keys] with
+// column i the key "k<i>" (n_keys = the number of M gates).
+#define MQREF_SAMPLE_ARGS                                                                                           \
+    int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl, const int *param,      \
+        const double *coeff, const double *cst, int n_params, const double *params, int shots, unsigned seed,     \
+        int ending, int *out
+#define MQREF_SAMPLE_PASS n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, n_params, params, shots, seed, ending, out
+
+template <typename sim_t>
+int sample_impl(MQREF_SAMPLE_ARGS) {
+    try {
+        const auto names = param_names(n_params);
+        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false);
+        if (int(c.size()) != n_gates) return -1;
+        ParameterResolver pr;
+        for (int i = 0; i < n_params; ++i) pr.SetItem(names[i], params[i]);
+        mindquantum::MST<size_t> key_map;
+        for (int k = 0; k < n_gates; ++k)
+            if (kind[k] == K_M) key_map["k" + std::to_string(param[k])] = size_t(param[k]);
+        sim_t sim{static_cast<Index>(n)};
+        const auto res = ending ? sim.SamplingMeasurementEndingWithoutNoise(c, pr, size_t(shots), key_map, seed)
+                                : sim.Sampling(c, pr, size_t(shots), key_map, seed);
+        for (size_t i = 0; i < res.size(); ++i) out[i] = int(res[i]);
         return 0;
     } catch (...) {
         return -2;

@@ -15,7 +15,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref.so')
 GPU_LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref_gpu.so')
-_KINDS = {'X': 0, 'H': 1, 'RX': 2, 'RY': 3, 'RZ': 4, 'Z': 5, 'Rzz': 6, 'Y': 7, 'PS': 8}
+_KINDS = {'X': 0, 'H': 1, 'RX': 2, 'RY': 3, 'RZ': 4, 'Z': 5, 'Rzz': 6, 'Y': 7, 'PS': 8, 'M': 9}
 _libs = {}
 
 
@@ -35,6 +35,9 @@ def lib(device='cpu'):
         pre = 'mqref_gpu_' if device == 'gpu' else 'mqref_'
         getattr(L, pre + 'apply').argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, ctypes.c_int,
                                                                                       P]
+        if device == 'cpu':
+            L.mqref_sample.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, ctypes.c_int,
+                                                                            ctypes.c_uint, ctypes.c_int, P]
         for fn in (getattr(L, pre + 'grad'), getattr(L, pre + 'grad_c64')):
             fn.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, P, P, P, ctypes.c_int,
                                                                     ctypes.c_int, P, ctypes.c_int, P]
@@ -42,9 +45,17 @@ def lib(device='cpu'):
     return _libs[device]
 
 
-def _gate_table(circ, names):
+def _gate_table(circ, names, mkeys=None):
+    """Columns of the harness's gate table; measurement gates take the index of their key in
+    ``mkeys`` (appended to in circuit order) as their param column."""
     cols = {k: [] for k in ('kind', 'o0', 'o1', 'ctrl', 'param', 'coeff', 'cst')}
     for g in circ:
+        if g.name == 'M' and mkeys is not None:
+            mkeys.append(g.key)
+            for k, v in (('kind', _KINDS['M']), ('o0', int(g.obj_qubits[0])), ('o1', -1), ('ctrl', -1),
+                         ('param', len(mkeys) - 1), ('coeff', 0.0), ('cst', 0.0)):
+                cols[k].append(v)
+            continue
         name = 'PS' if g.name in ('PS', 'PhaseShift') else g.name
         if name not in _KINDS or len(g.ctrl_qubits) > 1:
             raise ValueError(f"gate {g.name} is not supported by the reference harness")
@@ -118,3 +129,21 @@ def grad(n, circ, ham, params, threads=0, complex64=False, device='cpu'):
         raise RuntimeError(f"mqref_grad failed ({st})")
     out = out.reshape(S, 1 + len(names), 2)
     return out[..., 0] + 1j * out[..., 1]
+
+
+def sample(n, circ, params, shots, seed, ending=True):
+    """Shots of ``circ`` from |0...0> by the reference's own samplers (complex128):
+    SamplingMeasurementEndingWithoutNoise when ``ending``, else Sampling (one re-simulation per
+    shot, mid-circuit measurements).  Returns (keys in circuit order, samples[shots][n_keys])."""
+    names = list(circ.params_name)
+    keys = []
+    ints, dbls = _gate_table(circ, names, keys)
+    p = np.ascontiguousarray(params if len(names) else [0.0], dtype=np.float64).reshape(-1)
+    out = np.zeros(max(1, shots * len(keys)), dtype=np.int32)
+    L, _ = lib('cpu')
+    st = L.mqref_sample(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
+                        _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), len(names), _p(p), shots, seed,
+                        1 if ending else 0, _p(out))
+    if st != 0:
+        raise RuntimeError(f"mqref_sample failed ({st})")
+    return keys, out[:shots * len(keys)].reshape(shots, len(keys)).astype(np.int64)

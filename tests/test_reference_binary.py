@@ -5,6 +5,7 @@ and ApplyCircuit) runs here on the host through oracle/refbin.py; these tests pi
 restatement to it on the benchmark circuit families at full size where the host finishes in
 seconds: config 1 exactly (16 qubits x 8 layers), the QNN encoder/ansatz, QAOA MaxCut and random
 Pauli Hamiltonians with Y terms.  Tolerance: 1e-12 (both FP64), complex64 reference within 1e-5.
+Both samplers (measurement-ending and mid-circuit) are pinned shot for shot for the same seed.
 Skipped where the reference checkout was not available to build the library.
 
 The reference's thrust GPU simulator (`mqvector_gpu`, VectorState<GPUVectorPolicyDouble/Float>,
@@ -58,6 +59,47 @@ def test_random_pauli_hamiltonians_oracle_equals_reference():
     circ, _, params = W.hea(n, 3, 2, seed=3, encoder=True)
     ham = W.random_pauli_hamiltonian(n, 25, rng)
     assert np.max(np.abs(R.grad(n, circ, ham, params) - _oracle(n, circ, ham, params))) <= 1e-12
+
+
+def test_sampling_oracle_equals_reference():
+    """Both samplers shot for shot against the reference's own (its std::mt19937 streams, compiled
+    with this image's C++ library): a measurement-ending circuit through
+    SamplingMeasurementEndingWithoutNoise, and circuits with mid-circuit and repeated measurements
+    through Sampling (one re-simulation per shot)."""
+    from mindquantum_b200.core import gates as G
+    from mindquantum_b200.core.circuit import Circuit
+
+    n = 6
+    circ = Circuit().un(G.H, n).rx(0.7, 2).x(3, 1).ry(1.3, 4)
+    for q in range(n):
+        circ.measure(f'q{q}', q)
+    keys, ref = R.sample(n, circ, [], 500, 17, ending=True)
+    okeys, orc = O.sampling_measure_ending(n, circ, {}, 500, 17)
+    assert keys == okeys and np.array_equal(ref, orc)
+
+    n = 5
+    circ = Circuit().un(G.H, n).rx('t', 2).x(3, 1).ry(1.3, 4).rz('u', 0)
+    circ.measure('m0', 2)
+    circ += G.RX(0.4).on(2)
+    circ.measure('m1', 2)
+    circ.measure('m2', 0)
+    circ += G.H.on(0)
+    circ.measure('m3', 0)
+    prd = {'t': 0.9, 'u': 1.7}
+    keys, ref = R.sample(n, circ, [prd[k] for k in circ.params_name], 300, 1234, ending=False)
+    okeys, orc = O.sampling_general(n, circ, prd, 300, 1234)
+    assert keys == okeys and np.array_equal(ref, orc)
+
+    # the sampling example of mindquantum/simulator/simulator.py:470-484 (RY(a), RY(b), q0 measured
+    # twice): the compiled reference and the oracle agree shot for shot; neither reproduces the
+    # docstring's printed counts, which the reference's tests never execute
+    circ = Circuit().ry('a', 0).ry('b', 1)
+    circ += G.Measure('q0_0').on(0)
+    circ += G.Measure('q0_1').on(0)
+    circ += G.Measure('q1').on(1)
+    keys, ref = R.sample(2, circ, [1.1, 2.2], 100, 42, ending=False)
+    okeys, orc = O.sampling_general(2, circ, {'a': 1.1, 'b': 2.2}, 100, 42)
+    assert keys == okeys and np.array_equal(ref, orc)
 
 
 @pytest.mark.gpu
