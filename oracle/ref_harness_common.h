@@ -35,8 +35,13 @@ using parameter::ParameterResolver;
 using circuit_t = std::vector<std::shared_ptr<mindquantum::BasicGate>>;
 
 // Gate kinds of the harness's gate table.  A measurement (K_M) takes its key from the param column:
-// key "k<param>".
-enum Kind { K_X = 0, K_H = 1, K_RX = 2, K_RY = 3, K_RZ = 4, K_Z = 5, K_RZZ = 6, K_Y = 7, K_PS = 8, K_M = 9 };
+// key "k<param>".  Channels take their arguments from ch[3 k .. 3 k + 2]: Pauli (px, py, pz),
+// depolarizing (p), amplitude damping (gamma, -, daggered), phase damping (gamma), thermal
+// relaxation (t1, t2, gate time).
+enum Kind {
+    K_X = 0, K_H = 1, K_RX = 2, K_RY = 3, K_RZ = 4, K_Z = 5, K_RZZ = 6, K_Y = 7, K_PS = 8, K_M = 9,
+    K_PC = 10, K_DEP = 11, K_AD = 12, K_PD = 13, K_TR = 14
+};
 
 inline ParameterResolver angle(int param, double coeff, double cst, const std::vector<std::string> &names,
                                double sign) {
@@ -47,7 +52,7 @@ inline ParameterResolver angle(int param, double coeff, double cst, const std::v
 // The circuit of the table, or its Hermitian conjugate (reversed, parameter expressions negated).
 inline circuit_t build(int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl,
                        const int *param, const double *coeff, const double *cst, const std::vector<std::string> &names,
-                       bool herm) {
+                       bool herm, const double *ch = nullptr) {
     circuit_t c;
     for (int i = 0; i < n_gates; ++i) {
         const int k = herm ? n_gates - 1 - i : i;
@@ -79,6 +84,22 @@ inline circuit_t build(int n_gates, const int *kind, const int *obj0, const int 
             case K_M:
                 c.push_back(std::make_shared<mindquantum::MeasureGate>("k" + std::to_string(param[k]), obj1q));
                 break;
+            case K_PC:
+            case K_DEP:
+            case K_AD:
+            case K_PD:
+            case K_TR: {
+                if (!ch) return {};
+                const double *a = ch + 3 * k;
+                if (kind[k] == K_PC) c.push_back(std::make_shared<mindquantum::PauliChannel>(a[0], a[1], a[2], obj1q, ctrls));
+                if (kind[k] == K_DEP) c.push_back(std::make_shared<mindquantum::DepolarizingChannel>(a[0], obj1q, ctrls));
+                if (kind[k] == K_AD)
+                    c.push_back(std::make_shared<mindquantum::AmplitudeDampingChannel>(a[2] != 0, a[0], obj1q, ctrls));
+                if (kind[k] == K_PD) c.push_back(std::make_shared<mindquantum::PhaseDampingChannel>(a[0], obj1q, ctrls));
+                if (kind[k] == K_TR)
+                    c.push_back(std::make_shared<mindquantum::ThermalRelaxationChannel>(a[0], a[1], a[2], obj1q, ctrls));
+                break;
+            }
             default:
                 return {};
         }
@@ -120,21 +141,22 @@ int apply_impl(MQREF_APPLY_ARGS) {
     }
 }
 
-// Shots of a circuit with measurements from |0...0>: measurement-ending circuits by
-// SamplingMeasurementEndingWithoutNoise (ending != 0), others by Sampling (one re-simulation per
-// shot).  Measurement keys are "k<i>" for the M gates' param column i; out: [shots][n_keys] with
+// Shots of a circuit with measurements (and noise channels) from |0...0>: measurement-ending
+// circuits by SamplingMeasurementEndingWithoutNoise (ending != 0), others by Sampling (one
+// re-simulation per shot, channels drawing from the shot's stream, vector_state.tpp:465-709).  Measurement keys are "k<i>" for the M gates' param column i; out: [shots][n_keys] with
 // column i the key "k<i>" (n_keys = the number of M gates).
 #define MQREF_SAMPLE_ARGS                                                                                           \
     int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl, const int *param,      \
-        const double *coeff, const double *cst, int n_params, const double *params, int shots, unsigned seed,     \
-        int ending, int *out
-#define MQREF_SAMPLE_PASS n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, n_params, params, shots, seed, ending, out
+        const double *coeff, const double *cst, const double *ch, int n_params, const double *params, int shots,  \
+        unsigned seed, int ending, int *out
+#define MQREF_SAMPLE_PASS \
+    n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, ch, n_params, params, shots, seed, ending, out
 
 template <typename sim_t>
 int sample_impl(MQREF_SAMPLE_ARGS) {
     try {
         const auto names = param_names(n_params);
-        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false);
+        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false, ch);
         if (int(c.size()) != n_gates) return -1;
         ParameterResolver pr;
         for (int i = 0; i < n_params; ++i) pr.SetItem(names[i], params[i]);

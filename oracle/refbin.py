@@ -16,6 +16,17 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref.so')
 GPU_LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref_gpu.so')
 _KINDS = {'X': 0, 'H': 1, 'RX': 2, 'RY': 3, 'RZ': 4, 'Z': 5, 'Rzz': 6, 'Y': 7, 'PS': 8, 'M': 9}
+_CHANNELS = {'PC': 10, 'BFC': 10, 'PFC': 10, 'BPFC': 10, 'DC': 11, 'ADC': 12, 'PDC': 13, 'TRC': 14}
+
+
+def _channel_args(g):
+    if g.name in ('PC', 'BFC', 'PFC', 'BPFC'):
+        return [g.px, g.py, g.pz]
+    if g.name in ('DC', 'PDC'):
+        return [g.p if g.name == 'DC' else g.gamma, 0.0, 0.0]
+    if g.name == 'ADC':
+        return [g.gamma, 0.0, 1.0 if getattr(g, 'hermitianed', False) else 0.0]
+    return [g.t1, g.t2, g.gate_time]
 _libs = {}
 
 
@@ -36,7 +47,7 @@ def lib(device='cpu'):
         getattr(L, pre + 'apply').argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, ctypes.c_int,
                                                                                       P]
         if device == 'cpu':
-            L.mqref_sample.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, ctypes.c_int,
+            L.mqref_sample.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 8 + [ctypes.c_int, P, ctypes.c_int,
                                                                             ctypes.c_uint, ctypes.c_int, P]
         for fn in (getattr(L, pre + 'grad'), getattr(L, pre + 'grad_c64')):
             fn.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, P, P, P, ctypes.c_int,
@@ -48,8 +59,19 @@ def lib(device='cpu'):
 def _gate_table(circ, names, mkeys=None):
     """Columns of the harness's gate table; measurement gates take the index of their key in
     ``mkeys`` (appended to in circuit order) as their param column."""
-    cols = {k: [] for k in ('kind', 'o0', 'o1', 'ctrl', 'param', 'coeff', 'cst')}
+    cols = {k: [] for k in ('kind', 'o0', 'o1', 'ctrl', 'param', 'coeff', 'cst', 'ch')}
     for g in circ:
+        if g.name in _CHANNELS:
+            if len(g.obj_qubits) > 2 or len(g.ctrl_qubits) > 1:
+                raise ValueError(f"channel {g.name} on {g.obj_qubits} is not supported by the reference harness")
+            for k, v in (('kind', _CHANNELS[g.name]), ('o0', int(g.obj_qubits[0])),
+                         ('o1', int(g.obj_qubits[1]) if len(g.obj_qubits) > 1 else -1),
+                         ('ctrl', int(g.ctrl_qubits[0]) if g.ctrl_qubits else -1), ('param', -1), ('coeff', 0.0),
+                         ('cst', 0.0)):
+                cols[k].append(v)
+            cols['ch'].extend(_channel_args(g))
+            continue
+        cols['ch'].extend([0.0, 0.0, 0.0])
         if g.name == 'M' and mkeys is not None:
             mkeys.append(g.key)
             for k, v in (('kind', _KINDS['M']), ('o0', int(g.obj_qubits[0])), ('o1', -1), ('ctrl', -1),
@@ -77,7 +99,7 @@ def _gate_table(circ, names, mkeys=None):
             cols['coeff'].append(0.0)
             cols['cst'].append(0.0)
     ints = {k: np.ascontiguousarray(cols[k], dtype=np.int32) for k in ('kind', 'o0', 'o1', 'ctrl', 'param')}
-    dbls = {k: np.ascontiguousarray(cols[k], dtype=np.float64) for k in ('coeff', 'cst')}
+    dbls = {k: np.ascontiguousarray(cols[k] if cols[k] else [0.0], dtype=np.float64) for k in ('coeff', 'cst', 'ch')}
     return ints, dbls
 
 
@@ -142,7 +164,8 @@ def sample(n, circ, params, shots, seed, ending=True):
     out = np.zeros(max(1, shots * len(keys)), dtype=np.int32)
     L, _ = lib('cpu')
     st = L.mqref_sample(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
-                        _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), len(names), _p(p), shots, seed,
+                        _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), _p(dbls['ch']), len(names), _p(p), shots,
+                        seed,
                         1 if ending else 0, _p(out))
     if st != 0:
         raise RuntimeError(f"mqref_sample failed ({st})")

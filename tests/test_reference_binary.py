@@ -5,7 +5,8 @@ and ApplyCircuit) runs here on the host through oracle/refbin.py; these tests pi
 restatement to it on the benchmark circuit families at full size where the host finishes in
 seconds: config 1 exactly (16 qubits x 8 layers), the QNN encoder/ansatz, QAOA MaxCut and random
 Pauli Hamiltonians with Y terms.  Tolerance: 1e-12 (both FP64), complex64 reference within 1e-5.
-Both samplers (measurement-ending and mid-circuit) are pinned shot for shot for the same seed.
+Both samplers (measurement-ending and mid-circuit) and the noise channels' trajectories are pinned
+shot for shot for the same seed.
 Skipped where the reference checkout was not available to build the library.
 
 The reference's thrust GPU simulator (`mqvector_gpu`, VectorState<GPUVectorPolicyDouble/Float>,
@@ -99,6 +100,32 @@ def test_sampling_oracle_equals_reference():
     circ += G.Measure('q1').on(1)
     keys, ref = R.sample(2, circ, [1.1, 2.2], 100, 42, ending=False)
     okeys, orc = O.sampling_general(2, circ, {'a': 1.1, 'b': 2.2}, 100, 42)
+    assert keys == okeys and np.array_equal(ref, orc)
+
+
+def test_noise_channels_oracle_equals_reference():
+    """Noisy trajectories shot for shot against the reference's Sampling, whose shots apply each
+    channel with a draw from the shot's stream (ApplyChannel, vector_state.tpp:465-709): one- and
+    two-qubit depolarizing, amplitude damping, Pauli, phase damping, thermal relaxation and
+    bit-flip channels between gates, then measurements."""
+    from mindquantum_b200.core import gates as G
+    from mindquantum_b200.core.circuit import Circuit
+
+    n = 4
+    circ = Circuit().un(G.H, n).rx('t', 2).x(3, 1)
+    circ += G.DepolarizingChannel(0.1).on(0)
+    circ += G.AmplitudeDampingChannel(0.3).on(1)
+    circ += G.PauliChannel(0.05, 0.1, 0.15).on(2)
+    circ += G.PhaseDampingChannel(0.2).on(3)
+    circ += G.ThermalRelaxationChannel(10.0, 15.0, 3.0).on(1)
+    circ += G.BitFlipChannel(0.2).on(3)
+    circ += G.DepolarizingChannel(0.3, 2).on([0, 2])
+    circ += G.RY(0.8).on(1)
+    for q in range(n):
+        circ.measure(f'q{q}', q)
+    prd = {'t': 0.9}
+    keys, ref = R.sample(n, circ, [prd[k] for k in circ.params_name], 400, 99, ending=False)
+    okeys, orc = O.sampling_general(n, circ, prd, 400, 99)
     assert keys == okeys and np.array_equal(ref, orc)
 
 
