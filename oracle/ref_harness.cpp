@@ -9,17 +9,24 @@
 //   mqref_apply:  VectorState::ApplyCircuit + GetQS (vector_state.tpp:949-960);
 //   mqref_sample: SamplingMeasurementEndingWithoutNoise / Sampling (vector_state.tpp:1308-1373);
 //   mqref_grad:  VectorState::GetExpectationWithGradMultiMulti (the adjoint gradient,
-//                ccsrc/include/simulator/vector/gradient.h:100-197).
+//                ccsrc/include/simulator/vector/gradient.h:100-197);
+//   mqref_dm_apply / mqref_dm_grad: the density-matrix simulator (DensityMatrixState, its CPU
+//                policy under ccsrc/lib/simulator/densitymatrix/detail/cpu_common): rho after a
+//                circuit with channels, and the expectation gradient with and without noise.
 //
 // Only tests/ and bench.py's CPU legs load it, to pin the oracle to the reference itself and to
 // time the reference on the host; the product never does.
 #include "ref_harness_common.h"
+#include "simulator/densitymatrix/densitymatrix_state.h"
+#include "simulator/densitymatrix/detail/cpu_densitymatrix_avx_double_policy.h"
 #include "simulator/vector/detail/cpu_vector_avx_double_policy.h"
 #include "simulator/vector/detail/cpu_vector_avx_float_policy.h"
 
 namespace {
 using sim_d = mindquantum::sim::vector::detail::VectorState<mindquantum::sim::vector::detail::CPUVectorPolicyAvxDouble>;
 using sim_f = mindquantum::sim::vector::detail::VectorState<mindquantum::sim::vector::detail::CPUVectorPolicyAvxFloat>;
+using dm_d = mindquantum::sim::densitymatrix::detail::DensityMatrixState<
+    mindquantum::sim::densitymatrix::detail::CPUDensityMatrixPolicyAvxDouble>;
 }  // namespace
 
 extern "C" {
@@ -34,5 +41,67 @@ int mqref_grad(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_d, double>(MQREF_G
 
 // complex64 (CPUVectorPolicyAvxFloat)
 int mqref_grad_c64(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_f, float>(MQREF_GRAD_PASS); }
+
+// The reference's density-matrix simulator (DensityMatrixState<CPUDensityMatrixPolicyAvxDouble>,
+// ccsrc/include/simulator/densitymatrix/densitymatrix_state.tpp), complex128: the circuit (gates and
+// channels, table as in mqref_sample, measurements not allowed) applied to |0><0|; out: rho as
+// 2^n x 2^n complex128 (re, im), row-major.
+int mqref_dm_apply(int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl,
+                   const int *param, const double *coeff, const double *cst, const double *ch, int n_params,
+                   const double *params, double *out) {
+    try {
+        const auto names = mqref::param_names(n_params);
+        const mqref::circuit_t c = mqref::build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false, ch);
+        if (int(c.size()) != n_gates) return -1;
+        parameter::ParameterResolver pr;
+        for (int i = 0; i < n_params; ++i) pr.SetItem(names[i], params[i]);
+        dm_d sim{static_cast<mindquantum::Index>(n)};
+        sim.ApplyCircuit(c, pr);
+        const auto rho = sim.GetQS();
+        const size_t d = size_t(1) << n;
+        for (size_t i = 0; i < d; ++i)
+            for (size_t j = 0; j < d; ++j) {
+                out[2 * (i * d + j)] = rho[i][j].real();
+                out[2 * (i * d + j) + 1] = rho[i][j].imag();
+            }
+        return 0;
+    } catch (...) {
+        return -2;
+    }
+}
+
+// <H> and its gradient on the density-matrix simulator, as MQSim.get_expectation_with_grad calls it
+// (mindquantum/simulator/mqsim.py:389-400): GetExpectationWithNoiseGradMultiMulti when the circuit
+// holds a channel, else GetExpectationWithReversibleGradMultiMulti; every parameter an encoder
+// input.  Arguments as mqref_grad plus the channel column ch.
+int mqref_dm_grad(int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl,
+                  const int *param, const double *coeff, const double *cst, const double *ch, int n_terms,
+                  const int *term_len, const int *term_q, const char *term_p, const double *term_c, int n_params,
+                  int n_samples, const double *params, double *out) {
+    try {
+        const auto names = mqref::param_names(n_params);
+        const mqref::circuit_t c = mqref::build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false, ch);
+        const mqref::circuit_t h = mqref::build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, true, ch);
+        if (int(c.size()) != n_gates || int(h.size()) != n_gates) return -1;
+        bool noisy = false;
+        for (int k = 0; k < n_gates; ++k) noisy = noisy || kind[k] >= mqref::K_PC;
+        std::vector<std::shared_ptr<mindquantum::Hamiltonian<double>>> hams{
+            mqref::hamiltonian<double>(n_terms, term_len, term_q, term_p, term_c)};
+        std::vector<std::vector<double>> enc(n_samples, std::vector<double>(n_params));
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i < n_params; ++i) enc[s][i] = params[s * n_params + i];
+        dm_d sim{static_cast<mindquantum::Index>(n)};
+        const auto res = noisy ? sim.GetExpectationWithNoiseGradMultiMulti(hams, c, h, enc, {}, names, {}, 1, 1)
+                               : sim.GetExpectationWithReversibleGradMultiMulti(hams, c, h, enc, {}, names, {}, 1, 1);
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i <= n_params; ++i) {
+                out[2 * (s * (n_params + 1) + i)] = res[s][0][i].real();
+                out[2 * (s * (n_params + 1) + i) + 1] = res[s][0][i].imag();
+            }
+        return 0;
+    } catch (...) {
+        return -2;
+    }
+}
 
 }  // extern "C"

@@ -93,8 +93,9 @@ inline circuit_t build(int n_gates, const int *kind, const int *obj0, const int 
                 const double *a = ch + 3 * k;
                 if (kind[k] == K_PC) c.push_back(std::make_shared<mindquantum::PauliChannel>(a[0], a[1], a[2], obj1q, ctrls));
                 if (kind[k] == K_DEP) c.push_back(std::make_shared<mindquantum::DepolarizingChannel>(a[0], obj1q, ctrls));
-                if (kind[k] == K_AD)
-                    c.push_back(std::make_shared<mindquantum::AmplitudeDampingChannel>(a[2] != 0, a[0], obj1q, ctrls));
+                if (kind[k] == K_AD)   // the Hermitian circuit takes the daggered channel (basic.py hermitian())
+                    c.push_back(
+                        std::make_shared<mindquantum::AmplitudeDampingChannel>((a[2] != 0) != herm, a[0], obj1q, ctrls));
                 if (kind[k] == K_PD) c.push_back(std::make_shared<mindquantum::PhaseDampingChannel>(a[0], obj1q, ctrls));
                 if (kind[k] == K_TR)
                     c.push_back(std::make_shared<mindquantum::ThermalRelaxationChannel>(a[0], a[1], a[2], obj1q, ctrls));
@@ -185,6 +186,19 @@ int sample_impl(MQREF_SAMPLE_ARGS) {
 #define MQREF_GRAD_PASS                                                                                           \
     n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, n_terms, term_len, term_q, term_p, term_c, n_params, \
         n_samples, params, threads, out
+
+// The Hamiltonian of a gradient call as the reference's type.
+template <typename calc_t>
+std::shared_ptr<mindquantum::Hamiltonian<calc_t>> hamiltonian(int n_terms, const int *term_len, const int *term_q,
+                                                               const char *term_p, const double *term_c) {
+    std::vector<mindquantum::PauliTerm<calc_t>> terms;
+    for (int t = 0, o = 0; t < n_terms; ++t) {
+        std::vector<mindquantum::PauliWord> w;
+        for (int k = 0; k < term_len[t]; ++k, ++o) w.emplace_back(Index(term_q[o]), term_p[o]);
+        terms.emplace_back(w, calc_t(term_c[t]));
+    }
+    return std::make_shared<mindquantum::Hamiltonian<calc_t>>(terms);
+}
 
 template <typename sim_t, typename calc_t>
 int grad_impl(MQREF_GRAD_ARGS) {

@@ -170,3 +170,57 @@ def sample(n, circ, params, shots, seed, ending=True):
     if st != 0:
         raise RuntimeError(f"mqref_sample failed ({st})")
     return keys, out[:shots * len(keys)].reshape(shots, len(keys)).astype(np.int64)
+
+
+def _ham_arrays(ham):
+    tl, tq, tp, tc = [], [], [], []
+    for term, c in ham.ham_termlist:
+        tl.append(len(term))
+        tc.append(float(c))
+        for q, pch in term:
+            tq.append(int(q))
+            tp.append(pch)
+    return (np.ascontiguousarray(tl, dtype=np.int32), np.ascontiguousarray(tq if tq else [0], dtype=np.int32),
+            ctypes.create_string_buffer(''.join(tp).encode() or b'\0'), np.ascontiguousarray(tc, dtype=np.float64))
+
+
+def dm_apply(n, circ, params):
+    """The reference's density-matrix simulator (complex128): rho after ``circ`` (gates and
+    channels) from |0...0><0...0|, as a 2^n x 2^n array."""
+    names = list(circ.params_name)
+    ints, dbls = _gate_table(circ, names)
+    p = np.ascontiguousarray(params if len(names) else [0.0], dtype=np.float64).reshape(-1)
+    out = np.zeros(2 << (2 * n), dtype=np.float64)
+    L, _ = lib('cpu')
+    P = ctypes.c_void_p
+    L.mqref_dm_apply.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 8 + [ctypes.c_int, P, P]
+    st = L.mqref_dm_apply(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
+                          _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), _p(dbls['ch']), len(names), _p(p),
+                          _p(out))
+    if st != 0:
+        raise RuntimeError(f"mqref_dm_apply failed ({st})")
+    d = 1 << n
+    return (out[0::2] + 1j * out[1::2]).reshape(d, d)
+
+
+def dm_grad(n, circ, ham, params):
+    """The reference's density-matrix expectation gradient (GetExpectationWithNoiseGradMultiMulti
+    with channels in ``circ``, else GetExpectationWithReversibleGradMultiMulti), every parameter an
+    encoder input: params [samples][n_params] -> [samples][1 + n_params] complex."""
+    names = list(circ.params_name)
+    ints, dbls = _gate_table(circ, names)
+    tl, tq, tpb, tc = _ham_arrays(ham)
+    params = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
+    S = params.shape[0]
+    out = np.zeros(S * (1 + len(names)) * 2, dtype=np.float64)
+    L, _ = lib('cpu')
+    P = ctypes.c_void_p
+    L.mqref_dm_grad.argtypes = ([ctypes.c_int, ctypes.c_int] + [P] * 8 + [ctypes.c_int, P, P, P, P, ctypes.c_int,
+                                                                         ctypes.c_int, P, P])
+    st = L.mqref_dm_grad(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
+                         _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), _p(dbls['ch']), len(tl), _p(tl),
+                         _p(tq), ctypes.cast(tpb, ctypes.c_void_p), _p(tc), len(names), S, _p(params), _p(out))
+    if st != 0:
+        raise RuntimeError(f"mqref_dm_grad failed ({st})")
+    out = out.reshape(S, 1 + len(names), 2)
+    return out[..., 0] + 1j * out[..., 1]
