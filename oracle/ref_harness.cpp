@@ -84,7 +84,7 @@ int mqref_dm_grad(int n, int n_gates, const int *kind, const int *obj0, const in
         const mqref::circuit_t h = mqref::build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, true, ch);
         if (int(c.size()) != n_gates || int(h.size()) != n_gates) return -1;
         bool noisy = false;
-        for (int k = 0; k < n_gates; ++k) noisy = noisy || kind[k] >= mqref::K_PC;
+        for (int k = 0; k < n_gates; ++k) noisy = noisy || (kind[k] >= mqref::K_PC && kind[k] <= mqref::K_TR);
         std::vector<std::shared_ptr<mindquantum::Hamiltonian<double>>> hams{
             mqref::hamiltonian<double>(n_terms, term_len, term_q, term_p, term_c)};
         std::vector<std::vector<double>> enc(n_samples, std::vector<double>(n_params));

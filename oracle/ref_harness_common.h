@@ -35,18 +35,30 @@ using parameter::ParameterResolver;
 using circuit_t = std::vector<std::shared_ptr<mindquantum::BasicGate>>;
 
 // Gate kinds of the harness's gate table.  A measurement (K_M) takes its key from the param column:
-// key "k<param>".  Channels take their arguments from ch[3 k .. 3 k + 2]: Pauli (px, py, pz),
-// depolarizing (p), amplitude damping (gamma, -, daggered), phase damping (gamma), thermal
-// relaxation (t1, t2, gate time).
+// key "k<param>".  Each gate has six extra values ch[6 k .. 6 k + 5].  Channels take their arguments
+// from the first three: Pauli (px, py, pz), depolarizing (p), amplitude damping (gamma, -,
+// daggered), phase damping (gamma), thermal relaxation (t1, t2, gate time).  S, T, SX and ISWAP
+// take a daggered flag from ch[6 k].  The multi-angle gates U3 (theta, phi, lambda), Rn (alpha,
+// beta, gamma) and FSim (theta, phi) take angle i = ch[6 k + i] + ch[6 k + 3 + i] * p, p the
+// gate's parameter (param column, -1 for none).
 enum Kind {
     K_X = 0, K_H = 1, K_RX = 2, K_RY = 3, K_RZ = 4, K_Z = 5, K_RZZ = 6, K_Y = 7, K_PS = 8, K_M = 9,
-    K_PC = 10, K_DEP = 11, K_AD = 12, K_PD = 13, K_TR = 14
+    K_PC = 10, K_DEP = 11, K_AD = 12, K_PD = 13, K_TR = 14,
+    K_S = 15, K_T = 16, K_SX = 17, K_SWAP = 18, K_ISWAP = 19, K_RXX = 20, K_RYY = 21, K_RXY = 22, K_RXZ = 23,
+    K_RYZ = 24, K_GIVENS = 25, K_GP = 26, K_SWAPALPHA = 27, K_U3 = 28, K_RN = 29, K_FSIM = 30
 };
+constexpr int kCh = 6;   // extra values per gate
 
 inline ParameterResolver angle(int param, double coeff, double cst, const std::vector<std::string> &names,
                                double sign) {
     if (param < 0) return ParameterResolver(sign * cst);
     return ParameterResolver(sign * cst, std::map<std::string, double>{{names[param], sign * coeff}});
+}
+
+// Angle i of a multi-angle gate: ch[i] + ch[3 + i] * p.
+inline ParameterResolver angle_i(int param, const double *a, int i, const std::vector<std::string> &names,
+                                 double sign) {
+    return angle(param, a[3 + i], a[i], names, sign);
 }
 
 // The circuit of the table, or its Hermitian conjugate (reversed, parameter expressions negated).
@@ -90,7 +102,7 @@ inline circuit_t build(int n_gates, const int *kind, const int *obj0, const int 
             case K_PD:
             case K_TR: {
                 if (!ch) return {};
-                const double *a = ch + 3 * k;
+                const double *a = ch + kCh * k;
                 if (kind[k] == K_PC) c.push_back(std::make_shared<mindquantum::PauliChannel>(a[0], a[1], a[2], obj1q, ctrls));
                 if (kind[k] == K_DEP) c.push_back(std::make_shared<mindquantum::DepolarizingChannel>(a[0], obj1q, ctrls));
                 if (kind[k] == K_AD)   // the Hermitian circuit takes the daggered channel (basic.py hermitian())
@@ -99,6 +111,63 @@ inline circuit_t build(int n_gates, const int *kind, const int *obj0, const int 
                 if (kind[k] == K_PD) c.push_back(std::make_shared<mindquantum::PhaseDampingChannel>(a[0], obj1q, ctrls));
                 if (kind[k] == K_TR)
                     c.push_back(std::make_shared<mindquantum::ThermalRelaxationChannel>(a[0], a[1], a[2], obj1q, ctrls));
+                break;
+            }
+            case K_S:
+            case K_T:
+            case K_SX:
+            case K_ISWAP: {   // the Hermitian circuit takes the other of the gate and its dagger
+                const bool dag = ((ch && ch[kCh * k] != 0) != herm);
+                if (kind[k] == K_S) {
+                    if (dag) c.push_back(std::make_shared<mindquantum::SdagGate>(obj1q, ctrls));
+                    else c.push_back(std::make_shared<mindquantum::SGate>(obj1q, ctrls));
+                }
+                if (kind[k] == K_T) {
+                    if (dag) c.push_back(std::make_shared<mindquantum::TdagGate>(obj1q, ctrls));
+                    else c.push_back(std::make_shared<mindquantum::TGate>(obj1q, ctrls));
+                }
+                if (kind[k] == K_SX) {
+                    if (dag) c.push_back(std::make_shared<mindquantum::SXdagGate>(obj1q, ctrls));
+                    else c.push_back(std::make_shared<mindquantum::SXGate>(obj1q, ctrls));
+                }
+                if (kind[k] == K_ISWAP) c.push_back(std::make_shared<mindquantum::ISWAPGate>(dag, obj1q, ctrls));
+                break;
+            }
+            case K_SWAP: c.push_back(std::make_shared<mindquantum::SWAPGate>(obj1q, ctrls)); break;
+            case K_RXX:
+            case K_RYY:
+            case K_RXY:
+            case K_RXZ:
+            case K_RYZ:
+            case K_GIVENS:
+            case K_GP:
+            case K_SWAPALPHA: {
+                const ParameterResolver a = angle(param[k], coeff[k], cst[k], names, sign);
+                if (kind[k] == K_RXX) c.push_back(std::make_shared<mindquantum::RxxGate>(a, obj1q, ctrls));
+                if (kind[k] == K_RYY) c.push_back(std::make_shared<mindquantum::RyyGate>(a, obj1q, ctrls));
+                if (kind[k] == K_RXY) c.push_back(std::make_shared<mindquantum::RxyGate>(a, obj1q, ctrls));
+                if (kind[k] == K_RXZ) c.push_back(std::make_shared<mindquantum::RxzGate>(a, obj1q, ctrls));
+                if (kind[k] == K_RYZ) c.push_back(std::make_shared<mindquantum::RyzGate>(a, obj1q, ctrls));
+                if (kind[k] == K_GIVENS) c.push_back(std::make_shared<mindquantum::GivensGate>(a, obj1q, ctrls));
+                if (kind[k] == K_GP) c.push_back(std::make_shared<mindquantum::GPGate>(a, obj1q, ctrls));
+                if (kind[k] == K_SWAPALPHA) c.push_back(std::make_shared<mindquantum::SWAPalphaGate>(a, obj1q, ctrls));
+                break;
+            }
+            case K_U3:
+            case K_RN:
+            case K_FSIM: {
+                if (!ch) return {};
+                const double *a = ch + kCh * k;
+                const ParameterResolver a0 = angle_i(param[k], a, 0, names, sign);
+                const ParameterResolver a1 = angle_i(param[k], a, 1, names, sign);
+                const ParameterResolver a2 = angle_i(param[k], a, 2, names, sign);
+                // Hermitian forms (mindquantum/core/gates/basicgate.py): U3(-t, -l, -p), Rn(-a, -b, -g), FSim(-t, -p)
+                if (kind[k] == K_U3) {
+                    if (herm) c.push_back(std::make_shared<mindquantum::U3>(a0, a2, a1, obj1q, ctrls));
+                    else c.push_back(std::make_shared<mindquantum::U3>(a0, a1, a2, obj1q, ctrls));
+                }
+                if (kind[k] == K_RN) c.push_back(std::make_shared<mindquantum::Rn>(a0, a1, a2, obj1q, ctrls));
+                if (kind[k] == K_FSIM) c.push_back(std::make_shared<mindquantum::FSim>(a0, a1, obj1q, ctrls));
                 break;
             }
             default:
@@ -117,15 +186,16 @@ inline std::vector<std::string> param_names(int n_params) {
 // Apply the circuit to |0...0> with parameter values params[n_params]; out: 2^n complex128 (re, im).
 #define MQREF_APPLY_ARGS                                                                                            \
     int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl, const int *param,      \
-        const double *coeff, const double *cst, int n_params, const double *params, int threads, double *out
-#define MQREF_APPLY_PASS n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, n_params, params, threads, out
+        const double *coeff, const double *cst, const double *ch, int n_params, const double *params, int threads, \
+        double *out
+#define MQREF_APPLY_PASS n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, ch, n_params, params, threads, out
 
 template <typename sim_t>
 int apply_impl(MQREF_APPLY_ARGS) {
     try {
         if (threads > 0) omp_set_num_threads(threads);
         const auto names = param_names(n_params);
-        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false);
+        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false, ch);
         if (int(c.size()) != n_gates) return -1;
         ParameterResolver pr;
         for (int i = 0; i < n_params; ++i) pr.SetItem(names[i], params[i]);
@@ -180,11 +250,11 @@ int sample_impl(MQREF_SAMPLE_ARGS) {
 // out: [n_samples][1 + n_params] complex128 (re, im): f, then the gradient.
 #define MQREF_GRAD_ARGS                                                                                             \
     int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl, const int *param,      \
-        const double *coeff, const double *cst, int n_terms, const int *term_len, const int *term_q,               \
-        const char *term_p, const double *term_c, int n_params, int n_samples, const double *params, int threads, \
-        double *out
-#define MQREF_GRAD_PASS                                                                                           \
-    n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, n_terms, term_len, term_q, term_p, term_c, n_params, \
+        const double *coeff, const double *cst, const double *ch, int n_terms, const int *term_len,                \
+        const int *term_q, const char *term_p, const double *term_c, int n_params, int n_samples,                  \
+        const double *params, int threads, double *out
+#define MQREF_GRAD_PASS                                                                                               \
+    n, n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, ch, n_terms, term_len, term_q, term_p, term_c, n_params, \
         n_samples, params, threads, out
 
 // The Hamiltonian of a gradient call as the reference's type.
@@ -205,17 +275,11 @@ int grad_impl(MQREF_GRAD_ARGS) {
     try {
         if (threads > 0) omp_set_num_threads(threads);
         const auto names = param_names(n_params);
-        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false);
-        const circuit_t h = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, true);
+        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false, ch);
+        const circuit_t h = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, true, ch);
         if (int(c.size()) != n_gates || int(h.size()) != n_gates) return -1;
-        std::vector<mindquantum::PauliTerm<calc_t>> terms;
-        for (int t = 0, o = 0; t < n_terms; ++t) {
-            std::vector<mindquantum::PauliWord> w;
-            for (int k = 0; k < term_len[t]; ++k, ++o) w.emplace_back(Index(term_q[o]), term_p[o]);
-            terms.emplace_back(w, calc_t(term_c[t]));
-        }
         std::vector<std::shared_ptr<mindquantum::Hamiltonian<calc_t>>> hams{
-            std::make_shared<mindquantum::Hamiltonian<calc_t>>(terms)};
+            hamiltonian<calc_t>(n_terms, term_len, term_q, term_p, term_c)};
         std::vector<std::vector<calc_t>> enc(n_samples, std::vector<calc_t>(n_params));
         for (int s = 0; s < n_samples; ++s)
             for (int i = 0; i < n_params; ++i) enc[s][i] = calc_t(params[s * n_params + i]);

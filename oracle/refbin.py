@@ -4,8 +4,11 @@
 the CUDA path) to the reference itself, and bench.py's reference arm times them; the product never
 does.
 
-Supported gates: X, Y, Z, H (at most one control), RX, RY, RZ, Rzz and PhaseShift whose angle is
-``coeff * p + const`` of at most one parameter.  Hamiltonians: Pauli strings with real coefficients.
+Supported gates (at most one control, at most two object qubits): X, Y, Z, H, S, T, SX (and their
+daggers), SWAP, ISWAP (and its dagger), RX, RY, RZ, Rxx, Ryy, Rzz, Rxy, Rxz, Ryz, Givens, GlobalPhase,
+PhaseShift and SWAPalpha whose angle is ``coeff * p + const`` of at most one parameter; U3, Rn and
+FSim whose angles share at most one parameter; measurements; Pauli, depolarizing, amplitude- and
+phase-damping and thermal-relaxation channels.  Hamiltonians: Pauli strings with real coefficients.
 """
 import ctypes
 import os
@@ -15,7 +18,10 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref.so')
 GPU_LIB_PATH = os.path.join(_HERE, '_ref', 'libmqref_gpu.so')
-_KINDS = {'X': 0, 'H': 1, 'RX': 2, 'RY': 3, 'RZ': 4, 'Z': 5, 'Rzz': 6, 'Y': 7, 'PS': 8, 'M': 9}
+_KINDS = {'X': 0, 'H': 1, 'RX': 2, 'RY': 3, 'RZ': 4, 'Z': 5, 'Rzz': 6, 'Y': 7, 'PS': 8, 'M': 9, 'SWAP': 18,
+          'Rxx': 20, 'Ryy': 21, 'Rxy': 22, 'Rxz': 23, 'Ryz': 24, 'G': 25, 'GP': 26, 'SWAPalpha': 27}
+_FLAGGED = {'S': 15, 'T': 16, 'SX': 17, 'ISWAP': 19}
+_MULTI = {'U3': 28, 'Rn': 29, 'FSim': 30}
 _CHANNELS = {'PC': 10, 'BFC': 10, 'PFC': 10, 'BPFC': 10, 'DC': 11, 'ADC': 12, 'PDC': 13, 'TRC': 14}
 
 
@@ -44,60 +50,68 @@ def lib(device='cpu'):
         L = ctypes.CDLL(path)
         P = ctypes.c_void_p
         pre = 'mqref_gpu_' if device == 'gpu' else 'mqref_'
-        getattr(L, pre + 'apply').argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, ctypes.c_int,
+        getattr(L, pre + 'apply').argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 8 + [ctypes.c_int, P, ctypes.c_int,
                                                                                       P]
         if device == 'cpu':
             L.mqref_sample.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 8 + [ctypes.c_int, P, ctypes.c_int,
                                                                             ctypes.c_uint, ctypes.c_int, P]
         for fn in (getattr(L, pre + 'grad'), getattr(L, pre + 'grad_c64')):
-            fn.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 7 + [ctypes.c_int, P, P, P, P, ctypes.c_int,
+            fn.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 8 + [ctypes.c_int, P, P, P, P, ctypes.c_int,
                                                                     ctypes.c_int, P, ctypes.c_int, P]
         _libs[device] = (L, pre)
     return _libs[device]
 
 
+def _angle(pr, names):
+    """(param index or -1, coefficient, constant) of an angle of at most one parameter."""
+    keys = list(pr.params_name)
+    if len(keys) > 1:
+        raise ValueError("one parameter per angle")
+    if not keys:
+        return -1, 0.0, float(np.real(pr.const))
+    return names.index(keys[0]), float(np.real(pr[keys[0]])), float(np.real(pr.const))
+
+
 def _gate_table(circ, names, mkeys=None):
     """Columns of the harness's gate table; measurement gates take the index of their key in
-    ``mkeys`` (appended to in circuit order) as their param column."""
+    ``mkeys`` (appended to in circuit order) as their param column.  ``ch`` holds six values per
+    gate: channel arguments, the daggered flag of S / T / SX / ISWAP, or the constants and
+    coefficients of the angles of U3 / Rn / FSim (which share one parameter)."""
     cols = {k: [] for k in ('kind', 'o0', 'o1', 'ctrl', 'param', 'coeff', 'cst', 'ch')}
+
+    def row(kind, g, param=-1, coeff=0.0, cst=0.0, ch=(0.0,) * 6):
+        if len(g.obj_qubits) > 2 or len(g.ctrl_qubits) > 1:
+            raise ValueError(f"gate {g.name} on {g.obj_qubits} / {g.ctrl_qubits} is not supported by the harness")
+        for k, v in (('kind', kind), ('o0', int(g.obj_qubits[0]) if len(g.obj_qubits) else 0),
+                     ('o1', int(g.obj_qubits[1]) if len(g.obj_qubits) > 1 else -1),
+                     ('ctrl', int(g.ctrl_qubits[0]) if g.ctrl_qubits else -1), ('param', param), ('coeff', coeff),
+                     ('cst', cst)):
+            cols[k].append(v)
+        cols['ch'].extend(list(ch) + [0.0] * (6 - len(ch)))
+
     for g in circ:
         if g.name in _CHANNELS:
-            if len(g.obj_qubits) > 2 or len(g.ctrl_qubits) > 1:
-                raise ValueError(f"channel {g.name} on {g.obj_qubits} is not supported by the reference harness")
-            for k, v in (('kind', _CHANNELS[g.name]), ('o0', int(g.obj_qubits[0])),
-                         ('o1', int(g.obj_qubits[1]) if len(g.obj_qubits) > 1 else -1),
-                         ('ctrl', int(g.ctrl_qubits[0]) if g.ctrl_qubits else -1), ('param', -1), ('coeff', 0.0),
-                         ('cst', 0.0)):
-                cols[k].append(v)
-            cols['ch'].extend(_channel_args(g))
-            continue
-        cols['ch'].extend([0.0, 0.0, 0.0])
-        if g.name == 'M' and mkeys is not None:
+            row(_CHANNELS[g.name], g, ch=_channel_args(g))
+        elif g.name == 'M' and mkeys is not None:
             mkeys.append(g.key)
-            for k, v in (('kind', _KINDS['M']), ('o0', int(g.obj_qubits[0])), ('o1', -1), ('ctrl', -1),
-                         ('param', len(mkeys) - 1), ('coeff', 0.0), ('cst', 0.0)):
-                cols[k].append(v)
-            continue
-        name = 'PS' if g.name in ('PS', 'PhaseShift') else g.name
-        if name not in _KINDS or len(g.ctrl_qubits) > 1:
-            raise ValueError(f"gate {g.name} is not supported by the reference harness")
-        cols['kind'].append(_KINDS[name])
-        cols['o0'].append(int(g.obj_qubits[0]))
-        cols['o1'].append(int(g.obj_qubits[1]) if len(g.obj_qubits) > 1 else -1)
-        cols['ctrl'].append(int(g.ctrl_qubits[0]) if g.ctrl_qubits else -1)
-        prs = getattr(g, 'prs', None)
-        if prs:
-            pr = prs[0]
-            keys = list(pr.params_name)
-            if len(keys) > 1:
-                raise ValueError("one parameter per angle")
-            cols['param'].append(names.index(keys[0]) if keys else -1)
-            cols['coeff'].append(float(np.real(pr[keys[0]])) if keys else 0.0)
-            cols['cst'].append(float(np.real(pr.const)))
+            row(_KINDS['M'], g, param=len(mkeys) - 1)
+        elif g.name in _FLAGGED:
+            row(_FLAGGED[g.name], g, ch=(1.0 if g.hermitianed else 0.0,))
+        elif g.name in _MULTI:
+            ang = [_angle(pr, names) for pr in g.prs]
+            params = {a[0] for a in ang if a[0] >= 0}
+            if len(params) > 1:
+                raise ValueError(f"{g.name}: the angles must share one parameter")
+            pi = params.pop() if params else -1
+            ch = [a[2] for a in ang] + [0.0] * (3 - len(ang)) + [a[1] for a in ang]
+            row(_MULTI[g.name], g, param=pi, ch=ch)
         else:
-            cols['param'].append(-1)
-            cols['coeff'].append(0.0)
-            cols['cst'].append(0.0)
+            name = 'PS' if g.name in ('PS', 'PhaseShift') else g.name
+            if name not in _KINDS:
+                raise ValueError(f"gate {g.name} is not supported by the reference harness")
+            prs = getattr(g, 'prs', None)
+            pi, coeff, cst = _angle(prs[0], names) if prs else (-1, 0.0, 0.0)
+            row(_KINDS[name], g, param=pi, coeff=coeff, cst=cst)
     ints = {k: np.ascontiguousarray(cols[k], dtype=np.int32) for k in ('kind', 'o0', 'o1', 'ctrl', 'param')}
     dbls = {k: np.ascontiguousarray(cols[k] if cols[k] else [0.0], dtype=np.float64) for k in ('coeff', 'cst', 'ch')}
     return ints, dbls
@@ -116,7 +130,8 @@ def apply(n, circ, params, threads=0, device='cpu'):
     p = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
     L, pre = lib(device)
     st = getattr(L, pre + 'apply')(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
-                           _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), len(names), _p(p), threads, _p(out))
+                           _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), _p(dbls['ch']), len(names), _p(p),
+                           threads, _p(out))
     if st != 0:
         raise RuntimeError(f"mqref_apply failed ({st})")
     return out[0::2] + 1j * out[1::2]
@@ -145,7 +160,8 @@ def grad(n, circ, ham, params, threads=0, complex64=False, device='cpu'):
     L, pre = lib(device)
     fn = getattr(L, pre + ('grad_c64' if complex64 else 'grad'))
     st = fn(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']), _p(ints['param']),
-            _p(dbls['coeff']), _p(dbls['cst']), len(tl), _p(tl), _p(tq), ctypes.cast(tpb, ctypes.c_void_p), _p(tc),
+            _p(dbls['coeff']), _p(dbls['cst']), _p(dbls['ch']), len(tl), _p(tl), _p(tq), ctypes.cast(tpb, ctypes.c_void_p),
+            _p(tc),
             len(names), S, _p(params), threads, _p(out))
     if st != 0:
         raise RuntimeError(f"mqref_grad failed ({st})")

@@ -6,7 +6,9 @@ restatement to it on the benchmark circuit families at full size where the host 
 seconds: config 1 exactly (16 qubits x 8 layers), the QNN encoder/ansatz, QAOA MaxCut and random
 Pauli Hamiltonians with Y terms.  Tolerance: 1e-12 (both FP64), complex64 reference within 1e-5.
 Both samplers (measurement-ending and mid-circuit) and the noise channels' trajectories are pinned
-shot for shot for the same seed.
+shot for shot for the same seed; random circuits of every gate kind pin the gate formulas,
+Hermitian conjugates and Jacobians; the dense density-matrix oracle is pinned to the reference's
+DensityMatrixState.
 Skipped where the reference checkout was not available to build the library.
 
 The reference's thrust GPU simulator (`mqvector_gpu`, VectorState<GPUVectorPolicyDouble/Float>,
@@ -214,3 +216,63 @@ def test_density_matrix_thermal_relaxation_gradient_is_the_derivative():
                    for e in np.eye(len(names))[:, None, :]])
     assert np.max(np.abs(orc - fd)) <= 1e-8
     assert np.max(np.abs(ref - fd)) > 1e-3     # the reference's divergence (0.028 on 'u' here)
+
+
+def _every_gate_circuit(n, n_gates, seed):
+    """Random gates of every kind the reference's VectorState applies: fixed one- and two-qubit
+    gates and their daggers, one-parameter rotations, U3 / Rn / FSim with angles sharing a
+    parameter, controls on a third of them; angles coeff * p + const."""
+    from mindquantum_b200.core import gates as G
+    from mindquantum_b200.core.circuit import Circuit
+    from mindquantum_b200.core.parameterresolver import ParameterResolver
+
+    rng = np.random.default_rng(seed)
+    names = [f'p{i}' for i in range(6)]
+
+    def pr(k):
+        return ParameterResolver({k: float(rng.uniform(0.5, 2))}, const=float(rng.uniform(-1, 1)))
+
+    one = [G.X, G.Y, G.Z, G.H, G.S, G.T, G.SX]
+    p1 = [G.RX, G.RY, G.RZ, G.PhaseShift, G.GlobalPhase]
+    p2 = [G.Rxx, G.Ryy, G.Rzz, G.Rxy, G.Rxz, G.Ryz, G.Givens, G.SWAPalpha]
+    circ = Circuit()
+    for _ in range(n_gates):
+        q = [int(x) for x in rng.permutation(n)[:3]]
+        kind = int(rng.integers(7))
+        ctrl = [q[2]] if rng.random() < 0.3 else []
+        k = names[int(rng.integers(len(names)))]
+        if kind == 0:
+            g = one[int(rng.integers(len(one)))]
+            circ += (g.hermitian() if rng.random() < 0.5 else g).on(q[0], ctrl)
+        elif kind == 1:
+            g = (G.SWAP, G.ISWAP)[int(rng.integers(2))]
+            circ += (g.hermitian() if rng.random() < 0.5 else g).on(q[:2], ctrl)
+        elif kind == 2:
+            circ += p1[int(rng.integers(len(p1)))](pr(k)).on(q[0], ctrl)
+        elif kind == 3:
+            circ += p2[int(rng.integers(len(p2)))](pr(k)).on(q[:2], ctrl)
+        elif kind == 4:
+            circ += G.U3(pr(k), pr(k), pr(k)).on(q[0], ctrl)
+        elif kind == 5:
+            circ += G.Rn(pr(k), pr(k), pr(k)).on(q[0], ctrl)
+        else:
+            circ += G.FSim(pr(k), pr(k)).on(q[:2], ctrl)
+    return circ
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_every_gate_kind_oracle_equals_reference(seed):
+    """The oracle's gate formulas, Hermitian conjugates and Jacobians against the reference's own
+    ApplyCircuit and adjoint gradient on a random 120-gate circuit of every gate kind at 8 qubits
+    (amplitudes 1e-12, f and gradients 1e-12)."""
+    n = 8
+    circ = _every_gate_circuit(n, 120, seed)
+    names = list(circ.params_name)
+    vals = np.random.default_rng(seed).uniform(0, 2 * np.pi, len(names))
+    qs = R.apply(n, circ, vals)
+    oqs = O.OracleSim(n).apply_circuit(circ, dict(zip(names, vals.tolist()))).qs
+    assert np.max(np.abs(qs - oqs)) <= 1e-12
+    ham = W.random_pauli_hamiltonian(n, 12, np.random.default_rng(seed + 100))
+    ref = R.grad(n, circ, ham, vals[None, :])
+    orc = O.get_expectation_with_grad(n, [ham], circ, vals[None, :], np.zeros(0), names, [])[:, 0]
+    assert np.max(np.abs(ref - orc)) <= 1e-12
