@@ -42,6 +42,9 @@ int mqref_grad(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_d, double>(MQREF_G
 // complex64 (CPUVectorPolicyAvxFloat)
 int mqref_grad_c64(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_f, float>(MQREF_GRAD_PASS); }
 
+// the parameter-shift gradient, complex128
+int mqref_grad_pshift(MQREF_GRAD_ARGS) { return mqref::pshift_impl<sim_d, double>(MQREF_GRAD_PASS); }
+
 // The reference's density-matrix simulator (DensityMatrixState<CPUDensityMatrixPolicyAvxDouble>,
 // ccsrc/include/simulator/densitymatrix/densitymatrix_state.tpp), complex128: the circuit (gates and
 // channels, table as in mqref_sample, measurements not allowed) applied to |0><0|; out: rho as

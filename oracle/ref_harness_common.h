@@ -7,6 +7,7 @@
 //   apply_impl: VectorState::ApplyCircuit + GetQS (ccsrc/include/simulator/vector/vector_state.tpp:949-960);
 //   sample_impl: VectorState::SamplingMeasurementEndingWithoutNoise / Sampling (vector_state.tpp:1308-1373),
 //                the reference's seeded shot streams;
+//   pshift_impl: GetExpectationWithGradParameterShiftMultiMulti (vector_state.tpp:1033-1305);
 //   grad_impl:  VectorState::GetExpectationWithGradMultiMulti (the adjoint gradient,
 //               ccsrc/include/simulator/vector/gradient.h:100-197), with the Hermitian circuit
 //               built the way the reference's Python builds it (mindquantum/core/circuit/
@@ -285,6 +286,34 @@ int grad_impl(MQREF_GRAD_ARGS) {
             for (int i = 0; i < n_params; ++i) enc[s][i] = calc_t(params[s * n_params + i]);
         sim_t sim{static_cast<Index>(n)};
         const auto res = sim.GetExpectationWithGradMultiMulti(hams, c, h, enc, {}, names, {}, 1, 1);
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i <= n_params; ++i) {
+                out[2 * (s * (n_params + 1) + i)] = double(res[s][0][i].real());
+                out[2 * (s * (n_params + 1) + i) + 1] = double(res[s][0][i].imag());
+            }
+        return 0;
+    } catch (...) {
+        return -2;
+    }
+}
+
+// The parameter-shift gradient, as MQSim.get_expectation_with_grad(..., pr_shift=True) calls it
+// (GetExpectationWithGradParameterShiftMultiMulti, vector_state.tpp:1033-1305): same arguments and
+// output as grad_impl; the simulator keeps the reference's default seed (42).
+template <typename sim_t, typename calc_t>
+int pshift_impl(MQREF_GRAD_ARGS) {
+    try {
+        if (threads > 0) omp_set_num_threads(threads);
+        const auto names = param_names(n_params);
+        const circuit_t c = build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false, ch);
+        if (int(c.size()) != n_gates) return -1;
+        std::vector<std::shared_ptr<mindquantum::Hamiltonian<calc_t>>> hams{
+            hamiltonian<calc_t>(n_terms, term_len, term_q, term_p, term_c)};
+        std::vector<std::vector<calc_t>> enc(n_samples, std::vector<calc_t>(n_params));
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i < n_params; ++i) enc[s][i] = calc_t(params[s * n_params + i]);
+        sim_t sim{static_cast<Index>(n)};
+        const auto res = sim.GetExpectationWithGradParameterShiftMultiMulti(hams, c, enc, {}, names, {}, 1, 1);
         for (int s = 0; s < n_samples; ++s)
             for (int i = 0; i <= n_params; ++i) {
                 out[2 * (s * (n_params + 1) + i)] = double(res[s][0][i].real());

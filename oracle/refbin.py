@@ -137,7 +137,13 @@ def apply(n, circ, params, threads=0, device='cpu'):
     return out[0::2] + 1j * out[1::2]
 
 
-def grad(n, circ, ham, params, threads=0, complex64=False, device='cpu'):
+def grad_pshift(n, circ, ham, params, threads=0):
+    """The reference's parameter-shift gradient (GetExpectationWithGradParameterShiftMultiMulti,
+    complex128, CPU), every parameter an encoder input: [samples][1 + n_params] complex."""
+    return grad(n, circ, ham, params, threads=threads, _entry='grad_pshift')
+
+
+def grad(n, circ, ham, params, threads=0, complex64=False, device='cpu', _entry=None):
     """VectorState::GetExpectationWithGradMultiMulti for one Hamiltonian, every parameter an encoder
     input: params [samples][n_params] -> [samples][1 + n_params] complex (f, then the gradient), on
     the reference's CPU (``device='cpu'``) or thrust GPU (``device='gpu'``) policy."""
@@ -158,7 +164,10 @@ def grad(n, circ, ham, params, threads=0, complex64=False, device='cpu'):
     S = params.shape[0]
     out = np.zeros(S * (1 + len(names)) * 2, dtype=np.float64)
     L, pre = lib(device)
-    fn = getattr(L, pre + ('grad_c64' if complex64 else 'grad'))
+    fn = getattr(L, pre + (_entry or ('grad_c64' if complex64 else 'grad')))
+    if _entry:
+        fn.argtypes = L.mqref_grad.argtypes
+        fn.restype = ctypes.c_int
     st = fn(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']), _p(ints['param']),
             _p(dbls['coeff']), _p(dbls['cst']), _p(dbls['ch']), len(tl), _p(tl), _p(tq), ctypes.cast(tpb, ctypes.c_void_p),
             _p(tc),

@@ -218,7 +218,7 @@ def test_density_matrix_thermal_relaxation_gradient_is_the_derivative():
     assert np.max(np.abs(ref - fd)) > 1e-3     # the reference's divergence (0.028 on 'u' here)
 
 
-def _every_gate_circuit(n, n_gates, seed):
+def _every_gate_circuit(n, n_gates, seed, with_rn=True):
     """Random gates of every kind the reference's VectorState applies: fixed one- and two-qubit
     gates and their daggers, one-parameter rotations, U3 / Rn / FSim with angles sharing a
     parameter, controls on a third of them; angles coeff * p + const."""
@@ -239,6 +239,8 @@ def _every_gate_circuit(n, n_gates, seed):
     for _ in range(n_gates):
         q = [int(x) for x in rng.permutation(n)[:3]]
         kind = int(rng.integers(7))
+        if kind == 5 and not with_rn:
+            kind = 4
         ctrl = [q[2]] if rng.random() < 0.3 else []
         k = names[int(rng.integers(len(names)))]
         if kind == 0:
@@ -276,3 +278,18 @@ def test_every_gate_kind_oracle_equals_reference(seed):
     ref = R.grad(n, circ, ham, vals[None, :])
     orc = O.get_expectation_with_grad(n, [ham], circ, vals[None, :], np.zeros(0), names, [])[:, 0]
     assert np.max(np.abs(ref - orc)) <= 1e-12
+
+
+def test_parameter_shift_oracle_equals_reference():
+    """The oracle's parameter-shift loop against the reference's own
+    GetExpectationWithGradParameterShiftMultiMulti on random circuits of every gate kind that rule
+    supports (Rn is refused there), two parameter rows, angles sharing parameters (where the
+    reference's shift rule departs from the derivative, the oracle follows it): 1e-11."""
+    n = 6
+    circ = _every_gate_circuit(n, 40, 9, with_rn=False)
+    names = list(circ.params_name)
+    vals = np.random.default_rng(1).uniform(0, 2 * np.pi, (2, len(names)))
+    ham = W.random_pauli_hamiltonian(n, 8, np.random.default_rng(2))
+    ref = R.grad_pshift(n, circ, ham, vals)
+    orc = O.get_expectation_with_grad_parameter_shift(n, [ham], circ, vals, [], names, [])[:, 0]
+    assert np.max(np.abs(ref - orc)) <= 1e-11
