@@ -45,6 +45,88 @@ int mqref_grad_c64(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_f, float>(MQRE
 // the parameter-shift gradient, complex128
 int mqref_grad_pshift(MQREF_GRAD_ARGS) { return mqref::pshift_impl<sim_d, double>(MQREF_GRAD_PASS); }
 
+// The QRAM gradient (QramExpectationWithGrad, vector_state.tpp:1010-1018; gradient.h
+// QramHermitianAdjointGradient), complex128: one ansatz (every parameter an ansatz input, values
+// params[n_params]) applied to n_samples initial states init[n_samples][2^n] complex128 (re, im).
+// out: [n_samples][1 + n_params] complex128 (re, im).
+int mqref_grad_qram(int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl,
+                    const int *param, const double *coeff, const double *cst, const double *ch, int n_terms,
+                    const int *term_len, const int *term_q, const char *term_p, const double *term_c, int n_params,
+                    int n_samples, const double *params, const double *init, double *out) {
+    try {
+        const auto names = mqref::param_names(n_params);
+        const auto c = mqref::build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false, ch);
+        const auto h = mqref::build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, true, ch);
+        if (int(c.size()) != n_gates || int(h.size()) != n_gates) return -1;
+        std::vector<std::shared_ptr<mindquantum::Hamiltonian<double>>> hams{
+            mqref::hamiltonian<double>(n_terms, term_len, term_q, term_p, term_c)};
+        const size_t d = size_t(1) << n;
+        std::vector<std::vector<std::complex<double>>> states(n_samples, std::vector<std::complex<double>>(d));
+        for (int s = 0; s < n_samples; ++s)
+            for (size_t i = 0; i < d; ++i) states[s][i] = {init[2 * (s * d + i)], init[2 * (s * d + i) + 1]};
+        const std::vector<double> ans(params, params + n_params);
+        sim_d sim{static_cast<mindquantum::Index>(n)};
+        const auto res = sim.QramExpectationWithGrad(hams, c, h, states, ans, names, 1, 1);
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i <= n_params; ++i) {
+                out[2 * (s * (n_params + 1) + i)] = res[s][0][i].real();
+                out[2 * (s * (n_params + 1) + i) + 1] = res[s][0][i].imag();
+            }
+        return 0;
+    } catch (...) {
+        return -2;
+    }
+}
+
+// The non-Hermitian gradient <phi| U_l^dag H U_r(p) |psi> of MQSim.get_expectation_with_grad with
+// circ_left and simulator_left (GetExpectationNonHermitianWithGradMultiMulti,
+// vector_state.tpp:998-1008; gradient.h NonHermitianAdjointGradient), complex128: the right
+// circuit is table r_*, the left one table l_* (both with channel-free gates, the left one's
+// parameters fixed), psi and phi given as 2^n complex128 (re, im) amplitudes, every parameter of
+// the right circuit an encoder input.  out: [n_samples][1 + n_params] complex128 (re, im).
+int mqref_grad_nonherm(int n, int r_gates, const int *r_kind, const int *r_obj0, const int *r_obj1, const int *r_ctrl,
+                       const int *r_param, const double *r_coeff, const double *r_cst, const double *r_ch, int l_gates,
+                       const int *l_kind, const int *l_obj0, const int *l_obj1, const int *l_ctrl, const int *l_param,
+                       const double *l_coeff, const double *l_cst, const double *l_ch, const double *psi,
+                       const double *phi, int n_terms, const int *term_len, const int *term_q, const char *term_p,
+                       const double *term_c, int n_params, int n_samples, const double *params, double *out) {
+    try {
+        const auto names = mqref::param_names(n_params);
+        const std::vector<std::string> none;
+        using mqref::build;
+        const auto rc = build(r_gates, r_kind, r_obj0, r_obj1, r_ctrl, r_param, r_coeff, r_cst, names, false, r_ch);
+        const auto rh = build(r_gates, r_kind, r_obj0, r_obj1, r_ctrl, r_param, r_coeff, r_cst, names, true, r_ch);
+        const auto lc = build(l_gates, l_kind, l_obj0, l_obj1, l_ctrl, l_param, l_coeff, l_cst, none, false, l_ch);
+        const auto lh = build(l_gates, l_kind, l_obj0, l_obj1, l_ctrl, l_param, l_coeff, l_cst, none, true, l_ch);
+        if (int(rc.size()) != r_gates || int(lc.size()) != l_gates) return -1;
+        std::vector<std::shared_ptr<mindquantum::Hamiltonian<double>>> hams{
+            mqref::hamiltonian<double>(n_terms, term_len, term_q, term_p, term_c)};
+        const size_t d = size_t(1) << n;
+        std::vector<std::complex<double>> vpsi(d), vphi(d);
+        for (size_t i = 0; i < d; ++i) {
+            vpsi[i] = {psi[2 * i], psi[2 * i + 1]};
+            vphi[i] = {phi[2 * i], phi[2 * i + 1]};
+        }
+        sim_d right{static_cast<mindquantum::Index>(n)};
+        sim_d left{static_cast<mindquantum::Index>(n)};
+        right.SetQS(vpsi);
+        left.SetQS(vphi);
+        std::vector<std::vector<double>> enc(n_samples, std::vector<double>(n_params));
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i < n_params; ++i) enc[s][i] = params[s * n_params + i];
+        const auto res =
+            right.GetExpectationNonHermitianWithGradMultiMulti(hams, hams, lc, lh, rc, rh, enc, {}, names, {}, left, 1, 1);
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i <= n_params; ++i) {
+                out[2 * (s * (n_params + 1) + i)] = res[s][0][i].real();
+                out[2 * (s * (n_params + 1) + i) + 1] = res[s][0][i].imag();
+            }
+        return 0;
+    } catch (...) {
+        return -2;
+    }
+}
+
 // The reference's density-matrix simulator (DensityMatrixState<CPUDensityMatrixPolicyAvxDouble>,
 // ccsrc/include/simulator/densitymatrix/densitymatrix_state.tpp), complex128: the circuit (gates and
 // channels, table as in mqref_sample, measurements not allowed) applied to |0><0|; out: rho as

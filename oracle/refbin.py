@@ -249,3 +249,56 @@ def dm_grad(n, circ, ham, params):
         raise RuntimeError(f"mqref_dm_grad failed ({st})")
     out = out.reshape(S, 1 + len(names), 2)
     return out[..., 0] + 1j * out[..., 1]
+
+
+def grad_nonherm(n, circ, circ_left, ham, params, psi, phi):
+    """The reference's non-Hermitian gradient <phi| U_l^dag H U_r(p) |psi>
+    (GetExpectationNonHermitianWithGradMultiMulti, complex128, CPU) with ``circ_left`` fixed and the
+    right circuit's parameters as encoder inputs: params [samples][n_params] ->
+    [samples][1 + n_params] complex (f, then the gradient)."""
+    names = list(circ.params_name)
+    ri, rd = _gate_table(circ, names)
+    li, ld = _gate_table(circ_left, [])
+    tl, tq, tpb, tc = _ham_arrays(ham)
+    params = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
+    S = params.shape[0]
+    cplx = lambda v: np.ascontiguousarray(np.stack([np.real(v), np.imag(v)], axis=-1).reshape(-1))  # noqa: E731
+    psi_a, phi_a = cplx(np.asarray(psi, dtype=np.complex128)), cplx(np.asarray(phi, dtype=np.complex128))
+    out = np.zeros(S * (1 + len(names)) * 2, dtype=np.float64)
+    L, _ = lib('cpu')
+    P, I = ctypes.c_void_p, ctypes.c_int
+    L.mqref_grad_nonherm.argtypes = ([I, I] + [P] * 8 + [I] + [P] * 8 + [P, P, I, P, P, P, P, I, I, P, P])
+    tab = lambda i, d: [_p(i['kind']), _p(i['o0']), _p(i['o1']), _p(i['ctrl']), _p(i['param']),  # noqa: E731
+                        _p(d['coeff']), _p(d['cst']), _p(d['ch'])]
+    st = L.mqref_grad_nonherm(n, len(ri['kind']), *tab(ri, rd), len(li['kind']), *tab(li, ld), _p(psi_a), _p(phi_a),
+                              len(tl), _p(tl), _p(tq), ctypes.cast(tpb, ctypes.c_void_p), _p(tc), len(names), S,
+                              _p(params), _p(out))
+    if st != 0:
+        raise RuntimeError(f"mqref_grad_nonherm failed ({st})")
+    out = out.reshape(S, 1 + len(names), 2)
+    return out[..., 0] + 1j * out[..., 1]
+
+
+def grad_qram(n, circ, ham, ans, init_states):
+    """The reference's QRAM gradient (QramExpectationWithGrad, complex128, CPU): the ansatz with
+    values ``ans`` applied to every row of ``init_states`` [samples][2^n]; returns
+    [samples][1 + n_params] complex (f, then the ansatz gradient)."""
+    names = list(circ.params_name)
+    ints, dbls = _gate_table(circ, names)
+    tl, tq, tpb, tc = _ham_arrays(ham)
+    init = np.asarray(init_states, dtype=np.complex128)
+    S = init.shape[0]
+    init_a = np.ascontiguousarray(np.stack([init.real, init.imag], axis=-1).reshape(-1))
+    p = np.ascontiguousarray(ans if len(names) else [0.0], dtype=np.float64).reshape(-1)
+    out = np.zeros(S * (1 + len(names)) * 2, dtype=np.float64)
+    L, _ = lib('cpu')
+    P, I = ctypes.c_void_p, ctypes.c_int
+    L.mqref_grad_qram.argtypes = [I, I] + [P] * 8 + [I, P, P, P, P, I, I, P, P, P]
+    st = L.mqref_grad_qram(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
+                           _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), _p(dbls['ch']), len(tl), _p(tl),
+                           _p(tq), ctypes.cast(tpb, ctypes.c_void_p), _p(tc), len(names), S, _p(p), _p(init_a),
+                           _p(out))
+    if st != 0:
+        raise RuntimeError(f"mqref_grad_qram failed ({st})")
+    out = out.reshape(S, 1 + len(names), 2)
+    return out[..., 0] + 1j * out[..., 1]

@@ -7,8 +7,9 @@ seconds: config 1 exactly (16 qubits x 8 layers), the QNN encoder/ansatz, QAOA M
 Pauli Hamiltonians with Y terms.  Tolerance: 1e-12 (both FP64), complex64 reference within 1e-5.
 Both samplers (measurement-ending and mid-circuit) and the noise channels' trajectories are pinned
 shot for shot for the same seed; random circuits of every gate kind pin the gate formulas,
-Hermitian conjugates and Jacobians; the dense density-matrix oracle is pinned to the reference's
-DensityMatrixState.
+Hermitian conjugates and Jacobians; the parameter-shift loop, the QRAM gradient and the
+non-Hermitian gradient's convention are pinned to the reference's own entry points; the dense
+density-matrix oracle is pinned to the reference's DensityMatrixState.
 Skipped where the reference checkout was not available to build the library.
 
 The reference's thrust GPU simulator (`mqvector_gpu`, VectorState<GPUVectorPolicyDouble/Float>,
@@ -218,7 +219,7 @@ def test_density_matrix_thermal_relaxation_gradient_is_the_derivative():
     assert np.max(np.abs(ref - fd)) > 1e-3     # the reference's divergence (0.028 on 'u' here)
 
 
-def _every_gate_circuit(n, n_gates, seed, with_rn=True):
+def _every_gate_circuit(n, n_gates, seed, with_rn=True, fixed=False):
     """Random gates of every kind the reference's VectorState applies: fixed one- and two-qubit
     gates and their daggers, one-parameter rotations, U3 / Rn / FSim with angles sharing a
     parameter, controls on a third of them; angles coeff * p + const."""
@@ -230,6 +231,8 @@ def _every_gate_circuit(n, n_gates, seed, with_rn=True):
     names = [f'p{i}' for i in range(6)]
 
     def pr(k):
+        if fixed:   # numeric angles only
+            return float(rng.uniform(-3, 3))
         return ParameterResolver({k: float(rng.uniform(0.5, 2))}, const=float(rng.uniform(-1, 1)))
 
     one = [G.X, G.Y, G.Z, G.H, G.S, G.T, G.SX]
@@ -293,3 +296,48 @@ def test_parameter_shift_oracle_equals_reference():
     ref = R.grad_pshift(n, circ, ham, vals)
     orc = O.get_expectation_with_grad_parameter_shift(n, [ham], circ, vals, [], names, [])[:, 0]
     assert np.max(np.abs(ref - orc)) <= 1e-11
+
+
+def test_non_hermitian_gradient_convention_of_the_reference():
+    """<phi| U_l^dag H U_r(p) |psi> with circ_left and simulator_left: the reference's own
+    GetExpectationNonHermitianWithGradMultiMulti returns f (complex, equal to the oracle's states
+    and Hamiltonian within 1e-12) and the complex derivative df/dp (central differences of the
+    oracle's f, 1e-7), the quantity the B200 backend's non-Hermitian GPU tests expect."""
+    n = 5
+    rng = np.random.default_rng(3)
+    circ = _every_gate_circuit(n, 30, 11)
+    left = _every_gate_circuit(n, 20, 12, fixed=True)
+    names = list(circ.params_name)
+    vals = rng.uniform(0, 2 * np.pi, (1, len(names)))
+    psi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    phi = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi, phi = psi / np.linalg.norm(psi), phi / np.linalg.norm(phi)
+    ham = W.random_pauli_hamiltonian(n, 8, np.random.default_rng(4))
+    ref = R.grad_nonherm(n, circ, left, ham, vals, psi, phi)[0]
+    bra = O.OracleSim(n, state=phi).apply_circuit(left, {}).qs
+
+    def f(p):
+        ket = O.OracleSim(n, state=psi).apply_circuit(circ, dict(zip(names, p.tolist()))).qs
+        return np.vdot(bra, O.apply_terms(ket, n, ham))
+
+    assert abs(ref[0] - f(vals[0])) <= 1e-12
+    h = 1e-6
+    fd = np.array([(f(vals[0] + h * e) - f(vals[0] - h * e)) / (2 * h) for e in np.eye(len(names))])
+    assert np.max(np.abs(ref[1:] - fd)) <= 1e-7
+
+
+def test_qram_oracle_equals_reference():
+    """Per-sample initial states through one ansatz: the oracle's driver with an initial state
+    against the reference's own QramExpectationWithGrad (1e-12), on a circuit of every gate kind."""
+    n = 5
+    rng = np.random.default_rng(23)
+    circ = _every_gate_circuit(n, 30, 13)
+    names = list(circ.params_name)
+    ans = rng.uniform(0, 2 * np.pi, len(names))
+    qs = rng.normal(size=(3, 1 << n)) + 1j * rng.normal(size=(3, 1 << n))
+    qs /= np.linalg.norm(qs, axis=1, keepdims=True)
+    ham = W.random_pauli_hamiltonian(n, 8, np.random.default_rng(24))
+    ref = R.grad_qram(n, circ, ham, ans, qs)
+    for s in range(3):
+        orc = O.get_expectation_with_grad(n, [ham], circ, np.zeros((1, 0)), ans, [], names, np.complex128, qs[s])
+        assert np.max(np.abs(ref[s] - orc[0, 0])) <= 1e-12
