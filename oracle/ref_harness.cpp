@@ -45,6 +45,48 @@ int mqref_grad_c64(MQREF_GRAD_ARGS) { return mqref::grad_impl<sim_f, float>(MQRE
 // the parameter-shift gradient, complex128
 int mqref_grad_pshift(MQREF_GRAD_ARGS) { return mqref::pshift_impl<sim_d, double>(MQREF_GRAD_PASS); }
 
+// <H> and its gradient for a Hamiltonian given as a sparse matrix (mindquantum/core/operators/
+// hamiltonian.py get_cpp_obj: the scipy CSR arrays as a CsrHdMatrix, Hamiltonian(csr, n); the
+// simulator then takes ExpectationOfCsr / Csr_Dot_Vec), complex128, every parameter an encoder
+// input: the CSR rows indptr[2^n + 1], indices[nnz], data[nnz] complex128 (re, im).
+int mqref_grad_csr(int n, int n_gates, const int *kind, const int *obj0, const int *obj1, const int *ctrl,
+                   const int *param, const double *coeff, const double *cst, const double *ch, int64_t nnz,
+                   const int64_t *indptr, const int64_t *indices, const double *data, int n_params, int n_samples,
+                   const double *params, double *out) {
+    try {
+        const auto names = mqref::param_names(n_params);
+        const auto c = mqref::build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, false, ch);
+        const auto h = mqref::build(n_gates, kind, obj0, obj1, ctrl, param, coeff, cst, names, true, ch);
+        if (int(c.size()) != n_gates || int(h.size()) != n_gates) return -1;
+        const size_t d = size_t(1) << n;
+        // the matrix owns malloc'd copies (CsrHdMatrix::FreeMemory frees them)
+        auto *ip = static_cast<mindquantum::Index *>(malloc(sizeof(mindquantum::Index) * (d + 1)));
+        auto *ix = static_cast<mindquantum::Index *>(malloc(sizeof(mindquantum::Index) * std::max<int64_t>(1, nnz)));
+        auto *dt = static_cast<std::complex<double> *>(malloc(sizeof(std::complex<double>) * std::max<int64_t>(1, nnz)));
+        for (size_t i = 0; i <= d; ++i) ip[i] = mindquantum::Index(indptr[i]);
+        for (int64_t k = 0; k < nnz; ++k) {
+            ix[k] = mindquantum::Index(indices[k]);
+            dt[k] = {data[2 * k], data[2 * k + 1]};
+        }
+        auto csr = std::make_shared<mindquantum::sparse::CsrHdMatrix<double>>(d, mindquantum::Index(nnz), ip, ix, dt);
+        std::vector<std::shared_ptr<mindquantum::Hamiltonian<double>>> hams{
+            std::make_shared<mindquantum::Hamiltonian<double>>(csr, static_cast<mindquantum::Index>(n))};
+        std::vector<std::vector<double>> enc(n_samples, std::vector<double>(n_params));
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i < n_params; ++i) enc[s][i] = params[s * n_params + i];
+        sim_d sim{static_cast<mindquantum::Index>(n)};
+        const auto res = sim.GetExpectationWithGradMultiMulti(hams, c, h, enc, {}, names, {}, 1, 1);
+        for (int s = 0; s < n_samples; ++s)
+            for (int i = 0; i <= n_params; ++i) {
+                out[2 * (s * (n_params + 1) + i)] = res[s][0][i].real();
+                out[2 * (s * (n_params + 1) + i) + 1] = res[s][0][i].imag();
+            }
+        return 0;
+    } catch (...) {
+        return -2;
+    }
+}
+
 // The QRAM gradient (QramExpectationWithGrad, vector_state.tpp:1010-1018; gradient.h
 // QramHermitianAdjointGradient), complex128: one ansatz (every parameter an ansatz input, values
 // params[n_params]) applied to n_samples initial states init[n_samples][2^n] complex128 (re, im).

@@ -302,3 +302,28 @@ def grad_qram(n, circ, ham, ans, init_states):
         raise RuntimeError(f"mqref_grad_qram failed ({st})")
     out = out.reshape(S, 1 + len(names), 2)
     return out[..., 0] + 1j * out[..., 1]
+
+
+def grad_csr(n, circ, matrix, params):
+    """The reference's gradient with a Hamiltonian given as a sparse matrix (CsrHdMatrix from the
+    scipy CSR arrays, complex128, CPU), every parameter an encoder input: [samples][1 + n_params]."""
+    names = list(circ.params_name)
+    ints, dbls = _gate_table(circ, names)
+    m = matrix.tocsr()
+    indptr = np.ascontiguousarray(m.indptr, dtype=np.int64)
+    indices = np.ascontiguousarray(m.indices if m.nnz else [0], dtype=np.int64)
+    data = np.asarray(m.data if m.nnz else [0], dtype=np.complex128)
+    data = np.ascontiguousarray(np.stack([data.real, data.imag], axis=-1).reshape(-1))
+    params = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
+    S = params.shape[0]
+    out = np.zeros(S * (1 + len(names)) * 2, dtype=np.float64)
+    L, _ = lib('cpu')
+    P, I = ctypes.c_void_p, ctypes.c_int
+    L.mqref_grad_csr.argtypes = [I, I] + [P] * 8 + [ctypes.c_int64, P, P, P, I, I, P, P]
+    st = L.mqref_grad_csr(n, len(ints['kind']), _p(ints['kind']), _p(ints['o0']), _p(ints['o1']), _p(ints['ctrl']),
+                          _p(ints['param']), _p(dbls['coeff']), _p(dbls['cst']), _p(dbls['ch']), m.nnz, _p(indptr),
+                          _p(indices), _p(data), len(names), S, _p(params), _p(out))
+    if st != 0:
+        raise RuntimeError(f"mqref_grad_csr failed ({st})")
+    out = out.reshape(S, 1 + len(names), 2)
+    return out[..., 0] + 1j * out[..., 1]

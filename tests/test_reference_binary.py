@@ -7,8 +7,9 @@ seconds: config 1 exactly (16 qubits x 8 layers), the QNN encoder/ansatz, QAOA M
 Pauli Hamiltonians with Y terms.  Tolerance: 1e-12 (both FP64), complex64 reference within 1e-5.
 Both samplers (measurement-ending and mid-circuit) and the noise channels' trajectories are pinned
 shot for shot for the same seed; random circuits of every gate kind pin the gate formulas,
-Hermitian conjugates and Jacobians; the parameter-shift loop, the QRAM gradient and the
-non-Hermitian gradient's convention are pinned to the reference's own entry points; the dense
+Hermitian conjugates and Jacobians; the parameter-shift loop, the QRAM gradient, sparse-matrix
+Hamiltonians and the non-Hermitian gradient's convention are pinned to the reference's own entry
+points; the dense
 density-matrix oracle is pinned to the reference's DensityMatrixState.
 Skipped where the reference checkout was not available to build the library.
 
@@ -341,3 +342,27 @@ def test_qram_oracle_equals_reference():
     for s in range(3):
         orc = O.get_expectation_with_grad(n, [ham], circ, np.zeros((1, 0)), ans, [], names, np.complex128, qs[s])
         assert np.max(np.abs(ref[s] - orc[0, 0])) <= 1e-12
+
+
+def test_sparse_matrix_hamiltonian_oracle_equals_reference():
+    """A Hamiltonian given as a scipy CSR matrix (Hermitian, random rows of 0..20 entries, and the
+    CSR form of a Pauli sum): the oracle's Csr_Dot_Vec / ExpectationOfCsr path against the
+    reference's own gradient with its CsrHdMatrix Hamiltonian (1e-12)."""
+    import scipy.sparse as sp
+
+    from mindquantum_b200.core.operators import Hamiltonian
+
+    n = 6
+    rng = np.random.default_rng(31)
+    dim = 1 << n
+    lens = rng.integers(0, 21, size=dim)
+    rows = np.repeat(np.arange(dim), lens)
+    cols = np.concatenate([np.sort(rng.choice(dim, size=k, replace=False)) for k in lens])
+    m = sp.csr_matrix((rng.normal(size=rows.size) + 1j * rng.normal(size=rows.size), (rows, cols)), shape=(dim, dim))
+    circ = _every_gate_circuit(n, 30, 17)
+    names = list(circ.params_name)
+    vals = rng.uniform(0, 2 * np.pi, (2, len(names)))
+    for mat in ((m + m.conj().T).tocsr(), W.pauli_csr(W.random_pauli_hamiltonian(n, 10, rng), n)):
+        ref = R.grad_csr(n, circ, mat, vals)
+        orc = O.get_expectation_with_grad(n, [Hamiltonian(mat)], circ, vals, np.zeros(0), names, [])[:, 0]
+        assert np.max(np.abs(ref - orc)) <= 1e-12
