@@ -14,6 +14,12 @@ benchmark, and its results are stored next to this script:
 Run from the repository root (8 host threads: about five minutes for the 26-qubit case):
 
     python tests/golden/make_oracle_fixtures.py [hea26] [hea22]
+
+``--check-reference`` instead compares the committed fixtures with the reference's own CPU
+simulator built from its sources (oracle/_ref, ``make -C oracle ref``), complex128, and prints the
+largest differences (the 22-qubit one also runs in tests/test_reference_binary.py):
+
+    python tests/golden/make_oracle_fixtures.py --check-reference [hea26] [hea22]
 """
 import json
 import os
@@ -51,7 +57,27 @@ def _hea_fixture(n, layers, batch, samples, name):
         f.write('\n')
 
 
+def _check_reference(name):
+    from mindquantum_b200 import workloads
+    from oracle import refbin as R
+
+    with open(os.path.join(HERE, f"{name}_oracle.json"), encoding='utf8') as f:
+        fx = json.load(f)
+    circ, ham, params = workloads.hea(fx['n_qubits'], fx['layers'], fx['batch'], seed=0, encoder=True)
+    for row in fx['samples']:
+        s = row['sample']
+        t0 = time.time()
+        ref = R.grad(fx['n_qubits'], circ, ham, params[s:s + 1])[0]
+        print(f"{name}: sample {s}: |f - f_ref| = {abs(ref[0].real - row['f']):.3e}, max |g - g_ref| = "
+              f"{np.max(np.abs(ref[1:].real - np.array(row['grad']))):.3e} (reference {time.time() - t0:.1f} s)",
+              flush=True)
+
+
 def main(argv):
+    if '--check-reference' in argv:
+        for name in [a for a in argv if a != '--check-reference'] or ['hea22', 'hea26']:
+            _check_reference(name)
+        return
     which = argv or ['hea26', 'hea22']
     if 'hea22' in which:
         _hea_fixture(22, 6, 2, [0, 1], 'hea22')

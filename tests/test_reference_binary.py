@@ -366,3 +366,19 @@ def test_sparse_matrix_hamiltonian_oracle_equals_reference():
         ref = R.grad_csr(n, circ, mat, vals)
         orc = O.get_expectation_with_grad(n, [Hamiltonian(mat)], circ, vals, np.zeros(0), names, [])[:, 0]
         assert np.max(np.abs(ref - orc)) <= 1e-12
+
+
+def test_hea22_fixture_equals_reference():
+    """The committed FP64 fixture of the 22-qubit x 6-layer HEA workload (made by the oracle, used
+    by the GPU tests) against the reference's own adjoint gradient, both parameter rows (1e-12)."""
+    import json
+    import os
+
+    with open(os.path.join(os.path.dirname(__file__), 'golden', 'hea22_oracle.json'), encoding='utf8') as f:
+        fx = json.load(f)
+    circ, ham, params = W.hea(fx['n_qubits'], fx['layers'], fx['batch'], seed=0, encoder=True)
+    ref = R.grad(fx['n_qubits'], circ, ham, params)
+    for row in fx['samples']:
+        s = row['sample']
+        assert abs(ref[s, 0].real - row['f']) <= 1e-12
+        assert np.max(np.abs(ref[s, 1:].real - np.array(row['grad']))) <= 1e-12
