@@ -220,26 +220,21 @@ def reference_full_evaluations(n, layers, batch, threads, count):
     return times, kind
 
 
-def run_reference_gpu(args):
-    """The reference's own thrust GPU simulator (`mqvector_gpu`, built from its sources for sm_100a
-    into oracle/_ref/libmqref_gpu.so) on this GPU: full gradient evaluations of parameter set 0, one
-    at a time as the reference runs them, complex64 (the line's value) and complex128 (the plain
-    per-gate path of the reference).  Its API is synchronous and returns host values, so each
-    evaluation is timed on the host clock between device synchronizations."""
+def reference_gpu_evaluations(args, count, warmup):
+    """Seconds per full gradient evaluation of parameter set 0 on the reference's own thrust GPU
+    simulator (`mqvector_gpu`, built from its sources for sm_100a into oracle/_ref/libmqref_gpu.so),
+    one evaluation at a time as the reference runs them: {"c64": [...], "c128": [...]}.  Its API is
+    synchronous and returns host values, so each evaluation is timed on the host clock between
+    device synchronizations."""
     import torch
 
     from oracle import refbin as R
 
-    if not R.available('gpu'):
-        print(json.dumps({"impl": "reference", "unavailable": "the reference GPU simulator was not built "
-                                                              "(make -C oracle refgpu, with the reference checkout)"}))
-        return
     circ, ham, params = build_workload(args.qubits, args.layers, args.batch)
     c1, h1, p1 = build_workload(args.qubits, 1, args.batch)
-    count = max(1, min(args.steps, 3))
     out = {}
     for prec, c64 in (("c64", True), ("c128", False)):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             R.grad(args.qubits, c1, h1, p1[:1], complex64=c64, device='gpu')
         times = []
         for _ in range(count):
@@ -249,6 +244,20 @@ def run_reference_gpu(args):
             torch.cuda.synchronize()
             times.append(time.perf_counter() - t0)
         out[prec] = times
+    return out
+
+
+def run_reference_gpu(args):
+    """The reference's own thrust GPU simulator on this GPU: complex64 (the line's value) and
+    complex128 (the reference's plain per-gate GPU path) full gradient evaluations."""
+    from oracle import refbin as R
+
+    if not R.available('gpu'):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference GPU simulator was not built "
+                                                              "(make -C oracle refgpu, with the reference checkout)"}))
+        return
+    count = max(1, min(args.steps, 3))
+    out = reference_gpu_evaluations(args, count, args.warmup)
     t = float(np.mean(out["c64"]))
     value = 1.0 / t
     sample = (f"full gradient evaluations (all {args.layers} layers, lambda = H psi) of parameter set 0, "
@@ -303,7 +312,26 @@ def run_reference(args, rank):
                          "seconds": times},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    line["reference_gpu"] = _reference_gpu_extra(args)
     print(json.dumps(line), flush=True)
+
+
+def _reference_gpu_extra(args):
+    """Beside the CPU figure: the reference's own thrust GPU simulator on this box's GPU, one timed
+    evaluation per precision after a one-layer warm-up (a few seconds), or why it did not run."""
+    from oracle import refbin as R
+
+    try:
+        import torch
+
+        if not (R.available('gpu') and torch.cuda.is_available()):
+            return {"unavailable": "no GPU or the reference GPU simulator was not built"}
+        out = reference_gpu_evaluations(args, 1, 1)
+        return {"what": "the reference's thrust mqvector_gpu built for sm_100a, one evaluation of parameter set 0 "
+                        "at a time", "unit": UNIT,
+                "c64": 1.0 / float(np.mean(out["c64"])), "c128": 1.0 / float(np.mean(out["c128"])), "seconds": out}
+    except Exception as e:  # pylint: disable=broad-except
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def run_b200(args, rank, world, local_rank):
