@@ -1,6 +1,7 @@
 // extern "C" entry points of libmqb200: lowering of gate tables, pass execution, the
 // checkpointed adjoint-gradient driver, Hamiltonian passes, reductions and sampling.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -111,9 +112,22 @@ T *upload(const std::vector<T> &v) {
 
 bool is_diag_gid(int gid) { return gid == GID_RZ || gid == GID_PS || gid == GID_GP || gid == GID_RZZ; }
 
+// NVTX ranges: one per C-ABI call (named after it) and one around every kernel launch (named after
+// its kind), so an NVTX-aware profiler shows each call's pass structure.  With no tool attached a
+// range costs two calls through no-op function pointers.
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
+
 // Optional per-launch timing: CUDA events around every kernel launch of the engine, recorded on the
 // launching stream while enabled; mqb_timing_end synchronizes and reports the time per launch kind.
 enum TimedKind { TK_FWD = 0, TK_BWD, TK_HAM, TK_MATGEN, TK_PLAIN_APPLY, TK_PLAIN_GRAD, TK_SCATTER, TK_OTHER, TK_ROWS, TK_COUNT };
+const char *const kLaunchRange[TK_COUNT] = {"mqb forward pass",    "mqb adjoint pass",     "mqb hamiltonian pass",
+                                            "mqb gate matrices",   "mqb per-gate apply",   "mqb per-gate gradient",
+                                            "mqb gradient scatter", "mqb other launch",    "mqb row operations"};
 struct TimedLaunch {
     int kind;
     cudaEvent_t a, b;
@@ -122,10 +136,11 @@ bool g_timing = false;
 std::vector<TimedLaunch> g_timed;
 
 struct TimeScope {
+    Range range;
     TimedLaunch t{};
     cudaStream_t st;
     bool on;
-    TimeScope(int kind, cudaStream_t s) : st(s), on(g_timing) {
+    TimeScope(int kind, cudaStream_t s) : range(kLaunchRange[kind]), st(s), on(g_timing) {
         if (!on) return;
         t.kind = kind;
         cudaEventCreate(&t.a);
@@ -851,6 +866,7 @@ int mqb_program_create(int n_qubits, int precision, const mqb_gate_desc *gates, 
                        int n_terms, int n_params, const double *const_matrices, int64_t n_const_entries,
                        const mqb_program_options *options, mqb_program **out) {
     return guarded([&] {
+        Range range("mqb_program_create");
         if (!out) fail(MQB_ERR_INVALID, "out is null");
         *out = nullptr;
         if (n_qubits < 1 || n_qubits > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40], got %d", n_qubits);
@@ -1049,6 +1065,7 @@ int mqb_apply_workspace_size(const mqb_program *p, int64_t batch, size_t *bytes)
 int mqb_apply(mqb_program *p, void *states, int64_t batch, const double *params, int64_t param_stride,
               const double *custom, void *ws, size_t ws_bytes, void *stream) {
     return guarded([&] {
+        Range range("mqb_apply");
         if (!p || !states) fail(MQB_ERR_INVALID, "null argument");
         require_aligned(states, "states");
         if (batch < 1) fail(MQB_ERR_INVALID, "batch must be >= 1");
@@ -1065,6 +1082,7 @@ int mqb_apply(mqb_program *p, void *states, int64_t batch, const double *params,
 int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const uint64_t *mask_y, const uint64_t *mask_z,
                    const int32_t *num_y, const double *coeff, int n_terms, mqb_hamiltonian **out) {
     return guarded([&] {
+        Range range("mqb_ham_create");
         if (!out) fail(MQB_ERR_INVALID, "out is null");
         *out = nullptr;
         if (n_qubits < 1 || n_qubits > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
@@ -1107,6 +1125,7 @@ int mqb_ham_create(int n_qubits, int precision, const uint64_t *mask_x, const ui
 int mqb_ham_create_csr(int n_qubits, int precision, int64_t nnz, const int64_t *indptr, const int64_t *indices,
                        const void *data, mqb_hamiltonian **out) {
     return guarded([&] {
+        Range range("mqb_ham_create_csr");
         if (!out) fail(MQB_ERR_INVALID, "out is null");
         *out = nullptr;
         if (n_qubits < 1 || n_qubits > 31) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 31] for a sparse Hamiltonian");
@@ -1176,6 +1195,7 @@ int mqb_ham_destroy(mqb_hamiltonian *h) {
 
 int mqb_apply_hamiltonian(const mqb_hamiltonian *h, const void *in, void *out, int64_t batch, void *stream) {
     return guarded([&] {
+        Range range("mqb_apply_hamiltonian");
         if (!h || !in || !out) fail(MQB_ERR_INVALID, "null argument");
         require_aligned(in, "in");
         require_aligned(out, "out");
@@ -1192,6 +1212,7 @@ int mqb_apply_hamiltonian(const mqb_hamiltonian *h, const void *in, void *out, i
 
 int mqb_expectation(const mqb_hamiltonian *h, const void *bra, const void *ket, int64_t batch, double *out, void *stream) {
     return guarded([&] {
+        Range range("mqb_expectation");
         if (!h || !bra || !ket || !out) fail(MQB_ERR_INVALID, "null argument");
         if (batch < 0) fail(MQB_ERR_INVALID, "batch must be >= 0");
         require_aligned(bra, "bra");
@@ -1209,6 +1230,7 @@ int mqb_expectation(const mqb_hamiltonian *h, const void *bra, const void *ket, 
 int mqb_apply_matrix1(int n, int precision, void *states, int64_t batch, int qubit, uint64_t ctrl_mask,
                       const double *matrix, void *stream) {
     return guarded([&] {
+        Range range("mqb_apply_matrix1");
         if (!states || !matrix) fail(MQB_ERR_INVALID, "null argument");
         if (n < 1 || n > 40) fail(MQB_ERR_INVALID, "n_qubits must be in [1, 40]");
         if (qubit < 0 || qubit >= n) fail(MQB_ERR_INVALID, "qubit %d outside the register", qubit);
@@ -1277,6 +1299,7 @@ void rows_matrix1(int n, int precision, void *states, int64_t batch, int64_t cou
 int mqb_rows_apply_matrix1(int n, int precision, void *states, int64_t batch, int64_t count, const int64_t *rows,
                            const int32_t *qubits, const uint64_t *ctrl_masks, const double *matrices, void *stream) {
     return guarded([&] {
+        Range range("mqb_rows_apply_matrix1");
         rows_matrix1(n, precision, states, batch, count, rows, qubits, ctrl_masks, matrices, nullptr,
                      static_cast<cudaStream_t>(stream));
     });
@@ -1294,6 +1317,7 @@ int mqb_rows_matrix1_norm(int n, int precision, const void *states, int64_t batc
 
 int mqb_vdot(int n, int precision, const void *a, const void *b, int64_t batch, double *out, void *stream) {
     return guarded([&] {
+        Range range("mqb_vdot");
         if (!a || !b || !out) fail(MQB_ERR_INVALID, "null argument");
         require_register(n, precision);
         if (batch < 0) fail(MQB_ERR_INVALID, "batch must be >= 0");
@@ -1322,6 +1346,7 @@ int mqb_grad_workspace_size(const mqb_program *p, int64_t batch, int n_hams, int
 int mqb_grad_norm_checks(mqb_program *p, const void *ws, size_t ws_bytes, int64_t batch, int n_hams, int stride,
                          double *out, int capacity, int *n_checks, void *stream) {
     return guarded([&] {
+        Range range("mqb_grad_norm_checks");
         if (!p || !n_checks) fail(MQB_ERR_INVALID, "null argument");
         if (n_hams < 1 || batch < 1) fail(MQB_ERR_INVALID, "invalid batch or number of Hamiltonians");
         SchedDev &sd = grad_schedule(*p, n_hams);
@@ -1345,6 +1370,7 @@ int mqb_expectation_with_grad(mqb_program *p, const mqb_hamiltonian *const *hams
                               const double *custom, double *f, double *grad, int stride, void *ws, size_t ws_bytes,
                               void *stream) {
     return guarded([&] {
+        Range range("mqb_expectation_with_grad");
         if (!p || !hams || !f || !grad) fail(MQB_ERR_INVALID, "null argument");
         require_aligned(init, "init_states");
         require_aligned(ws, "workspace");
@@ -1371,6 +1397,7 @@ int mqb_adjoint_with_lambda(mqb_program *p, const void *lam, int lam_batched, co
                             int64_t batch, const double *params, int64_t param_stride, const double *custom,
                             double *grad, int stride, void *ws, size_t ws_bytes, void *stream) {
     return guarded([&] {
+        Range range("mqb_adjoint_with_lambda");
         if (!p || !lam || !grad) fail(MQB_ERR_INVALID, "null argument");
         require_aligned(lam, "lambda");
         require_aligned(init, "init_states");
@@ -1400,6 +1427,7 @@ int mqb_sample_scratch_size(int n, size_t *bytes) {
 int mqb_sample_indices(int n, int precision, const void *state, const double *u, int64_t shots, int64_t *out,
                        void *scratch, size_t scratch_bytes, void *stream) {
     return guarded([&] {
+        Range range("mqb_sample_indices");
         require_register(n, precision);
         if (shots < 0) fail(MQB_ERR_INVALID, "shots must be >= 0");
         if (!state || (shots > 0 && (!u || !out))) fail(MQB_ERR_INVALID, "null argument");
@@ -1423,6 +1451,7 @@ int mqb_sample_indices(int n, int precision, const void *state, const double *u,
 
 int mqb_qubit_one_probability(int n, int precision, const void *state, int q, double *out, void *stream) {
     return guarded([&] {
+        Range range("mqb_qubit_one_probability");
         require_register(n, precision);
         if (!state || !out) fail(MQB_ERR_INVALID, "null argument");
         if (q < 0 || q >= n) fail(MQB_ERR_INVALID, "qubit out of range");
@@ -1436,6 +1465,7 @@ int mqb_qubit_one_probability(int n, int precision, const void *state, int q, do
 
 int mqb_collapse(int n, int precision, void *state, int q, int outcome, double scale, void *stream) {
     return guarded([&] {
+        Range range("mqb_collapse");
         require_register(n, precision);
         if (!state) fail(MQB_ERR_INVALID, "null argument");
         if (q < 0 || q >= n) fail(MQB_ERR_INVALID, "qubit out of range");
