@@ -708,6 +708,9 @@ class MQVectorB200(BackendBase):
 
         wrapper = GradOpsWrapper(grad_ops, hams, circ_right, circ_left, enc_names, ans_names, parallel_worker, self)
         wrapper.set_str(f"{self.n_qubits} qubit{'' if self.n_qubits == 1 else 's'} {self.name} VQA Operator")
+        # the same evaluation on device tensors, for the autograd operators (framework/operations.py)
+        wrapper.device_grad = lambda params: sim.expectation_with_grad_tensor(
+            hams, circ_right, params, names, init_state=sim._state)  # pylint: disable=protected-access
         return wrapper
 
     # ------------------------------------------------------------------ non-Hermitian gradient

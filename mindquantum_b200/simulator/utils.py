@@ -40,6 +40,10 @@ class GradOpsWrapper:
         self.parallel_worker = parallel_worker
         self.sim = sim
         self.str = ''
+        # set by the Hermitian adjoint operator of the state-vector backend: device_grad(params
+        # [batch][n_enc + n_ans] float64 tensor) -> (f [batch][n_hams][2], g [batch][n_hams][P])
+        # tensors on the device, the path the autograd operators take
+        self.device_grad = None
 
     def __call__(self, *args):
         return self.grad_ops(*args)
