@@ -113,3 +113,39 @@ def test_layers_train_their_weights():
         assert layer.weight.grad.shape == (4,)
     with pytest.raises(ValueError, match="Weight init shape"):
         MQLayer(op, weight=torch.zeros(5))
+
+
+@pytest.mark.gpu
+def test_operators_over_non_hermitian_and_density_matrix_grad_ops():
+    """On the B200 backends: MQOps / MQN2Ops over a non-Hermitian operator
+    <phi| U_l^dag H U_r(enc, ans) |psi> (circ_left and simulator_left) give Re f and |f|^2 of the
+    operator's own values and pass gradcheck; MQAnsatzOnlyOps over a noisy density-matrix operator
+    passes gradcheck."""
+    from mindquantum_b200 import complex128
+    from mindquantum_b200.core import gates as G
+    from mindquantum_b200.core.circuit import Circuit
+    from mindquantum_b200.core.operators import Hamiltonian, QubitOperator
+    from mindquantum_b200.simulator import Simulator
+
+    n = 3
+    rng = np.random.default_rng(3)
+    enc = Circuit([G.RX(f'x{i}').on(i) for i in range(n)]).as_encoder()
+    ans = Circuit([G.RY(f'w{i}').on(i) for i in range(n)] + [G.X.on(1, 0), G.RZ('w9').on(2)])
+    circ = enc + ans
+    left = Circuit([G.H.on(0), G.RX(0.3).on(1), G.X.on(2, 1)])
+    ham = Hamiltonian(QubitOperator('Z0 X1', 0.7) + QubitOperator('Y2', 0.2))
+    sim = Simulator('mqvector_b200', n, dtype=complex128)
+    sim_left = Simulator('mqvector_b200', n, dtype=complex128)
+    sim_left.set_qs(rng.normal(size=8) + 1j * rng.normal(size=8))
+    ops = sim.get_expectation_with_grad(ham, circ, left, sim_left)
+    e = torch.tensor(rng.uniform(0, 3, (2, n)), dtype=torch.float64, requires_grad=True)
+    a = torch.tensor(rng.uniform(0, 3, len(circ.ansatz_params_name)), dtype=torch.float64, requires_grad=True)
+    f, _, _ = ops(e.detach().numpy(), a.detach().numpy())
+    for cls, ref in ((MQOps, f.real), (MQN2Ops, np.abs(f) ** 2)):
+        assert np.max(np.abs(cls(ops)(e, a).detach().cpu().numpy() - ref)) <= 1e-12
+        assert torch.autograd.gradcheck(lambda x, y, c=cls: c(ops)(x, y), (e, a), eps=1e-6, atol=1e-6)
+    dm = Simulator('mqmatrix_b200', n, dtype=complex128)
+    c2 = ans + G.DepolarizingChannel(0.1).on(0)
+    ops2 = dm.get_expectation_with_grad(ham, c2)
+    a2 = torch.tensor(rng.uniform(0, 3, len(c2.params_name)), dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(lambda y: MQAnsatzOnlyOps(ops2)(y), (a2,), eps=1e-6, atol=1e-6)
