@@ -106,12 +106,13 @@ class Simulator:
         fn = getattr(self.backend, 'entropy', None)
         return fn() if fn else 0.0
 
-    def get_partial_trace(self, obj_qubits):
-        if isinstance(obj_qubits, int):
-            obj_qubits = [obj_qubits]
+    def get_partial_trace(self, qubits_to_trace):
+        """Trace out ``qubits_to_trace`` (simulator.py:516; density-matrix backends only)."""
+        if isinstance(qubits_to_trace, int):
+            qubits_to_trace = [qubits_to_trace]
         if not hasattr(self.backend, 'get_partial_trace'):
             raise ValueError(f"{self.backend.name} simulator not support partial trace method.")
-        return self.backend.get_partial_trace(list(obj_qubits))
+        return self.backend.get_partial_trace(list(qubits_to_trace))
 
     def get_reduced_density_matrix(self, kept_qubits):
         if isinstance(kept_qubits, int):
