@@ -478,6 +478,13 @@ class MQMatrixB200(BackendBase):
         """Reduced state of ``qubits`` (mqsim.py:598-626)."""
         return qs_of_qubits(self, qubits, ket)
 
+    def get_circuit_matrix(self, circuit, pr):
+        """Unitary of a channel-free ``circuit`` (mqsim.py:199-201), from the state-vector engine."""
+        if circuit.is_noise_circuit:
+            raise ValueError("a circuit with noise channels has no circuit matrix")
+        return MQVectorB200('mqvector_b200', self.n_qubits, self.seed, self.arithmetic_type).get_circuit_matrix(
+            circuit, pr)
+
     def entropy(self):
         ev = np.real(np.linalg.eigvals(self.get_qs()))
         return float(-sum(x * np.log(x) for x in ev if x > 0))

@@ -148,6 +148,37 @@ class MQVectorB200(BackendBase):
             return '\n'.join(f"{v}¦{format(i, f'0{self.n_qubits}b')}⟩" for i, v in enumerate(qs) if abs(v) > 1e-12)
         return qs
 
+    # pure-state answers of MQSim's density-matrix methods for a state vector (mqsim.py:546-597)
+    def entropy(self):
+        return 0.0
+
+    def purity(self):
+        return 1.0
+
+    def get_pure_state_vector(self):
+        return self.get_qs()
+
+    def get_partial_trace(self, obj_qubits):
+        raise ValueError(f"{self.name} simulator not support partial trace method.")
+
+    def get_circuit_matrix(self, circuit, pr):
+        """Matrix of ``circuit`` with parameters ``pr`` (mqsim.py:199-201): column j is the circuit
+        applied to |j>, evaluated column by column on a scratch simulator of this size and dtype;
+        measurement gates are dropped."""
+        if not isinstance(circuit, Circuit):
+            raise TypeError(f"circuit requires a Circuit, but get {type(circuit)}")
+        body = circuit.remove_measure()
+        dim = 1 << self.n_qubits
+        sim = MQVectorB200(self.name, self.n_qubits, self.seed, self.arithmetic_type, self.fuse, self.device, self.jit)
+        cols = []
+        for j in range(dim):
+            e = np.zeros(dim, dtype=np.complex128)
+            e[j] = 1
+            sim.set_qs(e)
+            sim.apply_circuit(body, pr)
+            cols.append(sim.get_qs())
+        return np.array(cols).T
+
     def get_reduced_density_matrix(self, kept_qubits):
         """Density matrix of ``kept_qubits`` with the other qubits traced out (mqsim.py:559-570,
         VectorState::GetReducedDensityMatrix): computed on the device from the state."""

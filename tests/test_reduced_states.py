@@ -96,3 +96,29 @@ def test_reduced_states_on_both_backends():
         sv.get_reduced_density_matrix([0, 1, 2, 3, 4, 5])
     with pytest.raises(NotImplementedError):
         sv.set_threads_number(4)
+    # the pure-state answers of the density-matrix methods on a state vector (mqsim.py:546-597)
+    be = sv.backend
+    assert be.entropy() == 0 and be.purity() == 1.0
+    assert np.max(np.abs(be.get_pure_state_vector() - qs)) <= 1e-12
+    with pytest.raises(ValueError, match="partial trace"):
+        be.get_partial_trace([0])
+
+
+@pytest.mark.gpu
+def test_circuit_matrix_on_both_backends():
+    """get_circuit_matrix (mqsim.py:199-201): column j is the circuit applied to |j>, against the
+    oracle's columns (1e-12), on the state-vector and the density-matrix backend."""
+    from mindquantum_b200 import complex128, workloads as W
+    from mindquantum_b200.simulator import Simulator
+
+    n = 4
+    circ, _, params = W.hea(n, 2, 1, seed=6, encoder=False)
+    pr = dict(zip(circ.params_name, params[0].tolist()))
+    ref = np.zeros((1 << n, 1 << n), dtype=np.complex128)
+    for j in range(1 << n):
+        e = np.zeros(1 << n, dtype=np.complex128)
+        e[j] = 1
+        ref[:, j] = O.OracleSim(n, state=e).apply_circuit(circ, pr).qs
+    for backend in ('mqvector_b200', 'mqmatrix_b200'):
+        m = Simulator(backend, n, dtype=complex128).backend.get_circuit_matrix(circ, pr)
+        assert m.shape == ref.shape and np.max(np.abs(m - ref)) <= 1e-12
