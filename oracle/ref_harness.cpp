@@ -63,6 +63,12 @@ int mqref_grad_csr(int n, int n_gates, const int *kind, const int *obj0, const i
         auto *ip = static_cast<mindquantum::Index *>(malloc(sizeof(mindquantum::Index) * (d + 1)));
         auto *ix = static_cast<mindquantum::Index *>(malloc(sizeof(mindquantum::Index) * std::max<int64_t>(1, nnz)));
         auto *dt = static_cast<std::complex<double> *>(malloc(sizeof(std::complex<double>) * std::max<int64_t>(1, nnz)));
+        if (!ip || !ix || !dt) {
+            free(ip);
+            free(ix);
+            free(dt);
+            return -3;
+        }
         for (size_t i = 0; i <= d; ++i) ip[i] = mindquantum::Index(indptr[i]);
         for (int64_t k = 0; k < nnz; ++k) {
             ix[k] = mindquantum::Index(indices[k]);
